@@ -1,0 +1,386 @@
+"""Benchmark of the BVH build-and-trace hot path (one JSON line on rank 0).
+
+Default workload: the 1M-triangle displaced sphere (1024x512 UV sphere, 1,046,528 triangles, radius 1 with
+4-octave value-noise displacement 0.05) and 4M rays from a radius-3 sphere into the inward hemisphere;
+PLOC r = 16 over 30-bit Morton codes, binary FP32 BVH, closest hit with the reference-exact leaf test.
+
+A step = one build over the resident triangles + one closest-hit trace of the resident rays.
+  value          build throughput, Mtri/s (triangles / build time, CUDA events on the build stream)
+  trace          closest-hit throughput, Mrays/s (CUDA events around the trace launch)
+  e2e            the same step through the public API with HOST inputs: pinned vertex arrays copied in,
+                 build, rays copied in, trace, hits copied out; Mtri/s over the whole step
+  roofline       build pipeline against HBM (algorithmic bytes per triangle from the byte model in
+                 DESIGN.md, over the measured build time), plus the trace kernel's own roofline
+  cpu_baseline   the reference's SBvh::Build + SBvh::Intersect (oracle/_ref, compiled from the
+                 reference's sources) on the host cores, on a bounded sample of the same workload
+
+--impl reference runs only the reference CPU implementation on the same workload and prints its line.
+Multi-GPU (torchrun): replicas only; every rank builds and traces its own copy (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PLOC build Mtri/s + closest-hit Mrays/s on 1 B200; batched vs plain; SAH cost"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]
+                          and "Not" not in s[3 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def workload(name, rays_override=None):
+    from diplodocus_b200 import scenes as S
+    if name == "displaced_sphere":
+        tris, rays = S.displaced_sphere(n_rays=rays_override or 4 * 1024 * 1024)
+        desc = "1024x512 displaced UV sphere (1,046,528 tris), 4M inward-hemisphere rays from r=3"
+    elif name == "small":
+        tris, rays = S.small_scene()
+        desc = "open box + 64x32 sphere (3,978 tris), 512x512 pinhole primary rays"
+    elif name == "soup16m":
+        tris = S.soup(16 * 1024 * 1024, seed=3)
+        rays = S.random_rays(rays_override or 16 * 1024 * 1024, seed=3)
+        desc = "16M log-normal triangle soup, 16M random rays"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return tris, rays, desc
+
+
+# ---------------------------------------------------------------------------------------------------
+# Reference arm: the reference's own CPU code (SBvh) on the host cores.
+# ---------------------------------------------------------------------------------------------------
+def cpu_reference_step_stats(tris, rays, sample_rays, threads):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ref = O.RefOracle()
+    t0 = time.perf_counter()
+    sb = ref.sbvh(tris)
+    build_s = time.perf_counter() - t0
+    idx = np.linspace(0, len(rays) - 1, sample_rays).astype(np.int64)
+    sample = np.ascontiguousarray(rays[idx])
+    t0 = time.perf_counter()
+    sb.trace(sample, threads=threads)
+    trace_s = time.perf_counter() - t0
+    sah = sb.sah_cost()[0]
+    sb.close()
+    return build_s, trace_s, sah
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    tris, rays, desc = workload(args.workload, args.rays)
+    threads = os.cpu_count() or 1
+    sample_rays = min(len(rays), args.ref_sample_rays)
+    for _ in range(args.warmup if args.warmup <= 1 else 1):
+        cpu_reference_step_stats(tris, rays[:4096], 4096, threads)
+    builds, traces = [], []
+    sah = None
+    for _ in range(args.steps):
+        b, t, sah = cpu_reference_step_stats(tris, rays, sample_rays, threads)
+        builds.append(b)
+        traces.append(t)
+    n = len(tris)
+    value = n / np.mean(builds) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mtri/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * (np.mean(builds) + np.mean(traces)), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "triangles": n, "rays": len(rays),
+                   "build": "SBvh binned SAH (bin_count 16, leaf < 4, depth 32)"},
+        "trace": {"value": round(sample_rays / np.mean(traces) / 1e6, 4), "unit": "Mrays/s",
+                  "sample_rays": sample_rays},
+        "sah_cost": round(sah, 4),
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mtri/s", "cores": 1, "kind": "reference",
+                         "sample": f"SBvh::Build of all {n} triangles on 1 thread (it is single-threaded); "
+                                   f"SBvh::Intersect of {sample_rays} of {len(rays)} rays on {threads} threads"},
+        "e2e": {"value": round(value, 4), "unit": "Mtri/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------------
+# GPU arm.
+# ---------------------------------------------------------------------------------------------------
+def build_bytes_per_tri(code_type, digit_bits=8, node_bytes_per_tri=None):
+    """Algorithmic bytes of one build per triangle (byte model, Morton30: 176 B, EMC60: 308 B)."""
+    k = 4 if code_type == 0 else 8
+    passes = -(-(30 if code_type == 0 else 60) // 8)
+    node = 64.0 if node_bytes_per_tri is None else node_bytes_per_tri
+    return 36 + (k + 4) + passes * 2 * (k + 4) + node + 4
+
+
+def run_gpu(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    from diplodocus_b200 import _lib as L
+    from diplodocus_b200 import accel as A
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = L.load()
+    tris, rays_np, desc_txt = workload(args.workload, args.rays)
+    n, nr = len(tris), len(rays_np)
+    kind = {"morton30": A.AccelerationStructureType.kPloc, "emc60": A.AccelerationStructureType.kPlocEmc}[args.code]
+    cfg = A.AccelerationStructureConfig(kind, nn_search_radius=args.radius, leaf_test=args.leaf_test)
+    v = A.soa_vertices(tris, dev)
+    rays = A.as_device_rays(rays_np, dev)
+    hits = torch.empty((nr, 4), dtype=torch.int32, device=dev)
+    desc = A.make_desc(*v, cfg)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    lt = A._leaf_test(args.leaf_test)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
+
+    def step(ev=None):
+        h = C.c_void_p(0)
+        if ev is not None:
+            ev[0].record(stream)
+        L.check(lib.dipl_bvh_build(C.byref(desc), C.byref(h), sp), "dipl_bvh_build")
+        if ev is not None:
+            ev[1].record(stream)
+        L.check(lib.dipl_bvh_trace_closest(h, C.c_void_p(rays.data_ptr()), nr, C.c_void_p(hits.data_ptr()), lt, 0,
+                                           sp), "dipl_bvh_trace_closest")
+        if ev is not None:
+            ev[2].record(stream)
+        return h
+
+    def destroy(h):
+        lib.dipl_bvh_destroy(h)
+
+    for _ in range(args.warmup):
+        destroy(step())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    launches0 = lib.dipl_kernel_launch_count()
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        wall0 = time.perf_counter()
+        for k in range(args.steps):
+            flush.zero_()  # L2 flushed between steps; outside the events
+            h = step(evs[k])
+            destroy(h)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+    launches = lib.dipl_kernel_launch_count() - launches0
+    build_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    trace_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    step_ms = [e[0].elapsed_time(e[2]) for e in evs]
+    t_step = float(np.sum(step_ms))
+    t_build = float(np.sum(build_ms))
+    t_trace = float(np.sum(trace_ms))
+    if world > 1:
+        tt = torch.tensor([t_step, t_build, t_trace], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step, t_build, t_trace = tt.tolist()
+
+    # SAH cost and info of one build (outside the timed region)
+    h = step()
+    sah = C.c_double(0)
+    lib.dipl_bvh_sah_cost(h, C.byref(sah), sp)
+    info = L.BvhInfo()
+    lib.dipl_bvh_get_info(h, C.byref(info))
+    # counted trace for the trace byte model (same kernel, same rays)
+    ctr = torch.zeros(2, dtype=torch.int64, device=dev)
+    lib.dipl_bvh_trace_closest_counted(h, C.c_void_p(rays.data_ptr()), nr, C.c_void_p(hits.data_ptr()), lt, 0,
+                                       C.c_void_p(ctr.data_ptr()), sp)
+    torch.cuda.synchronize()
+    visits, tests = [int(x) for x in ctr.cpu().tolist()]
+    hit_rate = float((hits[:, 0] >= 0).float().mean().item())
+    destroy(h)
+
+    # ---- e2e through the public API with host buffers -------------------------------------------------
+    host_v = [x.cpu().pin_memory() for x in v]
+    host_rays = rays.cpu().pin_memory()
+    host_hits = torch.empty((nr, 4), dtype=torch.int32).pin_memory()
+    dv = [torch.empty_like(x) for x in v]
+    drays = torch.empty_like(rays)
+    dhits = torch.empty_like(hits)
+    edesc = A.make_desc(*dv, cfg)
+
+    def e2e_step():
+        for d_, h_ in zip(dv, host_v):
+            d_.copy_(h_, non_blocking=True)
+        hh = C.c_void_p(0)
+        L.check(lib.dipl_bvh_build(C.byref(edesc), C.byref(hh), sp), "dipl_bvh_build")
+        drays.copy_(host_rays, non_blocking=True)
+        L.check(lib.dipl_bvh_trace_closest(hh, C.c_void_p(drays.data_ptr()), nr, C.c_void_p(dhits.data_ptr()), lt, 0,
+                                           sp), "dipl_bvh_trace_closest")
+        host_hits.copy_(dhits, non_blocking=True)
+        return hh
+
+    for _ in range(2):
+        destroy(e2e_step())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        destroy(e2e_step())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([t_e2e], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = tt.item()
+    h2d = sum(x.numel() * 4 for x in v) + rays.numel() * 4
+    d2h = hits.numel() * 4
+
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    steps = args.steps
+    build_s = t_build / 1e3 / steps
+    trace_s = t_trace / 1e3 / steps
+    bpt = build_bytes_per_tri(desc.code_type, 8, info.node_bytes / max(n, 1))
+    achieved_build = bpt * n / build_s / 1e9
+    ray_bytes = 32 + 16 + (visits / nr) * 64 + (tests / nr) * 36
+    achieved_trace = ray_bytes * nr / trace_s / 1e9
+    value = world * n / build_s / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mtri/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": round(t_step / steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc_txt, "triangles": n, "rays": nr,
+                   "code": args.code, "nn_search_radius": args.radius, "leaf_test": args.leaf_test,
+                   "layout": "binary", "max_triangles_per_leaf": 4, "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "trace": {"value": round(world * nr / trace_s / 1e6, 3), "unit": "Mrays/s", "hit_rate": round(hit_rate, 4),
+                  "node_visits_per_ray": round(visits / nr, 3), "tri_tests_per_ray": round(tests / nr, 3)},
+        "build_ms": round(build_s * 1e3, 4), "trace_ms": round(trace_s * 1e3, 4),
+        "sah_cost": round(sah.value, 4), "ploc_iterations": int(info.ploc_iterations), "bvh_depth": int(info.depth),
+        "roofline": {"bound": "hbm", "achieved": round(achieved_build, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved_build / peak, 4), "traffic": None,
+                     "kernel": "build pipeline (bounds, codes, sort, PLOC, layout)",
+                     "bytes_per_unit": round(bpt, 1), "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
+        "roofline_trace": {"bound": "hbm", "achieved": round(achieved_trace, 1), "peak": peak, "unit": "GB/s",
+                           "frac": round(achieved_trace / peak, 4), "bytes_per_ray": round(ray_bytes, 1)},
+        "e2e": {"value": round(world * n * steps / (t_e2e / 1e3) / 1e6, 3), "unit": "Mtri/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "note": "whole step (H2D vertices + build + H2D rays + trace + D2H hits) per triangle"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "wall_s_timed_region": round(wall, 4),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        threads = os.cpu_count() or 1
+        sample_rays = min(nr, args.ref_sample_rays)
+        try:
+            b, t, rsah = cpu_reference_step_stats(tris, rays_np, sample_rays, threads)
+            line["cpu_baseline"] = {"value": round(n / b / 1e6, 4), "unit": "Mtri/s", "cores": 1, "kind": "reference",
+                                    "sample": f"one SBvh::Build of all {n} triangles (1 thread); SBvh::Intersect of "
+                                              f"{sample_rays} rays on {threads} threads: "
+                                              f"{sample_rays / t / 1e6:.3f} Mrays/s",
+                                    "trace_mrays_per_s": round(sample_rays / t / 1e6, 4),
+                                    "trace_threads": threads, "sah_cost": round(rsah, 4)}
+        except Exception as e:  # the harness is absent when it was never built here
+            line["cpu_baseline"] = {"value": None, "unit": "Mtri/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="dipl", choices=["dipl", "reference"])
+    ap.add_argument("--workload", default="displaced_sphere", choices=["displaced_sphere", "small", "soup16m"])
+    ap.add_argument("--code", default="morton30", choices=["morton30", "emc60"])
+    ap.add_argument("--radius", type=int, default=16)
+    ap.add_argument("--leaf-test", default="ref_mt", choices=["ref_mt", "watertight"])
+    ap.add_argument("--rays", type=int, default=None)
+    ap.add_argument("--ref-sample-rays", type=int, default=1 << 18)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

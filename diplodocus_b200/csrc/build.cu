@@ -1,0 +1,1117 @@
+// BVH build on the device: scene bounds -> Morton30 / EMC60 codes -> LSD radix sort -> PLOC clustering
+// (one persistent cooperative launch for every iteration) -> leaf collapse and node layout.
+//
+// The reference builds top-down on one CPU thread (SBvh::Build, src/acceleration/sbvh.cc:17-58, binned SAH
+// in FindBestSplit :193-266, partition in Subdivide :268-341). This is the bottom-up GPU replacement the
+// reference plans but does not contain (README.md:156-161; src/gpu/acceleration/ is empty): PLOC after
+// Meister & Bittner (2017), codes after Karras (2012) and Vinkler et al. (2017).
+//
+// Batching: a build of M meshes runs as one pipeline over the concatenation of their triangles. Sort
+// keys carry the mesh index above the code, so every mesh is a contiguous run of the sorted order, and
+// PLOC never pairs clusters of different meshes; it stops when one cluster per mesh is left.
+#include <cooperative_groups.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+
+namespace dipl {
+
+struct MeshDesc {
+    const float* v0;
+    const float* v1;
+    const float* v2;
+    long long first;  // first global triangle index
+    long long count;
+};
+
+// Per-mesh code parameters (computed on the device from the bounds).
+struct CodeParams {
+    float lo[4];
+    float s[4];
+    unsigned long long top[4];
+    unsigned long long mask[4];
+    int bits[4];
+};
+
+struct PlocCtrl {
+    uint32_t n[2];       // cluster count at the start of an iteration (by parity)
+    uint32_t merges[2];  // internal nodes created before an iteration (by parity)
+    uint32_t iterations;
+    uint32_t pad;
+    GridBarrier barrier;
+};
+
+namespace {
+
+constexpr int kRadiusMax = 32;
+constexpr int kPlocIpt = 4;
+constexpr uint32_t kMaxPlocIterations = 1u << 16;
+
+__device__ __forceinline__ int find_mesh(const long long* __restrict__ offsets, int m, long long g) {
+    int lo = 0, hi = m - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (offsets[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct Tri {
+    float3 a, b, c;
+};
+
+__device__ __forceinline__ Tri load_tri(const MeshDesc& md, long long local) {
+    const float* p0 = md.v0 + 3 * local;
+    const float* p1 = md.v1 + 3 * local;
+    const float* p2 = md.v2 + 3 * local;
+    Tri t;
+    t.a = make_float3(__ldg(p0), __ldg(p0 + 1), __ldg(p0 + 2));
+    t.b = make_float3(__ldg(p1), __ldg(p1 + 1), __ldg(p1 + 2));
+    t.c = make_float3(__ldg(p2), __ldg(p2 + 1), __ldg(p2 + 2));
+    return t;
+}
+
+// Centroid ((v0 + v1) + v2) / 3, the reference's CalculateTriangleCentroid (src/scene/triangle.h:36).
+__device__ __forceinline__ float3 centroid(const Tri& t) {
+    return make_float3(__fdiv_rn(__fadd_rn(__fadd_rn(t.a.x, t.b.x), t.c.x), 3.0f),
+                       __fdiv_rn(__fadd_rn(__fadd_rn(t.a.y, t.b.y), t.c.y), 3.0f),
+                       __fdiv_rn(__fadd_rn(__fadd_rn(t.a.z, t.b.z), t.c.z), 3.0f));
+}
+
+__device__ __forceinline__ void tri_box(const Tri& t, float3& lo, float3& hi) {
+    lo = make_float3(fminf(fminf(t.a.x, t.b.x), t.c.x), fminf(fminf(t.a.y, t.b.y), t.c.y),
+                     fminf(fminf(t.a.z, t.b.z), t.c.z));
+    hi = make_float3(fmaxf(fmaxf(t.a.x, t.b.x), t.c.x), fmaxf(fmaxf(t.a.y, t.b.y), t.c.y),
+                     fmaxf(fmaxf(t.a.z, t.b.z), t.c.z));
+}
+
+// ------------------------------------------------------------------------------------------------
+// Scene bounds: centroid box and vertex box per mesh, as order-preserving ints (atomic min/max).
+// ------------------------------------------------------------------------------------------------
+struct Bounds {
+    int v[12];  // cmin xyz, cmax xyz, bmin xyz, bmax xyz
+};
+
+__global__ void bounds_init_kernel(Bounds* b, int m) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    int pinf = float_to_ordered(__int_as_float(0x7F800000)), ninf = float_to_ordered(__int_as_float(0xFF800000));
+    for (int a = 0; a < 3; ++a) {
+        b[k].v[a] = pinf;
+        b[k].v[3 + a] = ninf;
+        b[k].v[6 + a] = pinf;
+        b[k].v[9 + a] = ninf;
+    }
+}
+
+__device__ __forceinline__ void flush_bounds(Bounds* b, const float* acc) {
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&b->v[a], float_to_ordered(acc[a]));
+        atomicMax(&b->v[3 + a], float_to_ordered(acc[3 + a]));
+        atomicMin(&b->v[6 + a], float_to_ordered(acc[6 + a]));
+        atomicMax(&b->v[9 + a], float_to_ordered(acc[9 + a]));
+    }
+}
+
+__device__ __forceinline__ void reset_acc(float* acc) {
+    for (int a = 0; a < 3; ++a) {
+        acc[a] = acc[6 + a] = __int_as_float(0x7F800000);
+        acc[3 + a] = acc[9 + a] = __int_as_float(0xFF800000);
+    }
+}
+
+__global__ void __launch_bounds__(256) bounds_kernel(const MeshDesc* __restrict__ meshes,
+                                                     const long long* __restrict__ offsets, int m, long long n,
+                                                     long long chunk, Bounds* __restrict__ out) {
+    const long long beg = blockIdx.x * chunk, end = min(n, beg + chunk);
+    if (beg >= end) return;
+    const int m_first = find_mesh(offsets, m, beg), m_last = find_mesh(offsets, m, end - 1);
+    float acc[12];
+    reset_acc(acc);
+    int cur = -1;
+    bool any = false;
+    for (long long g = beg + threadIdx.x; g < end; g += blockDim.x) {
+        int k = (m_first == m_last) ? m_first : find_mesh(offsets, m, g);
+        if (k != cur) {
+            if (any && m_first != m_last) {
+                flush_bounds(&out[cur], acc);
+                reset_acc(acc);
+            }
+            cur = k;
+        }
+        any = true;
+        Tri t = load_tri(meshes[k], g - meshes[k].first);
+        float3 c = centroid(t), lo, hi;
+        tri_box(t, lo, hi);
+        acc[0] = fminf(acc[0], c.x), acc[1] = fminf(acc[1], c.y), acc[2] = fminf(acc[2], c.z);
+        acc[3] = fmaxf(acc[3], c.x), acc[4] = fmaxf(acc[4], c.y), acc[5] = fmaxf(acc[5], c.z);
+        acc[6] = fminf(acc[6], lo.x), acc[7] = fminf(acc[7], lo.y), acc[8] = fminf(acc[8], lo.z);
+        acc[9] = fmaxf(acc[9], hi.x), acc[10] = fmaxf(acc[10], hi.y), acc[11] = fmaxf(acc[11], hi.z);
+    }
+    if (m_first != m_last) {
+        if (any) flush_bounds(&out[cur], acc);
+        return;
+    }
+    // single mesh in this block: warp + block reduction, then 12 atomics
+    __shared__ float s_acc[8][12];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        float v = acc[i];
+        bool is_min = (i % 6) < 3;
+        for (int o = 16; o > 0; o >>= 1) {
+            float w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = is_min ? fminf(v, w) : fmaxf(v, w);
+        }
+        if (lane == 0) s_acc[warp][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r[12];
+        for (int i = 0; i < 12; ++i) {
+            float v = s_acc[0][i];
+            bool is_min = (i % 6) < 3;
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = is_min ? fminf(v, s_acc[w][i]) : fmaxf(v, s_acc[w][i]);
+            r[i] = v;
+        }
+        flush_bounds(&out[m_first], r);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Codes.
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t expand10(uint32_t x) {
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__device__ __forceinline__ unsigned long long deposit_bits(unsigned long long value, unsigned long long mask) {
+    unsigned long long out = 0;
+    while (mask) {
+        unsigned long long low = mask & (~mask + 1ull);
+        if (value & 1ull) out |= low;
+        value >>= 1;
+        mask &= mask - 1ull;
+    }
+    return out;
+}
+
+// One thread per mesh: Morton30 scales, or the EMC60 bit plan (60 positions MSB first, each to the
+// dimension x, y, z, size with the largest remaining extent, which is then halved).
+__global__ void code_params_kernel(const Bounds* __restrict__ bounds, int m, int code_type, CodeParams* out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    float cmin[3], cmax[3], bmin[3], bmax[3];
+    for (int a = 0; a < 3; ++a) {
+        cmin[a] = ordered_to_float(bounds[k].v[a]);
+        cmax[a] = ordered_to_float(bounds[k].v[3 + a]);
+        bmin[a] = ordered_to_float(bounds[k].v[6 + a]);
+        bmax[a] = ordered_to_float(bounds[k].v[9 + a]);
+    }
+    CodeParams p;
+    if (code_type == DIPL_CODE_MORTON30) {
+        for (int a = 0; a < 3; ++a) {
+            float ext = __fsub_rn(cmax[a], cmin[a]);
+            p.lo[a] = cmin[a];
+            p.s[a] = ext > 0.0f ? __fdiv_rn(1024.0f, ext) : 0.0f;
+            p.bits[a] = 10;
+            p.top[a] = 1023;
+            p.mask[a] = 0;
+        }
+        p.lo[3] = 0.0f, p.s[3] = 0.0f, p.bits[3] = 0, p.top[3] = 0, p.mask[3] = 0;
+    } else {
+        float dx = __fsub_rn(bmax[0], bmin[0]), dy = __fsub_rn(bmax[1], bmin[1]), dz = __fsub_rn(bmax[2], bmin[2]);
+        float diag = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+        float ext[4] = {__fsub_rn(cmax[0], cmin[0]), __fsub_rn(cmax[1], cmin[1]), __fsub_rn(cmax[2], cmin[2]), diag};
+        float e[4];
+        for (int a = 0; a < 4; ++a) {
+            e[a] = ext[a] > 0.0f ? ext[a] : 0.0f;
+            p.bits[a] = 0;
+            p.mask[a] = 0;
+        }
+        for (int pos = 59; pos >= 0; --pos) {
+            int best = 0;
+            for (int a = 1; a < 4; ++a)
+                if (e[a] > e[best]) best = a;
+            p.bits[best] += 1;
+            p.mask[best] |= 1ull << pos;
+            e[best] = __fmul_rn(e[best], 0.5f);
+        }
+        for (int a = 0; a < 4; ++a) {
+            float cells = ldexpf(1.0f, p.bits[a]);
+            p.lo[a] = a < 3 ? cmin[a] : 0.0f;
+            p.s[a] = (ext[a] > 0.0f && p.bits[a] > 0) ? __fdiv_rn(cells, ext[a]) : 0.0f;
+            p.top[a] = p.bits[a] >= 64 ? ~0ull : ((1ull << p.bits[a]) - 1ull);
+        }
+    }
+    out[k] = p;
+}
+
+__device__ __forceinline__ unsigned long long tri_code(const Tri& t, const CodeParams& p, int code_type) {
+    float3 c = centroid(t);
+    if (code_type == DIPL_CODE_MORTON30) {
+        float xs[3] = {c.x, c.y, c.z};
+        uint32_t q[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float x = __fmul_rn(__fsub_rn(xs[a], p.lo[a]), p.s[a]);
+            x = fminf(fmaxf(x, 0.0f), 1023.0f);
+            q[a] = (uint32_t)x;
+        }
+        return (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
+    }
+    float dx = __fsub_rn(fmaxf(fmaxf(t.a.x, t.b.x), t.c.x), fminf(fminf(t.a.x, t.b.x), t.c.x));
+    float dy = __fsub_rn(fmaxf(fmaxf(t.a.y, t.b.y), t.c.y), fminf(fminf(t.a.y, t.b.y), t.c.y));
+    float dz = __fsub_rn(fmaxf(fmaxf(t.a.z, t.b.z), t.c.z), fminf(fminf(t.a.z, t.b.z), t.c.z));
+    float xs[4] = {c.x, c.y, c.z,
+                   __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)))};
+    unsigned long long code = 0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        if (p.bits[a] == 0) continue;
+        float q = fmaxf(__fmul_rn(__fsub_rn(xs[a], p.lo[a]), p.s[a]), 0.0f);
+        unsigned long long qi = q < 1.8e19f ? (unsigned long long)q : p.top[a];
+        if (qi > p.top[a]) qi = p.top[a];
+        code |= deposit_bits(qi, p.mask[a]);
+    }
+    return code;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) codes_kernel(const MeshDesc* __restrict__ meshes,
+                                                    const long long* __restrict__ offsets, int m, long long n,
+                                                    const CodeParams* __restrict__ params, int code_type,
+                                                    int code_shift, int mesh_shift, K* __restrict__ keys) {
+    long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    int k = find_mesh(offsets, m, g);
+    const MeshDesc md = meshes[k];
+    Tri t = load_tri(md, g - md.first);
+    unsigned long long code = tri_code(t, params[k], code_type) >> code_shift;
+    if (mesh_shift > 0) code |= (unsigned long long)k << mesh_shift;
+    keys[g] = static_cast<K>(code);
+}
+
+// ------------------------------------------------------------------------------------------------
+// PLOC.
+//
+// Clusters live in two ping-pong buffers of float4 pairs: lo = (min xyz, node id bits),
+// hi = (max xyz, mesh index bits). Internal node k (creation order) stores children (left, right,
+// height, 0), lo = (min xyz, triangle count bits), hi = (max xyz, first sorted position bits); node id
+// of internal node k is num_leaves + k; parent[] maps every node id to its parent (-1 at roots).
+//
+// Nearest neighbour of cluster i: argmin over j in [i-r, i+r], j != i, same mesh, of the 64-bit key
+// (distance bits << 32) | (|i-j| << 2) | ((min(i,j) & 1) << 1) | (j > i). The key order restricts one
+// strict total order on unordered pairs (distance, gap, parity of the lower index, lower index), so a
+// mutual pair always exists while a mesh has two clusters, ties are deterministic, and runs of equal
+// distances (duplicate geometry) still pair up neighbour with neighbour instead of chaining.
+// ------------------------------------------------------------------------------------------------
+struct PlocParams {
+    float4* lo[2];
+    float4* hi[2];
+    int4* child;
+    float4* node_lo;
+    float4* node_hi;
+    int* parent;
+    unsigned long long* status[2];
+    PlocCtrl* ctrl;
+    uint32_t* err;
+    int num_leaves;
+    int num_meshes;
+    int radius;
+};
+
+template <int B>
+struct PlocSmem {
+    static constexpr int T = B * kPlocIpt;
+    static constexpr int W = T + 4 * kRadiusMax;
+    float lx[W], ly[W], lz[W], hx[W], hy[W], hz[W];
+    int node[W];
+    int seg[W];
+    int nn[T + 2 * kRadiusMax];
+    uint32_t warp_sum[B / 32];
+    unsigned long long prefix;
+    int ok;
+    int n, mbase;
+};
+
+__device__ __forceinline__ void node_info(const PlocParams& P, int id, int& count, int& pmin, int& height) {
+    if (id < P.num_leaves) {
+        count = 1, pmin = id, height = 0;
+    } else {
+        int k = id - P.num_leaves;
+        count = __float_as_int(P.node_lo[k].w);
+        pmin = __float_as_int(P.node_hi[k].w);
+        height = P.child[k].z;
+    }
+}
+
+template <int B>
+__device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int tiles, int n, int mbase, int parity) {
+    constexpr int T = PlocSmem<B>::T;
+    const int r = P.radius;
+    const int s0 = tile * T;
+    const int w0 = max(s0 - 2 * r, 0), w1 = min(s0 + T + 2 * r, n);
+    const float4* __restrict__ in_lo = P.lo[parity];
+    const float4* __restrict__ in_hi = P.hi[parity];
+    for (int i = threadIdx.x; i < w1 - w0; i += B) {
+        float4 a = in_lo[w0 + i], b = in_hi[w0 + i];
+        s.lx[i] = a.x, s.ly[i] = a.y, s.lz[i] = a.z;
+        s.hx[i] = b.x, s.hy[i] = b.y, s.hz[i] = b.z;
+        s.node[i] = __float_as_int(a.w);
+        s.seg[i] = __float_as_int(b.w);
+    }
+    if (threadIdx.x == 0) P.status[parity ^ 1][tile] = 0ull;  // ready for the next iteration
+    __syncthreads();
+
+    // ---- nearest neighbours of [q0, q1) -----------------------------------------------------------
+    const int q0 = max(s0 - r, 0), q1 = min(s0 + T + r, n);
+    for (int q = q0 + threadIdx.x; q < q1; q += B) {
+        const int qi = q - w0;
+        const float lx = s.lx[qi], ly = s.ly[qi], lz = s.lz[qi], hx = s.hx[qi], hy = s.hy[qi], hz = s.hz[qi];
+        const int sg = s.seg[qi];
+        unsigned long long best = ~0ull;
+        const int jlo = max(q - r, 0), jhi = min(q + r, n - 1);
+        for (int j = jlo; j <= jhi; ++j) {
+            if (j == q) continue;
+            const int ji = j - w0;
+            if (s.seg[ji] != sg) continue;
+            float d = ploc_distance(lx, ly, lz, hx, hy, hz, s.lx[ji], s.ly[ji], s.lz[ji], s.hx[ji], s.hy[ji], s.hz[ji]);
+            unsigned int gap = (unsigned int)abs(j - q);
+            unsigned int mn = (unsigned int)min(j, q);
+            unsigned long long key = ((unsigned long long)__float_as_uint(d) << 32) |
+                                     (unsigned long long)((gap << 2) | ((mn & 1u) << 1) | (j > q ? 1u : 0u));
+            best = key < best ? key : best;
+        }
+        int nj = -1;
+        if (best != ~0ull) {
+            uint32_t tie = (uint32_t)best;
+            int gap = (int)(tie >> 2);
+            nj = (tie & 1u) ? q + gap : q - gap;
+        }
+        s.nn[q - q0] = nj;
+    }
+    __syncthreads();
+
+    // ---- merge decisions (blocked: kPlocIpt consecutive positions per thread) ----------------------
+    const int ib = s0 + threadIdx.x * kPlocIpt;
+    uint32_t keep_bits = 0, merge_bits = 0;
+#pragma unroll
+    for (int k = 0; k < kPlocIpt; ++k) {
+        int i = ib + k;
+        if (i >= n) break;
+        int j = s.nn[i - q0];
+        bool mutual = j >= 0 && s.nn[j - q0] == i;
+        if (!(mutual && i > j)) keep_bits |= 1u << k;
+        if (mutual && i < j) merge_bits |= 1u << k;
+    }
+    const uint32_t mine = (uint32_t)__popc(keep_bits) | ((uint32_t)__popc(merge_bits) << 16);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s.warp_sum[warp] = x;
+    __syncthreads();
+    uint32_t woff = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < B / 32; ++w) {
+        uint32_t v = s.warp_sum[w];
+        if (w < warp) woff += v;
+        total += v;
+    }
+    const uint32_t excl = woff + x - mine;
+
+    // ---- decoupled look-back over tiles: (kept, merged) prefixes ----------------------------------
+    if (threadIdx.x == 0) {
+        const unsigned long long agg = ((unsigned long long)(total & 0xFFFFu) << 31) | (total >> 16);
+        unsigned long long* st = P.status[parity];
+        unsigned long long prefix = 0;
+        int ok = 1;
+        if (tile == 0) {
+            st_release_u64(&st[0], (2ull << 62) | agg);
+        } else {
+            st_release_u64(&st[tile], (1ull << 62) | agg);
+            int j = tile - 1;
+            uint32_t spins = 0;
+            while (j >= 0) {
+                unsigned long long w = ld_acquire_u64(&st[j]);
+                unsigned long long state = w >> 62;
+                if (state == 0ull) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(P.err, kErrTimeout);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                prefix += w & ((1ull << 62) - 1ull);
+                if (state == 2ull) break;
+                --j;
+            }
+            st_release_u64(&st[tile], (2ull << 62) | (prefix + agg));
+        }
+        s.prefix = prefix;
+        s.ok = ok;
+        if (tile == tiles - 1 && ok) {
+            unsigned long long inc = prefix + agg;
+            P.ctrl->n[parity ^ 1] = (uint32_t)(inc >> 31);
+            P.ctrl->merges[parity ^ 1] = (uint32_t)mbase + (uint32_t)(inc & 0x7FFFFFFFull);
+        }
+    }
+    __syncthreads();
+    if (!s.ok) return;
+    const uint32_t kept_before = (uint32_t)(s.prefix >> 31);
+    const uint32_t merged_before = (uint32_t)(s.prefix & 0x7FFFFFFFull);
+
+    // ---- write surviving clusters and new nodes ----------------------------------------------------
+    float4* __restrict__ out_lo = P.lo[parity ^ 1];
+    float4* __restrict__ out_hi = P.hi[parity ^ 1];
+    uint32_t kpos = kept_before + (excl & 0xFFFFu);
+    uint32_t mpos = (uint32_t)mbase + merged_before + (excl >> 16);
+    const int max_internal = P.num_leaves - P.num_meshes;
+#pragma unroll
+    for (int k = 0; k < kPlocIpt; ++k) {
+        if (!((keep_bits >> k) & 1u)) continue;
+        const int i = ib + k, ii = i - w0;
+        float lx = s.lx[ii], ly = s.ly[ii], lz = s.lz[ii], hx = s.hx[ii], hy = s.hy[ii], hz = s.hz[ii];
+        int node = s.node[ii];
+        if ((merge_bits >> k) & 1u) {
+            const int j = s.nn[i - q0], ji = j - w0;
+            lx = fminf(lx, s.lx[ji]), ly = fminf(ly, s.ly[ji]), lz = fminf(lz, s.lz[ji]);
+            hx = fmaxf(hx, s.hx[ji]), hy = fmaxf(hy, s.hy[ji]), hz = fmaxf(hz, s.hz[ji]);
+            const int left = node, right = s.node[ji];
+            const int knew = (int)mpos++;
+            if (knew >= max_internal) {
+                atomicOr(P.err, kErrIterations);
+                continue;
+            }
+            int cl, pl, hl, cr, pr, hr;
+            node_info(P, left, cl, pl, hl);
+            node_info(P, right, cr, pr, hr);
+            node = P.num_leaves + knew;
+            P.child[knew] = make_int4(left, right, max(hl, hr) + 1, 0);
+            P.node_lo[knew] = make_float4(lx, ly, lz, __int_as_float(cl + cr));
+            P.node_hi[knew] = make_float4(hx, hy, hz, __int_as_float(min(pl, pr)));
+            P.parent[left] = node;
+            P.parent[right] = node;
+        }
+        if (kpos < (uint32_t)P.num_leaves) {
+            out_lo[kpos] = make_float4(lx, ly, lz, __int_as_float(node));
+            out_hi[kpos] = make_float4(hx, hy, hz, __int_as_float(s.seg[ii]));
+        }
+        ++kpos;
+    }
+}
+
+// Every PLOC iteration in one cooperative launch. Iterations are separated by a grid barrier; once a
+// single tile is left, block 0 finishes alone with block barriers.
+template <int B>
+__global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    PlocSmem<B>& s = *reinterpret_cast<PlocSmem<B>*>(s_raw);
+    constexpr int T = PlocSmem<B>::T;
+    bool solo = false;
+    uint32_t iter = 0;
+    for (;;) {
+        const int parity = iter & 1;
+        if (threadIdx.x == 0) {
+            s.n = (int)ld_acquire_u32(&P.ctrl->n[parity]);
+            s.mbase = (int)ld_acquire_u32(&P.ctrl->merges[parity]);
+            s.ok = ld_acquire_u32(P.err) == 0u;
+        }
+        __syncthreads();
+        const int n = s.n, mbase = s.mbase;
+        const bool ok = s.ok != 0;
+        __syncthreads();
+        if (!ok || n <= P.num_meshes) break;
+        if (iter >= kMaxPlocIterations) {
+            if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+            break;
+        }
+        const int tiles = (n + T - 1) / T;
+        if (tiles == 1 && !solo) {
+            if (blockIdx.x != 0) break;
+            solo = true;
+        }
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+            ploc_tile<B>(P, s, t, tiles, n, mbase, parity);
+            __syncthreads();
+        }
+        if (solo) {
+            __threadfence();
+            __syncthreads();
+        } else if (!grid_barrier(&P.ctrl->barrier, P.err)) {
+            break;
+        }
+        ++iter;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.ctrl->iterations = iter;
+}
+
+__global__ void ploc_init_kernel(const MeshDesc* __restrict__ meshes, const long long* __restrict__ offsets, int m,
+                                 long long n, const uint32_t* __restrict__ perm, float4* __restrict__ lo,
+                                 float4* __restrict__ hi, int* __restrict__ parent) {
+    long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    long long g = perm[p];
+    int k = find_mesh(offsets, m, g);
+    Tri t = load_tri(meshes[k], g - meshes[k].first);
+    float3 a, b;
+    tri_box(t, a, b);
+    lo[p] = make_float4(a.x, a.y, a.z, __int_as_float((int)p));
+    hi[p] = make_float4(b.x, b.y, b.z, __int_as_float(k));
+    parent[p] = -1;
+}
+
+__global__ void fill_int_kernel(int* p, long long n, int v) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Layout: a node with fewer than L triangles is a leaf (the reference's rule, sbvh.cc:273-276);
+// inner nodes are numbered in reverse creation order (every root first, children after parents);
+// each leaf's triangles go to one contiguous range, ranges ordered by the leaf's first sorted position.
+// ------------------------------------------------------------------------------------------------
+struct LayoutParams {
+    const int4* child;
+    const float4* node_lo;
+    const float4* node_hi;
+    const int* parent;
+    int num_leaves;
+    int num_inner;
+    int L;
+};
+
+__device__ __forceinline__ int node_count(const LayoutParams& P, int id) {
+    return id < P.num_leaves ? 1 : __float_as_int(P.node_lo[id - P.num_leaves].w);
+}
+__device__ __forceinline__ int node_pmin(const LayoutParams& P, int id) {
+    return id < P.num_leaves ? id : __float_as_int(P.node_hi[id - P.num_leaves].w);
+}
+
+__global__ void inner_flags_kernel(LayoutParams P, uint32_t* __restrict__ rev_flags, const uint32_t* err) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.num_inner) return;
+    uint32_t f = (*err == 0u) && __float_as_int(P.node_lo[k].w) >= P.L ? 1u : 0u;
+    rev_flags[P.num_inner - 1 - k] = f;
+}
+
+__global__ void leaf_owner_kernel(LayoutParams P, uint32_t* __restrict__ contrib, int* __restrict__ owner_leaf,
+                                  const uint32_t* err) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.num_leaves) return;
+    if (*err != 0u) {
+        contrib[p] = 0;
+        owner_leaf[p] = -1;
+        return;
+    }
+    int x = p;
+    for (int guard = 0; guard < 64; ++guard) {
+        int par = P.parent[x];
+        if (par < 0 || node_count(P, par) >= P.L) break;
+        x = par;
+    }
+    bool own = node_pmin(P, x) == p;
+    contrib[p] = own ? (uint32_t)node_count(P, x) : 0u;
+    owner_leaf[p] = own ? x : -1;
+    (void)contrib;
+}
+
+__device__ __forceinline__ void write_tri(const MeshDesc* meshes, const long long* offsets, int m,
+                                          const uint32_t* perm, int pos, float4* tris, int slot) {
+    long long g = perm[pos];
+    int k = find_mesh(offsets, m, g);
+    long long local = g - meshes[k].first;
+    Tri t = load_tri(meshes[k], local);
+    tris[3 * (long long)slot + 0] = make_float4(t.a.x, t.a.y, t.a.z, __int_as_float((int)local));
+    tris[3 * (long long)slot + 1] = make_float4(t.b.x, t.b.y, t.b.z, 0.0f);
+    tris[3 * (long long)slot + 2] = make_float4(t.c.x, t.c.y, t.c.z, 0.0f);
+}
+
+__global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
+                                  const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
+                                  const uint32_t* __restrict__ starts, const int* __restrict__ owner_leaf,
+                                  int* __restrict__ leaf_start_of, float4* __restrict__ tris, const uint32_t* err) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.num_leaves || *err != 0u) return;
+    int x = owner_leaf[p];
+    if (x < 0) return;
+    int start = (int)starts[p];
+    leaf_start_of[x] = start;
+    int stack[16];
+    int sp = 0, slot = start;
+    stack[sp++] = x;
+    while (sp > 0) {
+        int y = stack[--sp];
+        if (y < P.num_leaves) {
+            write_tri(meshes, offsets, m, perm, y, tris, slot++);
+        } else if (sp + 2 <= 16) {
+            int4 c = P.child[y - P.num_leaves];
+            stack[sp++] = c.y;  // right after left
+            stack[sp++] = c.x;
+        }
+    }
+}
+
+__device__ __forceinline__ float pad_down(float lo, float hi) {
+    float m = fmaxf(fabsf(lo), fabsf(hi));
+    return lo - (m * 9.5367431640625e-07f + 1e-30f);  // 2^-20 of the magnitude
+}
+__device__ __forceinline__ float pad_up(float lo, float hi) {
+    float m = fmaxf(fabsf(lo), fabsf(hi));
+    return hi + (m * 9.5367431640625e-07f + 1e-30f);
+}
+
+__device__ __forceinline__ double box_area(float3 lo, float3 hi) {
+    double dx = (double)hi.x - lo.x, dy = (double)hi.y - lo.y, dz = (double)hi.z - lo.z;
+    return 2.0 * (dx * dy + dy * dz + dz * dx);
+}
+
+__device__ __forceinline__ void child_box(const LayoutParams& P, const MeshDesc* meshes, const long long* offsets,
+                                          int m, const uint32_t* perm, int id, float3& lo, float3& hi) {
+    if (id < P.num_leaves) {
+        long long g = perm[id];
+        int k = find_mesh(offsets, m, g);
+        Tri t = load_tri(meshes[k], g - meshes[k].first);
+        tri_box(t, lo, hi);
+    } else {
+        float4 a = P.node_lo[id - P.num_leaves], b = P.node_hi[id - P.num_leaves];
+        lo = make_float3(a.x, a.y, a.z);
+        hi = make_float3(b.x, b.y, b.z);
+    }
+}
+
+__global__ void node_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
+                                  const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
+                                  const uint32_t* __restrict__ rev_index, const int* __restrict__ leaf_start_of,
+                                  BNode* __restrict__ nodes, double* __restrict__ sah, const uint32_t* err) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.num_inner || *err != 0u) return;
+    if (__float_as_int(P.node_lo[k].w) < P.L) return;
+    const int f = (int)rev_index[P.num_inner - 1 - k];
+    const int4 c = P.child[k];
+    float3 lo[2], hi[2];
+    int ref[2];
+    double acc = box_area(make_float3(P.node_lo[k].x, P.node_lo[k].y, P.node_lo[k].z),
+                          make_float3(P.node_hi[k].x, P.node_hi[k].y, P.node_hi[k].z));
+    for (int s = 0; s < 2; ++s) {
+        int id = s == 0 ? c.x : c.y;
+        child_box(P, meshes, offsets, m, perm, id, lo[s], hi[s]);
+        int cnt = node_count(P, id);
+        if (cnt >= P.L) {
+            ref[s] = (int)rev_index[P.num_inner - 1 - (id - P.num_leaves)];
+        } else {
+            ref[s] = make_leaf_ref(leaf_start_of[id], cnt);
+            acc += box_area(lo[s], hi[s]) * cnt;
+        }
+    }
+    BNode nd;
+    nd.a = make_float4(pad_down(lo[0].x, hi[0].x), pad_up(lo[0].x, hi[0].x), pad_down(lo[0].y, hi[0].y),
+                       pad_up(lo[0].y, hi[0].y));
+    nd.b = make_float4(pad_down(lo[1].x, hi[1].x), pad_up(lo[1].x, hi[1].x), pad_down(lo[1].y, hi[1].y),
+                       pad_up(lo[1].y, hi[1].y));
+    nd.c = make_float4(pad_down(lo[0].z, hi[0].z), pad_up(lo[0].z, hi[0].z), pad_down(lo[1].z, hi[1].z),
+                       pad_up(lo[1].z, hi[1].z));
+    nd.d = make_int4(ref[0], ref[1], 0, 0);
+    nodes[f] = nd;
+    int mesh = find_mesh(offsets, m, (long long)perm[__float_as_int(P.node_hi[k].w)]);
+    atomicAdd(&sah[2 * mesh], acc);
+    atomicAdd(&sah[2 * mesh + 1], 1.0);
+}
+
+// Roots of every mesh: the final clusters (one per mesh, in mesh order).
+struct RootInfo {
+    int root_ref;
+    int depth;
+    int num_leaves;
+    int pad;
+    double root_area;
+    double leaf_cost;  // SAH cost contribution when the root itself is a leaf
+};
+
+__global__ void roots_kernel(LayoutParams P, const float4* __restrict__ lo0, const float4* __restrict__ hi0,
+                             const float4* __restrict__ lo1, const float4* __restrict__ hi1, const PlocCtrl* ctrl,
+                             int m, const uint32_t* __restrict__ rev_index, const int* __restrict__ leaf_start_of,
+                             RootInfo* __restrict__ roots, const uint32_t* err) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    RootInfo ri{};
+    if (*err != 0u) {
+        roots[k] = ri;
+        return;
+    }
+    const bool odd = (ctrl->iterations & 1u) != 0u;
+    const float4* final_lo = odd ? lo1 : lo0;
+    const float4* final_hi = odd ? hi1 : hi0;
+    int id = __float_as_int(final_lo[k].w);
+    int cnt = node_count(P, id);
+    float3 lo = make_float3(final_lo[k].x, final_lo[k].y, final_lo[k].z);
+    float3 hi = make_float3(final_hi[k].x, final_hi[k].y, final_hi[k].z);
+    ri.root_area = box_area(lo, hi);
+    if (cnt >= P.L) {
+        ri.root_ref = (int)rev_index[P.num_inner - 1 - (id - P.num_leaves)];
+        ri.depth = P.child[id - P.num_leaves].z;
+    } else {
+        ri.root_ref = make_leaf_ref(leaf_start_of[id], cnt);
+        ri.depth = id < P.num_leaves ? 0 : P.child[id - P.num_leaves].z;
+        ri.leaf_cost = ri.root_area * cnt;
+    }
+    ri.num_leaves = cnt;
+    roots[k] = ri;
+}
+
+int ploc_block_for(int requested) {
+    if (requested == 128 || requested == 256 || requested == 512) return requested;
+    return 256;
+}
+
+template <int B>
+dipl_status launch_ploc(const PlocParams& P, int initial_tiles, cudaStream_t stream) {
+    const size_t smem = sizeof(PlocSmem<B>);
+    DIPL_CUDA(cudaFuncSetAttribute(ploc_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 0, per_sm = 0;
+    DIPL_CUDA(cudaGetDevice(&dev));
+    DIPL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    DIPL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ploc_kernel<B>, B, smem));
+    if (per_sm < 1) {
+        set_last_error("PLOC kernel cannot be resident");
+        return DIPL_ERR_CUDA;
+    }
+    int grid = std::max(1, std::min(initial_tiles, sms * per_sm));
+    void* args[] = {const_cast<PlocParams*>(&P)};
+    DIPL_CUDA(cudaLaunchCooperativeKernel((const void*)ploc_kernel<B>, dim3(grid), dim3(B), args, smem, stream));
+    note_launches();
+    return DIPL_OK;
+}
+
+inline unsigned blocks_for(long long n, int threads) { return (unsigned)std::max<long long>(1, (n + threads - 1) / threads); }
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// Host orchestration.
+// ------------------------------------------------------------------------------------------------
+static dipl_status validate_desc(const dipl_build_desc& d) {
+    DIPL_CHECK_ARG(d.num_triangles >= 0 && d.num_triangles < (1ll << 27), "num_triangles must be in [0, 2^27)");
+    DIPL_CHECK_ARG(d.num_triangles == 0 || (d.d_v0 && d.d_v1 && d.d_v2), "vertex arrays must be non-NULL");
+    DIPL_CHECK_ARG(d.code_type == DIPL_CODE_MORTON30 || d.code_type == DIPL_CODE_EMC60, "bad code_type");
+    DIPL_CHECK_ARG(d.bv_type == DIPL_BV_AABB || d.bv_type == DIPL_BV_SOBB, "bad bv_type");
+    DIPL_CHECK_ARG(d.layout == DIPL_LAYOUT_BINARY || d.layout == DIPL_LAYOUT_WIDE8_Q8, "bad layout");
+    DIPL_CHECK_ARG(d.max_triangles_per_leaf >= 2 && d.max_triangles_per_leaf <= 8,
+                   "max_triangles_per_leaf must be in [2, 8]");
+    DIPL_CHECK_ARG(d.nn_search_radius >= 1 && d.nn_search_radius <= kRadiusMax, "nn_search_radius must be in [1, 32]");
+    DIPL_CHECK_ARG(d.kdop_size >= 6 && d.kdop_size <= 32 && d.kdop_size % 2 == 0, "kdop_size must be even, 6..32");
+    DIPL_CHECK_ARG(d.ploc_block_size == 0 || d.ploc_block_size == 128 || d.ploc_block_size == 256 ||
+                       d.ploc_block_size == 512,
+                   "ploc_block_size must be 0, 128, 256 or 512");
+    if (d.bv_type != DIPL_BV_AABB || d.layout != DIPL_LAYOUT_BINARY) {
+        set_last_error("SOBB and 8-wide layouts are not available in this build");
+        return DIPL_ERR_UNSUPPORTED;
+    }
+    DIPL_CHECK_ARG(d.sort_digit_bits == 0 || d.sort_digit_bits == 6 || d.sort_digit_bits == 7 ||
+                       d.sort_digit_bits == 8 || d.sort_digit_bits == 10,
+                   "sort_digit_bits must be 0, 6, 7, 8 or 10");
+    return DIPL_OK;
+}
+
+dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** out, cudaStream_t stream) {
+    DIPL_CHECK_ARG(descs && out && count >= 1, "descs/out must be non-NULL and count >= 1");
+    for (int i = 0; i < count; ++i) {
+        dipl_status st = validate_desc(descs[i]);
+        if (st != DIPL_OK) return st;
+        out[i] = nullptr;
+    }
+    const dipl_build_desc& d0 = descs[0];
+    for (int i = 1; i < count; ++i) {
+        DIPL_CHECK_ARG(descs[i].code_type == d0.code_type && descs[i].bv_type == d0.bv_type &&
+                           descs[i].layout == d0.layout && descs[i].max_triangles_per_leaf == d0.max_triangles_per_leaf &&
+                           descs[i].nn_search_radius == d0.nn_search_radius && descs[i].kdop_size == d0.kdop_size,
+                       "batched builds need one set of build options");
+    }
+    // Meshes with triangles take part in the pipeline; empty meshes get empty handles.
+    std::vector<MeshDesc> meshes;
+    std::vector<long long> offsets;
+    std::vector<int> mesh_of_desc(count, -1);
+    long long total = 0;
+    for (int i = 0; i < count; ++i) {
+        if (descs[i].num_triangles == 0) continue;
+        mesh_of_desc[i] = (int)meshes.size();
+        meshes.push_back(MeshDesc{descs[i].d_v0, descs[i].d_v1, descs[i].d_v2, total, descs[i].num_triangles});
+        offsets.push_back(total);
+        total += descs[i].num_triangles;
+    }
+    DIPL_CHECK_ARG(total < (1ll << 27), "total triangles of a build must be < 2^27");
+    const int m = (int)meshes.size();
+    offsets.push_back(total);
+
+    auto storage = std::make_shared<Storage>();
+    storage->stream = stream;
+    uint32_t* d_err = nullptr;
+    dipl_status st = storage->alloc(&d_err, 4);
+    if (st != DIPL_OK) return st;
+    DIPL_CUDA(cudaMemsetAsync(d_err, 0, 4, stream));
+
+    auto make_handle = [&](int i) {
+        auto* h = new dipl_bvh();
+        h->storage = storage;
+        h->num_triangles = descs[i].num_triangles;
+        h->code_type = descs[i].code_type;
+        h->bv_type = descs[i].bv_type;
+        h->layout = descs[i].layout;
+        h->max_leaf = descs[i].max_triangles_per_leaf;
+        h->radius = descs[i].nn_search_radius;
+        h->kdop = descs[i].kdop_size;
+        h->d_err = d_err;
+        h->root = 0;
+        return h;
+    };
+
+    if (m == 0) {
+        for (int i = 0; i < count; ++i) out[i] = make_handle(i);
+        return DIPL_OK;
+    }
+
+    const long long N = total;
+    const long long K = N - m;  // internal nodes
+    const int L = d0.max_triangles_per_leaf;
+    ScratchArena scratch(stream);
+
+    MeshDesc* d_meshes;
+    long long* d_offsets;
+    Bounds* d_bounds;
+    CodeParams* d_params;
+    if ((st = scratch.alloc(&d_meshes, m)) != DIPL_OK || (st = scratch.alloc(&d_offsets, m + 1)) != DIPL_OK ||
+        (st = scratch.alloc(&d_bounds, m)) != DIPL_OK || (st = scratch.alloc(&d_params, m)) != DIPL_OK)
+        return st;
+    DIPL_CUDA(cudaMemcpyAsync(d_meshes, meshes.data(), sizeof(MeshDesc) * m, cudaMemcpyHostToDevice, stream));
+    DIPL_CUDA(cudaMemcpyAsync(d_offsets, offsets.data(), sizeof(long long) * (m + 1), cudaMemcpyHostToDevice, stream));
+
+    // ---- bounds + code parameters ------------------------------------------------------------------
+    bounds_init_kernel<<<blocks_for(m, 128), 128, 0, stream>>>(d_bounds, m); note_launches();
+    {
+        long long grid = std::min<long long>((N + 1023) / 1024, 148 * 16);
+        grid = std::max<long long>(grid, 1);
+        long long chunk = (N + grid - 1) / grid;
+        bounds_kernel<<<(unsigned)grid, 256, 0, stream>>>(d_meshes, d_offsets, m, N, chunk, d_bounds); note_launches();
+    }
+    code_params_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(d_bounds, m, d0.code_type, d_params); note_launches();
+    DIPL_CUDA(cudaGetLastError());
+
+    // ---- codes + sort --------------------------------------------------------------------------------
+    const int code_bits = d0.code_type == DIPL_CODE_MORTON30 ? 30 : 60;
+    int mesh_bits = 0;
+    while ((1ll << mesh_bits) < m) ++mesh_bits;
+    int key_bits = code_bits + mesh_bits, code_shift = 0;
+    if (key_bits > 64) {
+        code_shift = key_bits - 64;
+        key_bits = 64;
+    }
+    const int mesh_shift = mesh_bits > 0 ? code_bits - code_shift : 0;
+    const int key_bytes = key_bits <= 32 ? 4 : 8;
+    const int digit_bits = d0.sort_digit_bits > 0 ? d0.sort_digit_bits : 8;
+    void *keys, *keys_sorted, *keys_alt;
+    uint32_t *perm, *perm_alt;
+    unsigned char* sort_scratch;
+    if ((st = scratch.alloc((unsigned char**)&keys, N * key_bytes)) != DIPL_OK ||
+        (st = scratch.alloc((unsigned char**)&keys_sorted, N * key_bytes)) != DIPL_OK ||
+        (st = scratch.alloc((unsigned char**)&keys_alt, N * key_bytes)) != DIPL_OK ||
+        (st = storage->alloc(&perm, N)) != DIPL_OK || (st = scratch.alloc(&perm_alt, N)) != DIPL_OK ||
+        (st = scratch.alloc(&sort_scratch, radix_sort_scratch_bytes(N, 0, key_bits, digit_bits))) != DIPL_OK)
+        return st;
+    if (key_bytes == 4)
+        codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, m, N, d_params,
+                                                                       d0.code_type, code_shift, mesh_shift,
+                                                                       (uint32_t*)keys);
+    else
+        codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
+            d_meshes, d_offsets, m, N, d_params, d0.code_type, code_shift, mesh_shift, (unsigned long long*)keys); note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    st = radix_sort_pairs(keys, nullptr, keys_sorted, perm, keys_alt, perm_alt, N, key_bytes, 0, key_bits, digit_bits,
+                          sort_scratch, stream, d_err);
+    if (st != DIPL_OK) return st;
+
+    // ---- PLOC ------------------------------------------------------------------------------------------
+    const int B = ploc_block_for(d0.ploc_block_size);
+    const int T = B * kPlocIpt;
+    const int tiles0 = (int)((N + T - 1) / T);
+    PlocParams P{};
+    PlocCtrl* d_ctrl;
+    int4* child;
+    float4 *nlo, *nhi;
+    int* parent;
+    unsigned long long* status;
+    float4 *c_lo0, *c_hi0, *c_lo1, *c_hi1;
+    const long long Kalloc = std::max<long long>(K, 1);
+    if ((st = scratch.alloc(&d_ctrl, 1)) != DIPL_OK || (st = storage->alloc(&child, Kalloc)) != DIPL_OK ||
+        (st = storage->alloc(&nlo, Kalloc)) != DIPL_OK || (st = storage->alloc(&nhi, Kalloc)) != DIPL_OK ||
+        (st = scratch.alloc(&parent, N + Kalloc)) != DIPL_OK || (st = scratch.alloc(&status, 2 * tiles0 + 2)) != DIPL_OK ||
+        (st = scratch.alloc(&c_lo0, N)) != DIPL_OK || (st = scratch.alloc(&c_hi0, N)) != DIPL_OK ||
+        (st = scratch.alloc(&c_lo1, N)) != DIPL_OK || (st = scratch.alloc(&c_hi1, N)) != DIPL_OK)
+        return st;
+    PlocCtrl hctrl{};
+    hctrl.n[0] = (uint32_t)N;
+    hctrl.merges[0] = 0;
+    DIPL_CUDA(cudaMemcpyAsync(d_ctrl, &hctrl, sizeof(PlocCtrl), cudaMemcpyHostToDevice, stream));
+    DIPL_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (2 * tiles0 + 2), stream));
+    fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(parent, N + K, -1); note_launches();
+    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, m, N, perm, c_lo0, c_hi0, parent); note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    P.lo[0] = c_lo0, P.hi[0] = c_hi0, P.lo[1] = c_lo1, P.hi[1] = c_hi1;
+    P.child = child, P.node_lo = nlo, P.node_hi = nhi, P.parent = parent;
+    P.status[0] = status, P.status[1] = status + tiles0 + 1;
+    P.ctrl = d_ctrl, P.err = d_err;
+    P.num_leaves = (int)N, P.num_meshes = m, P.radius = d0.nn_search_radius;
+    if (N > m) {
+        switch (B) {
+            case 128: st = launch_ploc<128>(P, tiles0, stream); break;
+            case 512: st = launch_ploc<512>(P, tiles0, stream); break;
+            default: st = launch_ploc<256>(P, tiles0, stream); break;
+        }
+        if (st != DIPL_OK) return st;
+    }
+
+    // ---- layout -------------------------------------------------------------------------------------
+    LayoutParams LP{child, nlo, nhi, parent, (int)N, (int)K, L};
+    uint32_t *rev_flags, *contrib;
+    int *owner_leaf, *leaf_start_of;
+    unsigned char* scan_scratch;
+    uint32_t* d_counts;  // [0] = inner nodes of the layout
+    BNode* nodes;
+    float4* tris;
+    double* d_sah;
+    RootInfo* d_roots;
+    if ((st = scratch.alloc(&rev_flags, Kalloc)) != DIPL_OK || (st = scratch.alloc(&contrib, N)) != DIPL_OK ||
+        (st = scratch.alloc(&owner_leaf, N)) != DIPL_OK || (st = scratch.alloc(&leaf_start_of, N + Kalloc)) != DIPL_OK ||
+        (st = scratch.alloc(&scan_scratch, scan_scratch_bytes(std::max(N, Kalloc)))) != DIPL_OK ||
+        (st = scratch.alloc(&d_counts, 4)) != DIPL_OK || (st = storage->alloc(&nodes, Kalloc)) != DIPL_OK ||
+        (st = storage->alloc(&tris, 3 * N)) != DIPL_OK || (st = scratch.alloc(&d_sah, 2 * m)) != DIPL_OK ||
+        (st = scratch.alloc(&d_roots, m)) != DIPL_OK)
+        return st;
+    DIPL_CUDA(cudaMemsetAsync(d_sah, 0, sizeof(double) * 2 * m, stream));
+    DIPL_CUDA(cudaMemsetAsync(d_counts, 0, 16, stream));
+    if (K > 0) {
+        inner_flags_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, rev_flags, d_err); note_launches();
+        if ((st = exclusive_scan_u32(rev_flags, rev_flags, K, d_counts, scan_scratch, stream, d_err)) != DIPL_OK)
+            return st;
+    }
+    leaf_owner_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, contrib, owner_leaf, d_err); note_launches();
+    if ((st = exclusive_scan_u32(contrib, contrib, N, nullptr, scan_scratch, stream, d_err)) != DIPL_OK) return st;
+    leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, d_meshes, d_offsets, m, perm, contrib, owner_leaf,
+                                                               leaf_start_of, tris, d_err); note_launches();
+    if (K > 0) {
+        node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, d_meshes, d_offsets, m, perm, rev_flags,
+                                                                   leaf_start_of, nodes, d_sah, d_err);
+        note_launches();
+    }
+    roots_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(LP, c_lo0, c_hi0, c_lo1, c_hi1, d_ctrl, m, rev_flags,
+                                                       leaf_start_of, d_roots, d_err); note_launches();
+    DIPL_CUDA(cudaGetLastError());
+
+    // ---- read back the per-mesh summary (the one host synchronisation of a build) -------------------
+    const size_t summary_bytes = sizeof(RootInfo) * m + sizeof(double) * 2 * m + 16;
+    unsigned char* host = pinned_host_buffer(summary_bytes);
+    if (!host) {
+        set_last_error("pinned host allocation failed");
+        return DIPL_ERR_OUT_OF_MEMORY;
+    }
+    RootInfo* h_roots = reinterpret_cast<RootInfo*>(host);
+    double* h_sah = reinterpret_cast<double*>(host + sizeof(RootInfo) * m);
+    uint32_t* h_tail = reinterpret_cast<uint32_t*>(host + sizeof(RootInfo) * m + sizeof(double) * 2 * m);
+    DIPL_CUDA(cudaMemcpyAsync(h_roots, d_roots, sizeof(RootInfo) * m, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_sah, d_sah, sizeof(double) * 2 * m, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_tail, d_counts, 4, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_tail + 1, &d_ctrl->iterations, 4, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_tail + 2, d_err, 4, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaStreamSynchronize(stream));
+    const uint32_t err = h_tail[2];
+    if (err != 0u) {
+        set_last_error(err & kErrTimeout ? "build: a bounded device wait timed out"
+                                         : "build: clustering did not converge");
+        return (err & kErrTimeout) ? DIPL_ERR_TIMEOUT : DIPL_ERR_INTERNAL;
+    }
+    const int64_t inner_total = (int64_t)h_tail[0];
+    const int iterations = (int)h_tail[1];
+
+    std::vector<dipl_bvh*> made;
+    for (int i = 0; i < count; ++i) {
+        dipl_bvh* h = make_handle(i);
+        h->nodes = nodes;
+        h->tris = tris;
+        h->perm = reinterpret_cast<int32_t*>(perm);
+        h->children = child;
+        h->node_lo = nlo;
+        h->node_hi = nhi;
+        h->batch_leaves = N;
+        h->node_capacity = inner_total;
+        h->ploc_iterations = iterations;
+        const int k = mesh_of_desc[i];
+        if (k >= 0) {
+            const RootInfo& ri = h_roots[k];
+            h->root = ri.root_ref;
+            h->depth = ri.depth;
+            h->leaf_base = offsets[k];
+            h->num_nodes = (int64_t)h_sah[2 * k + 1];
+            h->sah_area = ri.root_area;
+            h->sah_sum = h_sah[2 * k] + ri.leaf_cost;
+            h->num_leaves = 0;
+        }
+        out[i] = h;
+        made.push_back(h);
+    }
+    return DIPL_OK;
+}
+
+}  // namespace dipl
+
+namespace dipl {
+
+// Codes of one mesh, as the build computes them (without mesh bits).
+dipl_status compute_codes(const dipl_build_desc* desc, void* d_codes, cudaStream_t stream) {
+    DIPL_CHECK_ARG(desc != nullptr, "desc must be non-NULL");
+    dipl_status st = validate_desc(*desc);
+    if (st != DIPL_OK) return st;
+    const long long N = desc->num_triangles;
+    if (N == 0) return DIPL_OK;
+    DIPL_CHECK_ARG(d_codes != nullptr, "codes must be non-NULL");
+    ScratchArena scratch(stream);
+    MeshDesc md{desc->d_v0, desc->d_v1, desc->d_v2, 0, N};
+    long long offs[2] = {0, N};
+    MeshDesc* d_meshes;
+    long long* d_offsets;
+    Bounds* d_bounds;
+    CodeParams* d_params;
+    if ((st = scratch.alloc(&d_meshes, 1)) != DIPL_OK || (st = scratch.alloc(&d_offsets, 2)) != DIPL_OK ||
+        (st = scratch.alloc(&d_bounds, 1)) != DIPL_OK || (st = scratch.alloc(&d_params, 1)) != DIPL_OK)
+        return st;
+    DIPL_CUDA(cudaMemcpyAsync(d_meshes, &md, sizeof(md), cudaMemcpyHostToDevice, stream));
+    DIPL_CUDA(cudaMemcpyAsync(d_offsets, offs, sizeof(offs), cudaMemcpyHostToDevice, stream));
+    bounds_init_kernel<<<1, 32, 0, stream>>>(d_bounds, 1); note_launches();
+    long long grid = std::max<long long>(1, std::min<long long>((N + 1023) / 1024, 148 * 16));
+    long long chunk = (N + grid - 1) / grid;
+    bounds_kernel<<<(unsigned)grid, 256, 0, stream>>>(d_meshes, d_offsets, 1, N, chunk, d_bounds); note_launches();
+    code_params_kernel<<<1, 32, 0, stream>>>(d_bounds, 1, desc->code_type, d_params); note_launches();
+    if (desc->code_type == DIPL_CODE_MORTON30)
+        codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, 1, N, d_params,
+                                                                       desc->code_type, 0, 0, (uint32_t*)d_codes);
+    else
+        codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
+            d_meshes, d_offsets, 1, N, d_params, desc->code_type, 0, 0, (unsigned long long*)d_codes); note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    // keep the scratch alive until the kernels ran (frees are stream-ordered)
+    return DIPL_OK;
+}
+
+}  // namespace dipl

@@ -1,0 +1,218 @@
+/*
+ * dipl_bvh.h — C ABI of the B200 BVH build-and-trace engine (libdipl_bvh.so, sm_100a).
+ *
+ * The engine stands behind the reference's acceleration-structure boundary:
+ *   AccelerationStructure::Build(config, stats, span<const Triangle>)   src/acceleration/acceleration_structure.h:15-16
+ *   AccelerationStructure::Intersect(stats, ray, ray_hit, backface)     src/acceleration/acceleration_structure.h:17
+ *   AccelerationStructure::IntersectAny(stats, ray, backface)           src/acceleration/acceleration_structure.h:18
+ * and replaces the brute-force device loops DummyIntersect / DummyIntersectAny
+ * (src/gpu/renderer/gpu_renderer_util.h:29-94) behind the GPU frontend. The reference's GPU side has no
+ * C ABI (namespace diplodocus::cuda_kernels, src/gpu/renderer/gpu_renderer_api.h:8-11); this header is
+ * the batch-oriented C replacement: a scene in, a BVH handle out; a ray batch in, hit records out.
+ *
+ * Conventions
+ *  - Every pointer argument named d_* or documented as "device" is a CUDA device pointer; the rest are
+ *    host pointers. `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *  - Every call returns a dipl_status; nothing aborts. dipl_last_error() gives a message for the
+ *    calling thread's most recent failure. There is no CPU fallback: without a usable sm_100 device
+ *    every entry point that touches the GPU returns DIPL_ERR_CUDA.
+ *  - Calls are asynchronous on `stream` unless documented otherwise. A BVH handle is immutable after
+ *    its build completes, so concurrent traces on one handle (any streams) are safe once the build
+ *    has been ordered before them.
+ */
+#ifndef DIPL_BVH_H_
+#define DIPL_BVH_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DIPL_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define DIPL_API __attribute__((visibility("default")))
+#else
+#define DIPL_API
+#endif
+
+typedef enum dipl_status {
+    DIPL_OK = 0,
+    DIPL_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size or enum value */
+    DIPL_ERR_CUDA = 2,             /* a CUDA runtime call failed (no device, launch failure, ...) */
+    DIPL_ERR_OUT_OF_MEMORY = 3,    /* a device allocation failed */
+    DIPL_ERR_TIMEOUT = 4,          /* a bounded device-side wait (look-back, grid barrier) gave up */
+    DIPL_ERR_INTERNAL = 5,         /* a device-side consistency check failed (e.g. traversal stack) */
+    DIPL_ERR_UNSUPPORTED = 6       /* a valid option this build does not provide */
+} dipl_status;
+
+/* Code used to order primitives before clustering.
+ * Mirrors MortonType (src/gpu/config/gpu_acceleration_structure_config.h:5). */
+typedef enum dipl_code_type { DIPL_CODE_MORTON30 = 0, DIPL_CODE_EMC60 = 1 } dipl_code_type;
+
+/* Bounding volume of the nodes. Mirrors BoundingVolumeType (gpu_acceleration_structure_config.h:7). */
+typedef enum dipl_bv_type { DIPL_BV_AABB = 0, DIPL_BV_SOBB = 1 } dipl_bv_type;
+
+/* Node layout used by traces. BINARY: two FP32 child boxes per 64-byte node (80 bytes with SOBB).
+ * WIDE8_Q8: 8-wide nodes with 8-bit conservatively quantised child bounds (80 bytes), FP32 leaf re-test. */
+typedef enum dipl_layout { DIPL_LAYOUT_BINARY = 0, DIPL_LAYOUT_WIDE8_Q8 = 1 } dipl_layout;
+
+/* Leaf test. REF_MT reproduces Triangle::IntersectRay (src/scene/triangle.cc:10-43) bit for bit
+ * (|det| < 1e-6 cull, no FMA, IEEE divide). WATERTIGHT is Woop, Benthin & Wald (2013). */
+typedef enum dipl_leaf_test { DIPL_LEAF_REF_MT = 0, DIPL_LEAF_WATERTIGHT = 1 } dipl_leaf_test;
+
+/* Trace flags. BACKFACE_CULLING has the reference's meaning (triangle.cc:18-21): with it, a triangle
+ * is hit only when e1 . (dir x e2) > 0. */
+#define DIPL_TRACE_BACKFACE_CULLING 1u
+
+/* Build description. The three vertex arrays are the reference GPU scene's SoA positions
+ * tri_v0_pos / tri_v1_pos / tri_v2_pos (src/gpu/scene/gpu_scene.h:18-20): float3 per triangle,
+ * i.e. 3 floats with a 12-byte stride, DEVICE memory. The engine keeps no pointer to them after the
+ * build returns (it copies what traces need), unlike SBvh, which keeps a span (sbvh.h:33). */
+typedef struct dipl_build_desc {
+    const float* d_v0;
+    const float* d_v1;
+    const float* d_v2;
+    int64_t num_triangles;
+    int32_t code_type;              /* dipl_code_type */
+    int32_t bv_type;                /* dipl_bv_type */
+    int32_t layout;                 /* dipl_layout */
+    int32_t max_triangles_per_leaf; /* a node with fewer triangles than this is a leaf (reference
+                                       meaning, sbvh.cc:273-276); 2..8, default 4 */
+    int32_t nn_search_radius;       /* PLOC radius r, 1..32 (GpuAccelerationStructureConfig::nn_search_radius) */
+    int32_t kdop_size;              /* SOBB direction set: kdop_size/2 directions, 6..32 (kdop_size) */
+    int32_t ploc_block_size;        /* PLOC threads per block: 0 = auto, else 128, 256 or 512 */
+    int32_t sort_digit_bits;        /* radix sort digit width: 0 = auto (8), else 6, 7, 8 or 10 */
+} dipl_build_desc;
+
+/* A ray: origin, hit interval lower bound, direction, upper bound (32 bytes). A hit needs
+ * tmin < t < tmax. The reference's Ray (src/scene/ray.h:7-11) has origin, dir and t_max and always
+ * uses tmin = kEpsilon = 1e-6 (sbvh.cc:85); pass tmin = 1e-6f to reproduce it. */
+typedef struct dipl_ray {
+    float ox, oy, oz, tmin;
+    float dx, dy, dz, tmax;
+} dipl_ray;
+
+/* A closest-hit record (16 bytes): the reference RayHit's triangle_id, t, b1 and b2
+ * (src/scene/ray_hit.h:8-17; b0 = 1 - u - v). A miss is prim = -1, t = +inf, u = v = 0. */
+typedef struct dipl_hit {
+    int32_t prim;
+    float t, u, v;
+} dipl_hit;
+
+typedef struct dipl_bvh dipl_bvh; /* opaque, owns its device memory */
+
+typedef struct dipl_bvh_info {
+    int64_t num_triangles;
+    int64_t num_inner_nodes;     /* nodes of the traced layout */
+    int64_t num_leaves;
+    int64_t node_bytes;          /* bytes of the traced node array */
+    int64_t triangle_bytes;      /* bytes of the leaf triangle array */
+    int32_t depth;               /* levels of the PLOC tree (bounds the traversal stack) */
+    int32_t ploc_iterations;
+    int32_t code_type, bv_type, layout, max_triangles_per_leaf, nn_search_radius, kdop_size;
+} dipl_bvh_info;
+
+/* Fills a description with the defaults (Morton30, AABB, binary, leaves < 4, r = 16, 32-DOP, auto). */
+DIPL_API void dipl_build_desc_init(dipl_build_desc* desc);
+
+/* Builds a BVH over desc->num_triangles triangles (0 is allowed: every ray misses).
+ * Replaces AccelerationStructure::Build (acceleration_structure.h:15-16) / SBvh::Build (sbvh.cc:17-58).
+ * The work is queued on `stream`; the call returns once the BVH is complete (it reads back the roots,
+ * depth and SAH sums, the build's one host synchronisation), so, like SBvh::Build, the result is ready
+ * when it returns. Device memory is released in stream order on `stream` by dipl_bvh_destroy, so that
+ * stream must outlive the handle. */
+DIPL_API dipl_status dipl_bvh_build(const dipl_build_desc* desc, dipl_bvh** out, void* stream);
+
+/* Builds `count` independent BVHs in one pipeline: one persistent clustering launch for all meshes
+ * (their clusters never merge across meshes). out[i] is an ordinary handle for descs[i]; all descs must
+ * share the build options. Returns when complete, like dipl_bvh_build. */
+DIPL_API dipl_status dipl_bvh_build_batched(const dipl_build_desc* descs, int32_t count, dipl_bvh** out, void* stream);
+
+/* Closest hit for n rays (device arrays of dipl_ray / dipl_hit). Replaces
+ * AccelerationStructure::Intersect (acceleration_structure.h:17; SBvh::Intersect sbvh.cc:60-145) and the
+ * device brute force DummyIntersect (gpu_renderer_util.h:29-72). Exact-t ties resolve to the lowest
+ * primitive id, like DummyAccelerationStucture::Intersect (dummy_acceleration_structure.cc:21-64). */
+DIPL_API dipl_status dipl_bvh_trace_closest(const dipl_bvh* bvh, const dipl_ray* d_rays, int64_t n, dipl_hit* d_hits,
+                                   int32_t leaf_test, uint32_t flags, void* stream);
+
+/* As dipl_bvh_trace_closest, also adding the node visits and triangle tests of the batch to
+ * d_counters[0] and d_counters[1] (device, 2 x uint64). The counts mirror AccelerationStats'
+ * traversal_count / intersection_count (src/stats/acceleration_stats.h:14-16) in 64 bits. */
+DIPL_API dipl_status dipl_bvh_trace_closest_counted(const dipl_bvh* bvh, const dipl_ray* d_rays, int64_t n, dipl_hit* d_hits,
+                                           int32_t leaf_test, uint32_t flags, uint64_t* d_counters, void* stream);
+
+/* Any hit (occlusion) for n rays: d_occluded[i] = 1 if some triangle has tmin < t < tmax.
+ * Replaces AccelerationStructure::IntersectAny (acceleration_structure.h:18; SBvh::IntersectAny
+ * sbvh.cc:147-191) and DummyIntersectAny (gpu_renderer_util.h:74-94). */
+DIPL_API dipl_status dipl_bvh_trace_any(const dipl_bvh* bvh, const dipl_ray* d_rays, int64_t n, uint8_t* d_occluded,
+                               int32_t leaf_test, uint32_t flags, void* stream);
+
+/* SAH cost C = [sum over inner nodes SA(n) + sum over leaves SA(n) |n|] / SA(root), C_t = C_i = 1,
+ * summed in FP64 on the device over the traced layout. Synchronises `stream`. */
+DIPL_API dipl_status dipl_bvh_sah_cost(const dipl_bvh* bvh, double* cost, void* stream);
+
+DIPL_API dipl_status dipl_bvh_get_info(const dipl_bvh* bvh, dipl_bvh_info* info);
+
+/* Copies the clustering result to HOST buffers (any may be NULL): h_perm[num_triangles] = triangle id at
+ * each sorted-code position (leaf node id = position); h_children[2*(num_triangles-1)] = left/right node
+ * ids of internal node k in creation order (id num_triangles + k); h_boxes[6*(num_triangles-1)] = its box
+ * (lo xyz, hi xyz). Synchronises `stream`. For checking and debugging. */
+DIPL_API dipl_status dipl_bvh_download_topology(const dipl_bvh* bvh, int32_t* h_perm, int32_t* h_children, float* h_boxes,
+                                       void* stream);
+
+/* Copies the traced node array and leaf triangle array to HOST memory (sizes from dipl_bvh_info),
+ * and the root reference (>= 0: node index; < 0: ~(first_triangle << 3 | count) leaf). Synchronises. */
+DIPL_API dipl_status dipl_bvh_download_layout(const dipl_bvh* bvh, void* h_nodes, void* h_triangles, int32_t* h_root,
+                                     void* stream);
+
+/* Synchronises `stream` and reports device-side failures recorded by earlier traces on this handle
+ * (a traversal stack or step limit hit: DIPL_ERR_INTERNAL), then clears them. Traces never fault on
+ * such a failure; they finish the ray with what they have and record it here. */
+DIPL_API dipl_status dipl_bvh_check_errors(const dipl_bvh* bvh, void* stream);
+
+/* Releases the handle's device memory in stream order on its build stream. NULL is a no-op. */
+DIPL_API dipl_status dipl_bvh_destroy(dipl_bvh* bvh);
+
+/* ---- building blocks exported for tests and callers that need them on their own ---------------- */
+
+/* Codes of the build (Morton30 in the low 30 bits of uint32, or EMC60 in the low 60 bits of uint64)
+ * for the triangles of desc (uses d_v0/d_v1/d_v2, num_triangles, code_type). d_codes is device memory
+ * of num_triangles uint32 (MORTON30) or uint64 (EMC60). */
+DIPL_API dipl_status dipl_compute_codes(const dipl_build_desc* desc, void* d_codes, void* stream);
+
+/* Stable LSD radix sort of (key, value) pairs on bits [begin_bit, end_bit) of the keys. Keys are uint32
+ * (key_bytes = 4) or uint64 (key_bytes = 8); values uint32. d_vals_in may be NULL (values 0..n-1).
+ * Input and output arrays must not overlap. */
+DIPL_API dipl_status dipl_radix_sort_pairs(const void* d_keys_in, const uint32_t* d_vals_in, void* d_keys_out,
+                                  uint32_t* d_vals_out, int64_t n, int32_t key_bytes, int32_t begin_bit,
+                                  int32_t end_bit, int32_t digit_bits, void* stream);
+
+/* FP64 oracle re-intersection (checking only): for each hit, t/u/v of the ray against triangle `prim`
+ * of the original vertex arrays, in double precision (d_tuv: 3 doubles per ray; misses give +inf,0,0). */
+DIPL_API dipl_status dipl_reintersect_f64(const float* d_v0, const float* d_v1, const float* d_v2, const dipl_ray* d_rays,
+                                 const dipl_hit* d_hits, int64_t n, double* d_tuv, void* stream);
+
+/* Adjoint of the closest-hit t/u/v (differentiation form). Given the forward hits and upstream
+ * gradients d_dtuv (3 floats per ray: dL/dt, dL/du, dL/dv), ADDS dL/dvertex into d_dv0/d_dv1/d_dv2
+ * (float3 per triangle, like the vertex arrays; atomically) and WRITES dL/dorigin and dL/ddirection
+ * (float3 per ray) into d_dorig / d_ddir (either may be NULL). Hit ids are held fixed (visibility is
+ * discrete); misses contribute nothing. */
+DIPL_API dipl_status dipl_trace_adjoint(const float* d_v0, const float* d_v1, const float* d_v2, const dipl_ray* d_rays,
+                               const dipl_hit* d_hits, const float* d_dtuv, int64_t n, float* d_dv0, float* d_dv1,
+                               float* d_dv2, float* d_dorig, float* d_ddir, void* stream);
+
+DIPL_API const char* dipl_status_string(dipl_status status);
+/* Message of the calling thread's most recent failure ("" if none). */
+DIPL_API const char* dipl_last_error(void);
+DIPL_API int32_t dipl_abi_version(void);
+/* Number of CUDA kernels this library has launched in the process so far (all entry points). */
+DIPL_API uint64_t dipl_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIPL_BVH_H_ */

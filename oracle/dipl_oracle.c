@@ -1,0 +1,551 @@
+/*
+ * TEST INFRASTRUCTURE — CHECKER ONLY. Never linked into, or called by, the product library;
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ *
+ * Plain-C restatement of the BVH build-and-trace path, used as the oracle for the CUDA kernels
+ * in diplodocus_b200/csrc. Compile with -ffp-contract=off (oracle/Makefile) so every float
+ * operation rounds exactly as written, like the reference's own CPU build (CMakeLists.txt:9-11).
+ *
+ * What each part restates:
+ *  - orc_mt: the reference Moller-Trumbore test, Triangle::IntersectRay (src/scene/triangle.cc:10-43),
+ *    operation for operation (plain mul/add, IEEE divide, |det| < 1e-6 cull, b1/b2 range tests).
+ *  - orc_brute_closest: DummyAccelerationStucture::Intersect
+ *    (src/acceleration/dummy_acceleration_structure.cc:21-64): ascending ids, accept t > 1e-6 && t < t_hit,
+ *    so exact-t ties go to the lowest id. The same loop runs with the watertight test.
+ *  - orc_brute_any: DummyAccelerationStucture::IntersectAny (dummy_acceleration_structure.cc:66-79).
+ *  - orc_wt: watertight ray/triangle test of Woop, Benthin and Wald (JCGT 2013), FP32 with the
+ *    paper's FP64 recomputation of zero edge functions. Absent from the reference.
+ *  - orc_morton30 / orc_emc60: this project's Morton and extended-Morton codes (absent from the
+ *    reference; README.md:14-16 names Vinkler et al. 2017 for EMC).
+ *  - orc_ploc: this project's PLOC (Meister & Bittner 2017) merge loop with its deterministic
+ *    tie rule, restated sequentially so the device topology can be compared bit for bit.
+ *  - orc_intersect_f64 / orc_brute_closest_f64: FP64 re-intersection used as the error oracle.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+#include <unistd.h>
+
+/* ------------------------------------------------------------------------------------------ */
+/* Minimal parallel-for over [0, n) with pthreads (static contiguous chunks).                   */
+/* ------------------------------------------------------------------------------------------ */
+typedef void (*orc_range_fn)(void* ctx, int64_t begin, int64_t end);
+typedef struct {
+    orc_range_fn fn;
+    void* ctx;
+    int64_t b, e;
+} orc_job;
+
+static void* orc_job_run(void* p) {
+    orc_job* j = (orc_job*)p;
+    j->fn(j->ctx, j->b, j->e);
+    return NULL;
+}
+
+static int orc_threads = 0;
+void orc_set_threads(int n) { orc_threads = n; }
+
+static void orc_parallel_for(int64_t n, orc_range_fn fn, void* ctx) {
+    int nt = orc_threads > 0 ? orc_threads : (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (nt < 1) nt = 1;
+    if (nt > 256) nt = 256;
+    if (n < 4 * nt) nt = 1;
+    if (nt == 1) {
+        fn(ctx, 0, n);
+        return;
+    }
+    pthread_t th[256];
+    orc_job jobs[256];
+    int64_t chunk = (n + nt - 1) / nt;
+    int launched = 0;
+    for (int k = 0; k < nt; ++k) {
+        int64_t b = k * chunk, e = b + chunk < n ? b + chunk : n;
+        if (b >= e) break;
+        jobs[k].fn = fn;
+        jobs[k].ctx = ctx;
+        jobs[k].b = b;
+        jobs[k].e = e;
+        pthread_create(&th[k], NULL, orc_job_run, &jobs[k]);
+        ++launched;
+    }
+    for (int k = 0; k < launched; ++k) pthread_join(th[k], NULL);
+}
+
+#define ORC_EPS 1e-6f                 /* kEpsilon, src/util/util.h:15 */
+#define ORC_INF 3.40282346638528859812e+38F /* kInfinity = FLT_MAX, src/util/util.h:16 */
+
+/* ------------------------------------------------------------------------------------------ */
+/* Reference Moller-Trumbore (triangle.cc:10-43).                                               */
+/* ------------------------------------------------------------------------------------------ */
+float orc_mt(const float* a, const float* b, const float* c, const float* o, const float* d, int backface,
+             float* b1_out, float* b2_out) {
+    float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
+    float e2x = c[0] - a[0], e2y = c[1] - a[1], e2z = c[2] - a[2];
+    /* pvec = Cross(dir, e2) (vec3.h:119-121) */
+    float px = d[1] * e2z - d[2] * e2y;
+    float py = d[2] * e2x - d[0] * e2z;
+    float pz = d[0] * e2y - d[1] * e2x;
+    /* det = Dot(e1, pvec) = (x*x + y*y) + z*z (vec3.h:118) */
+    float det = e1x * px + e1y * py + e1z * pz;
+    if (backface) {
+        if (det < ORC_EPS) return ORC_INF;
+    } else {
+        if (fabsf(det) < ORC_EPS) return ORC_INF;
+    }
+    float inv = 1.0f / det;
+    float tx = o[0] - a[0], ty = o[1] - a[1], tz = o[2] - a[2];
+    float b1 = (tx * px + ty * py + tz * pz) * inv;
+    if (b1 < 0.0f || b1 > 1.0f) return ORC_INF;
+    /* qvec = Cross(tvec, e1) */
+    float qx = ty * e1z - tz * e1y;
+    float qy = tz * e1x - tx * e1z;
+    float qz = tx * e1y - ty * e1x;
+    float b2 = (d[0] * qx + d[1] * qy + d[2] * qz) * inv;
+    if (b2 < 0.0f || b1 + b2 > 1.0f) return ORC_INF;
+    float t = (e2x * qx + e2y * qy + e2z * qz) * inv;
+    *b1_out = b1;
+    *b2_out = b2;
+    return t;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Watertight test (Woop, Benthin, Wald 2013). Returns t, or ORC_INF on a miss.                 */
+/* Backface culling keeps the reference's meaning: a hit needs e1.(d x e2) > 0 (triangle.cc:18). */
+/* ------------------------------------------------------------------------------------------ */
+float orc_wt(const float* v0, const float* v1, const float* v2, const float* o, const float* d, int backface,
+             float* b1_out, float* b2_out) {
+    float ax = fabsf(d[0]), ay = fabsf(d[1]), az = fabsf(d[2]);
+    int kz = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    if (d[kz] < 0.0f) { int tmp = kx; kx = ky; ky = tmp; }
+    float sx = d[kx] / d[kz];
+    float sy = d[ky] / d[kz];
+    float sz = 1.0f / d[kz];
+    float A[3] = {v0[0] - o[0], v0[1] - o[1], v0[2] - o[2]};
+    float B[3] = {v1[0] - o[0], v1[1] - o[1], v1[2] - o[2]};
+    float C[3] = {v2[0] - o[0], v2[1] - o[1], v2[2] - o[2]};
+    float Ax = A[kx] - sx * A[kz], Ay = A[ky] - sy * A[kz];
+    float Bx = B[kx] - sx * B[kz], By = B[ky] - sy * B[kz];
+    float Cx = C[kx] - sx * C[kz], Cy = C[ky] - sy * C[kz];
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return ORC_INF;
+    float det = U + V + W;
+    if (det == 0.0f) return ORC_INF;
+    if (backface) {
+        /* front face: e1.(d x e2) > 0, which is det > 0 in the sheared frame */
+        if (det < 0.0f) return ORC_INF;
+    }
+    float Az = sz * A[kz], Bz = sz * B[kz], Cz = sz * C[kz];
+    float T = U * Az + V * Bz + W * Cz;
+    float rcp = 1.0f / det;
+    *b1_out = V * rcp;
+    *b2_out = W * rcp;
+    return T * rcp;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Brute force closest / any hit.                                                               */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct {
+    const float *tris, *rays;
+    int64_t n;
+    int leaf_test, backface;
+    int32_t* prim;
+    float *t, *u, *v;
+    uint8_t* occ;
+} orc_brute_ctx;
+
+static void brute_closest_range(void* p, int64_t rb, int64_t re) {
+    orc_brute_ctx* c = (orc_brute_ctx*)p;
+    for (int64_t r = rb; r < re; ++r) {
+        const float* ray = c->rays + 8 * r;
+        float tmin = ray[3];
+        float t_hit = ray[7];
+        int32_t best = -1;
+        float bu = 0.0f, bv = 0.0f;
+        for (int64_t i = 0; i < c->n; ++i) {
+            const float* q = c->tris + 9 * i;
+            float b1 = 0.0f, b2 = 0.0f;
+            float t = c->leaf_test ? orc_wt(q, q + 3, q + 6, ray, ray + 4, c->backface, &b1, &b2)
+                                   : orc_mt(q, q + 3, q + 6, ray, ray + 4, c->backface, &b1, &b2);
+            /* t == ORC_INF is the tests' miss value; it never hits, also when tmax is +inf */
+            if (t > tmin && t < t_hit && t < ORC_INF) {
+                t_hit = t;
+                best = (int32_t)i;
+                bu = b1;
+                bv = b2;
+            }
+        }
+        c->prim[r] = best;
+        c->t[r] = best >= 0 ? t_hit : INFINITY;
+        c->u[r] = best >= 0 ? bu : 0.0f;
+        c->v[r] = best >= 0 ? bv : 0.0f;
+    }
+}
+
+void orc_brute_closest(const float* tris, int64_t n, const float* rays, int64_t nr, int leaf_test, int backface,
+                       int32_t* prim, float* t_out, float* u_out, float* v_out) {
+    orc_brute_ctx c = {tris, rays, n, leaf_test, backface, prim, t_out, u_out, v_out, NULL};
+    orc_parallel_for(nr, brute_closest_range, &c);
+}
+
+static void brute_any_range(void* p, int64_t rb, int64_t re) {
+    orc_brute_ctx* c = (orc_brute_ctx*)p;
+    for (int64_t r = rb; r < re; ++r) {
+        const float* ray = c->rays + 8 * r;
+        uint8_t hit = 0;
+        for (int64_t i = 0; i < c->n && !hit; ++i) {
+            const float* q = c->tris + 9 * i;
+            float b1, b2;
+            float t = c->leaf_test ? orc_wt(q, q + 3, q + 6, ray, ray + 4, c->backface, &b1, &b2)
+                                   : orc_mt(q, q + 3, q + 6, ray, ray + 4, c->backface, &b1, &b2);
+            if (t > ray[3] && t < ray[7] && t < ORC_INF) hit = 1;
+        }
+        c->occ[r] = hit;
+    }
+}
+
+void orc_brute_any(const float* tris, int64_t n, const float* rays, int64_t nr, int leaf_test, int backface,
+                   uint8_t* occluded) {
+    orc_brute_ctx c = {tris, rays, n, leaf_test, backface, NULL, NULL, NULL, NULL, occluded};
+    orc_parallel_for(nr, brute_any_range, &c);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* FP64 oracle: intersection of each ray with a given triangle (Cramer's rule in double), and   */
+/* an FP64 closest hit (no epsilon cull; inclusive edges) for classifying disagreements.        */
+/* ------------------------------------------------------------------------------------------ */
+static int f64_hit(const float* p, const float* ray, double* t, double* u, double* v) {
+    double a[3] = {p[0], p[1], p[2]};
+    double e1[3] = {(double)p[3] - a[0], (double)p[4] - a[1], (double)p[5] - a[2]};
+    double e2[3] = {(double)p[6] - a[0], (double)p[7] - a[1], (double)p[8] - a[2]};
+    double d[3] = {ray[4], ray[5], ray[6]};
+    double s[3] = {(double)ray[0] - a[0], (double)ray[1] - a[1], (double)ray[2] - a[2]};
+    double pv[3] = {d[1] * e2[2] - d[2] * e2[1], d[2] * e2[0] - d[0] * e2[2], d[0] * e2[1] - d[1] * e2[0]};
+    double det = e1[0] * pv[0] + e1[1] * pv[1] + e1[2] * pv[2];
+    if (det == 0.0) return 0;
+    double inv = 1.0 / det;
+    double uu = (s[0] * pv[0] + s[1] * pv[1] + s[2] * pv[2]) * inv;
+    double q[3] = {s[1] * e1[2] - s[2] * e1[1], s[2] * e1[0] - s[0] * e1[2], s[0] * e1[1] - s[1] * e1[0]};
+    double vv = (d[0] * q[0] + d[1] * q[1] + d[2] * q[2]) * inv;
+    double tt = (e2[0] * q[0] + e2[1] * q[1] + e2[2] * q[2]) * inv;
+    *t = tt;
+    *u = uu;
+    *v = vv;
+    return (uu >= 0.0 && vv >= 0.0 && uu + vv <= 1.0) ? 1 : 0;
+}
+
+typedef struct {
+    const float *tris, *rays;
+    int64_t n;
+    const int32_t* prim_in;
+    int32_t* prim_out;
+    double *t, *u, *v;
+} orc_f64_ctx;
+
+static void isect_f64_range(void* p, int64_t rb, int64_t re) {
+    orc_f64_ctx* c = (orc_f64_ctx*)p;
+    for (int64_t r = rb; r < re; ++r) {
+        if (c->prim_in[r] < 0) {
+            c->t[r] = INFINITY;
+            c->u[r] = c->v[r] = 0.0;
+            continue;
+        }
+        f64_hit(c->tris + 9 * (int64_t)c->prim_in[r], c->rays + 8 * r, &c->t[r], &c->u[r], &c->v[r]);
+    }
+}
+
+void orc_intersect_f64(const float* tris, const float* rays, int64_t nr, const int32_t* prim, double* t, double* u,
+                       double* v) {
+    orc_f64_ctx c = {tris, rays, 0, prim, NULL, t, u, v};
+    orc_parallel_for(nr, isect_f64_range, &c);
+}
+
+static void brute_f64_range(void* p, int64_t rb, int64_t re) {
+    orc_f64_ctx* c = (orc_f64_ctx*)p;
+    for (int64_t r = rb; r < re; ++r) {
+        const float* ray = c->rays + 8 * r;
+        double best_t = ray[7];
+        int32_t best = -1;
+        for (int64_t i = 0; i < c->n; ++i) {
+            double t, u, v;
+            if (f64_hit(c->tris + 9 * i, ray, &t, &u, &v) && t > (double)ray[3] && t < best_t) {
+                best_t = t;
+                best = (int32_t)i;
+            }
+        }
+        c->prim_out[r] = best;
+        c->t[r] = best >= 0 ? best_t : INFINITY;
+    }
+}
+
+void orc_brute_closest_f64(const float* tris, int64_t n, const float* rays, int64_t nr, int32_t* prim,
+                           double* t_out) {
+    orc_f64_ctx c = {tris, rays, n, NULL, prim, t_out, NULL, NULL};
+    orc_parallel_for(nr, brute_f64_range, &c);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Scene bounds, centroids and codes.                                                           */
+/* Centroid = (v0 + v1 + v2) / 3 evaluated as ((v0 + v1) + v2) / 3.0f, the reference's          */
+/* CalculateTriangleCentroid (src/scene/triangle.h:36).                                          */
+/* ------------------------------------------------------------------------------------------ */
+static inline void centroid(const float* p, float* c) {
+    for (int a = 0; a < 3; ++a) c[a] = ((p[a] + p[3 + a]) + p[6 + a]) / 3.0f;
+}
+
+void orc_scene_bounds(const float* tris, int64_t n, float* cmin, float* cmax, float* bmin, float* bmax) {
+    for (int a = 0; a < 3; ++a) {
+        cmin[a] = bmin[a] = INFINITY;
+        cmax[a] = bmax[a] = -INFINITY;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = tris + 9 * i;
+        float c[3];
+        centroid(p, c);
+        for (int a = 0; a < 3; ++a) {
+            cmin[a] = fminf(cmin[a], c[a]);
+            cmax[a] = fmaxf(cmax[a], c[a]);
+            for (int k = 0; k < 3; ++k) {
+                bmin[a] = fminf(bmin[a], p[3 * k + a]);
+                bmax[a] = fmaxf(bmax[a], p[3 * k + a]);
+            }
+        }
+    }
+}
+
+static inline uint32_t expand10(uint32_t x) {
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+/* 30-bit Morton code of the centroid in the centroid bounds: 10 bits per axis, x highest. */
+void orc_morton30(const float* tris, int64_t n, const float* cmin, const float* cmax, uint32_t* codes) {
+    float s[3];
+    for (int a = 0; a < 3; ++a) {
+        float ext = cmax[a] - cmin[a];
+        s[a] = ext > 0.0f ? 1024.0f / ext : 0.0f;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        float c[3];
+        centroid(tris + 9 * i, c);
+        uint32_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            float x = (c[a] - cmin[a]) * s[a];
+            x = fminf(fmaxf(x, 0.0f), 1023.0f);
+            q[a] = (uint32_t)x;
+        }
+        codes[i] = (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
+    }
+}
+
+/* EMC60 bit plan: 60 positions handed out MSB first, each to the dimension (x, y, z, size) with
+ * the largest remaining extent (first in that order on ties), which is then halved. Spatial
+ * extents are the centroid-bounds extents; the size dimension's extent is the scene-box diagonal. */
+void orc_emc60_plan(const float* cmin, const float* cmax, float diag, int* bits, uint64_t* masks) {
+    float e[4] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2], diag};
+    for (int a = 0; a < 4; ++a) {
+        bits[a] = 0;
+        masks[a] = 0;
+        if (!(e[a] > 0.0f)) e[a] = 0.0f;
+    }
+    for (int pos = 59; pos >= 0; --pos) {
+        int best = 0;
+        for (int a = 1; a < 4; ++a)
+            if (e[a] > e[best]) best = a;
+        bits[best] += 1;
+        masks[best] |= (uint64_t)1 << pos;
+        e[best] *= 0.5f;
+    }
+}
+
+static inline uint64_t deposit(uint64_t value, uint64_t mask) {
+    /* scatter the low bits of value into the set bits of mask, low to high */
+    uint64_t out = 0;
+    while (mask) {
+        uint64_t low = mask & (~mask + 1);
+        if (value & 1) out |= low;
+        value >>= 1;
+        mask &= mask - 1;
+    }
+    return out;
+}
+
+float orc_scene_diag(const float* bmin, const float* bmax) {
+    float dx = bmax[0] - bmin[0], dy = bmax[1] - bmin[1], dz = bmax[2] - bmin[2];
+    return sqrtf((dx * dx + dy * dy) + dz * dz);
+}
+
+void orc_emc60(const float* tris, int64_t n, const float* cmin, const float* cmax, float diag, uint64_t* codes) {
+    int bits[4];
+    uint64_t masks[4];
+    orc_emc60_plan(cmin, cmax, diag, bits, masks);
+    float lo[4] = {cmin[0], cmin[1], cmin[2], 0.0f};
+    float ext[4] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2], diag};
+    float s[4];
+    uint64_t top[4];
+    for (int a = 0; a < 4; ++a) {
+        float cells = ldexpf(1.0f, bits[a]);
+        s[a] = (ext[a] > 0.0f && bits[a] > 0) ? cells / ext[a] : 0.0f;
+        top[a] = bits[a] >= 64 ? ~(uint64_t)0 : (((uint64_t)1 << bits[a]) - 1);
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = tris + 9 * i;
+        float x[4];
+        centroid(p, x);
+        float dx = fmaxf(fmaxf(p[0], p[3]), p[6]) - fminf(fminf(p[0], p[3]), p[6]);
+        float dy = fmaxf(fmaxf(p[1], p[4]), p[7]) - fminf(fminf(p[1], p[4]), p[7]);
+        float dz = fmaxf(fmaxf(p[2], p[5]), p[8]) - fminf(fminf(p[2], p[5]), p[8]);
+        x[3] = sqrtf((dx * dx + dy * dy) + dz * dz);
+        uint64_t code = 0;
+        for (int a = 0; a < 4; ++a) {
+            if (bits[a] == 0) continue;
+            /* quantise: clamp below at 0 (NaN -> 0), truncate, clamp to the top cell in integers */
+            float q = fmaxf((x[a] - lo[a]) * s[a], 0.0f);
+            uint64_t qi = q < 1.8e19f ? (uint64_t)q : top[a];
+            if (qi > top[a]) qi = top[a];
+            code |= deposit(qi, masks[a]);
+        }
+        codes[i] = code;
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* PLOC (Meister & Bittner 2017) as built on the device, restated sequentially.                 */
+/*                                                                                              */
+/* Clusters start as the triangles in sorted-code order (leaf node id = sorted position).       */
+/* Each iteration: NN(i) = argmin over j in [i-r, i+r], j != i, same segment, of the key         */
+/* (d(i,j), |i-j|, min(i,j) & 1, j > i), d = dx*dy + dy*dz + dz*dx of the merged box            */
+/* (half its surface area), evaluated as fmaf(dx, dy, fmaf(dy, dz, dz*dx)); a NaN distance       */
+/* counts as +inf. Mutual pairs (NN(NN(i)) == i) merge: a new node (left = cluster i's node,     */
+/* right = cluster j's node) takes the lower position, the higher one is dropped, the rest keep  */
+/* their order. Internal node k (creation order: iteration, then position) has id n_leaves + k.  */
+/* Stops when one cluster per segment is left.                                                   */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct {
+    float lo[3], hi[3];
+    int32_t node, seg;
+} orc_cluster;
+
+static inline uint64_t ploc_key(const orc_cluster* a, const orc_cluster* b, int64_t i, int64_t j) {
+    float dx = fmaxf(a->hi[0], b->hi[0]) - fminf(a->lo[0], b->lo[0]);
+    float dy = fmaxf(a->hi[1], b->hi[1]) - fminf(a->lo[1], b->lo[1]);
+    float dz = fmaxf(a->hi[2], b->hi[2]) - fminf(a->lo[2], b->lo[2]);
+    float d = fmaf(dx, dy, fmaf(dy, dz, dz * dx));
+    uint32_t bits;
+    if (d != d) d = INFINITY;
+    memcpy(&bits, &d, 4);
+    uint64_t gap = (uint64_t)(j > i ? j - i : i - j);
+    uint64_t mn = (uint64_t)(j > i ? i : j);
+    uint64_t tie = (gap << 2) | ((mn & 1) << 1) | (uint64_t)(j > i ? 1 : 0);
+    return ((uint64_t)bits << 32) | tie;
+}
+
+/* perm: triangle id at each sorted position; seg: segment id per sorted position (NULL = one).
+ * Outputs: children[2k], children[2k+1]; boxes[6k..6k+5] = lo xyz, hi xyz of internal node k.
+ * Returns the number of internal nodes, or -1 on bad input. */
+int64_t orc_ploc(const float* tris, int64_t n, const int32_t* perm, const int32_t* seg, int64_t nseg, int radius,
+                 int32_t* children, float* boxes, int32_t* iterations) {
+    if (n <= 0 || radius < 1) return n == 0 ? 0 : -1;
+    orc_cluster* cur = (orc_cluster*)malloc(sizeof(orc_cluster) * (size_t)n);
+    orc_cluster* nxt = (orc_cluster*)malloc(sizeof(orc_cluster) * (size_t)n);
+    int64_t* nn = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = tris + 9 * (int64_t)perm[i];
+        for (int a = 0; a < 3; ++a) {
+            cur[i].lo[a] = fminf(fminf(p[a], p[3 + a]), p[6 + a]);
+            cur[i].hi[a] = fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]);
+        }
+        cur[i].node = (int32_t)i;
+        cur[i].seg = seg ? seg[i] : 0;
+    }
+    int64_t m = n, made = 0;
+    int32_t iters = 0;
+    while (m > nseg) {
+        for (int64_t i = 0; i < m; ++i) {
+            uint64_t best = ~(uint64_t)0;
+            int64_t bj = -1;
+            int64_t jlo = i - radius < 0 ? 0 : i - radius;
+            int64_t jhi = i + radius > m - 1 ? m - 1 : i + radius;
+            for (int64_t j = jlo; j <= jhi; ++j) {
+                if (j == i || cur[j].seg != cur[i].seg) continue;
+                uint64_t k = ploc_key(&cur[i], &cur[j], i, j);
+                if (k < best) {
+                    best = k;
+                    bj = j;
+                }
+            }
+            nn[i] = bj;
+        }
+        int64_t w = 0;
+        for (int64_t i = 0; i < m; ++i) {
+            int64_t j = nn[i];
+            int mutual = (j >= 0 && nn[j] == i);
+            if (mutual && i > j) continue; /* merged into the lower position */
+            if (mutual) {
+                orc_cluster c;
+                for (int a = 0; a < 3; ++a) {
+                    c.lo[a] = fminf(cur[i].lo[a], cur[j].lo[a]);
+                    c.hi[a] = fmaxf(cur[i].hi[a], cur[j].hi[a]);
+                }
+                children[2 * made] = cur[i].node;
+                children[2 * made + 1] = cur[j].node;
+                for (int a = 0; a < 3; ++a) {
+                    boxes[6 * made + a] = c.lo[a];
+                    boxes[6 * made + 3 + a] = c.hi[a];
+                }
+                c.node = (int32_t)(n + made);
+                c.seg = cur[i].seg;
+                ++made;
+                nxt[w++] = c;
+            } else {
+                nxt[w++] = cur[i];
+            }
+        }
+        if (w == m) break; /* no progress: cannot happen with a strict total order on pairs */
+        orc_cluster* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+        m = w;
+        ++iters;
+    }
+    if (iterations) *iterations = iters;
+    free(cur);
+    free(nxt);
+    free(nn);
+    return made;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Per-(ray, triangle) re-test: the leaf test of ray r against triangle prim[r] (miss -> t=INF). */
+/* ------------------------------------------------------------------------------------------ */
+void orc_test_pairs(const float* tris, const float* rays, int64_t nr, const int32_t* prim, int leaf_test,
+                    int backface, float* t_out, float* u_out, float* v_out) {
+    for (int64_t r = 0; r < nr; ++r) {
+        t_out[r] = INFINITY;
+        u_out[r] = v_out[r] = 0.0f;
+        if (prim[r] < 0) continue;
+        const float* q = tris + 9 * (int64_t)prim[r];
+        const float* ray = rays + 8 * r;
+        float b1 = 0.0f, b2 = 0.0f;
+        float t = leaf_test ? orc_wt(q, q + 3, q + 6, ray, ray + 4, backface, &b1, &b2)
+                            : orc_mt(q, q + 3, q + 6, ray, ray + 4, backface, &b1, &b2);
+        t_out[r] = t;
+        u_out[r] = b1;
+        v_out[r] = b2;
+    }
+}

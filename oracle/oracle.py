@@ -1,0 +1,282 @@
+"""TEST INFRASTRUCTURE — CHECKER ONLY.
+
+ctypes bindings for the two oracles:
+
+* ``RefOracle``  — the reference's own SBvh / brute force / Moller-Trumbore compiled from its
+  sources (oracle/_ref/libref_oracle.so, built by oracle/Makefile in a tree where the reference
+  is present; the built file then travels with the repository snapshot).
+* ``Oracle``     — the plain-C restatement in oracle/dipl_oracle.c (oracle/libdipl_oracle.so).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libref_oracle.so")
+ORC_LIB = os.path.join(HERE, "libdipl_oracle.so")
+REFERENCE_TREE = "/root/reference"
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+
+
+def build(force=False):
+    """Compile the C restatement always, and the reference harness when the reference tree is here."""
+    targets = ["libdipl_oracle.so"]
+    if os.path.isdir(REFERENCE_TREE):
+        targets.append("ref")
+    cmd = ["make", "-C", HERE] + (["-B"] if force else []) + targets
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+
+
+def _tris(t):
+    t = np.ascontiguousarray(t, dtype=np.float32)
+    assert t.ndim == 3 and t.shape[1:] == (3, 3), t.shape
+    return t
+
+
+def _rays(r):
+    r = np.ascontiguousarray(r, dtype=np.float32)
+    assert r.ndim == 2 and r.shape[1] == 8, r.shape
+    return r
+
+
+class Hits:
+    """Closest-hit records: prim (int32, -1 = miss), t, u (= b1), v (= b2)."""
+
+    def __init__(self, n):
+        self.prim = np.empty(n, np.int32)
+        self.t = np.empty(n, np.float32)
+        self.u = np.empty(n, np.float32)
+        self.v = np.empty(n, np.float32)
+
+
+class RefOracle:
+    """The reference's own code (SBvh, DummyAccelerationStucture, Triangle::IntersectRay)."""
+
+    def __init__(self, path=REF_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run make -C oracle ref where the reference tree exists)")
+        L = self.lib = C.CDLL(path)
+        L.ref_sbvh_build.restype = C.c_void_p
+        L.ref_sbvh_build.argtypes = [_f32p, C.c_int64, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+        L.ref_sbvh_rebuild.restype = C.c_double
+        L.ref_sbvh_rebuild.argtypes = [C.c_void_p]
+        L.ref_sbvh_destroy.argtypes = [C.c_void_p]
+        L.ref_sbvh_trace.argtypes = [C.c_void_p, _f32p, C.c_int64, _i32p, _f32p, _f32p, _f32p, C.c_int, C.c_int,
+                                     _i64p]
+        L.ref_sbvh_sah_cost.restype = C.c_double
+        L.ref_sbvh_sah_cost.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.ref_brute_trace.argtypes = [_f32p, C.c_int64, _f32p, C.c_int64, _i32p, _f32p, _f32p, _f32p, C.c_int,
+                                      C.c_int]
+        L.ref_intersect_one.restype = C.c_float
+        L.ref_intersect_one.argtypes = [_f32p, _f32p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+
+    def sbvh(self, tris, max_depth=32, max_triangles_per_leaf=4, bin_count=16):
+        return SBvh(self, _tris(tris), max_depth, max_triangles_per_leaf, bin_count)
+
+    def brute(self, tris, rays, backface=False, threads=None):
+        tris, rays = _tris(tris), _rays(rays)
+        h = Hits(len(rays))
+        self.lib.ref_brute_trace(tris, len(tris), rays, len(rays), h.prim, h.t, h.u, h.v, int(backface),
+                                 int(threads or os.cpu_count() or 1))
+        return h
+
+
+class SBvh:
+    def __init__(self, ref, tris, max_depth, max_leaf, bins):
+        self.ref, self.tris = ref, tris
+        ms = C.c_double(0.0)
+        self.h = ref.lib.ref_sbvh_build(tris, len(tris), max_depth, max_leaf, bins, C.byref(ms))
+        self.build_ms = ms.value
+
+    def rebuild_ms(self):
+        return self.ref.lib.ref_sbvh_rebuild(self.h)
+
+    def trace(self, rays, backface=False, threads=None):
+        rays = _rays(rays)
+        h = Hits(len(rays))
+        cnt = np.zeros(3, np.int64)
+        self.ref.lib.ref_sbvh_trace(self.h, rays, len(rays), h.prim, h.t, h.u, h.v, int(backface),
+                                    int(threads or os.cpu_count() or 1), cnt)
+        h.counters = cnt
+        return h
+
+    def sah_cost(self):
+        ni, nl = C.c_int64(0), C.c_int64(0)
+        c = self.ref.lib.ref_sbvh_sah_cost(self.h, C.byref(ni), C.byref(nl))
+        return c, ni.value, nl.value
+
+    def close(self):
+        if self.h:
+            self.ref.lib.ref_sbvh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Oracle:
+    """The plain-C restatement (oracle/dipl_oracle.c)."""
+
+    def __init__(self, path=ORC_LIB):
+        if not os.path.exists(path):
+            build()
+        L = self.lib = C.CDLL(path)
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_mt.restype = C.c_float
+        L.orc_mt.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.orc_wt.restype = C.c_float
+        L.orc_wt.argtypes = L.orc_mt.argtypes
+        L.orc_brute_closest.argtypes = [_f32p, C.c_int64, _f32p, C.c_int64, C.c_int, C.c_int, _i32p, _f32p, _f32p,
+                                        _f32p]
+        L.orc_brute_any.argtypes = [_f32p, C.c_int64, _f32p, C.c_int64, C.c_int, C.c_int, _u8p]
+        L.orc_intersect_f64.argtypes = [_f32p, _f32p, C.c_int64, _i32p, _f64p, _f64p, _f64p]
+        L.orc_brute_closest_f64.argtypes = [_f32p, C.c_int64, _f32p, C.c_int64, _i32p, _f64p]
+        L.orc_scene_bounds.argtypes = [_f32p, C.c_int64, _f32p, _f32p, _f32p, _f32p]
+        L.orc_morton30.argtypes = [_f32p, C.c_int64, _f32p, _f32p, _u32p]
+        L.orc_emc60_plan.argtypes = [_f32p, _f32p, C.c_float, _i32p, _u64p]
+        L.orc_scene_diag.restype = C.c_float
+        L.orc_scene_diag.argtypes = [_f32p, _f32p]
+        L.orc_emc60.argtypes = [_f32p, C.c_int64, _f32p, _f32p, C.c_float, _u64p]
+        L.orc_test_pairs.argtypes = [_f32p, _f32p, C.c_int64, _i32p, C.c_int, C.c_int, _f32p, _f32p, _f32p]
+        L.orc_ploc.restype = C.c_int64
+        L.orc_ploc.argtypes = [_f32p, C.c_int64, _i32p, C.c_void_p, C.c_int64, C.c_int, _i32p, _f32p, _i32p]
+
+    def set_threads(self, n):
+        self.lib.orc_set_threads(int(n))
+
+    def brute(self, tris, rays, leaf_test=0, backface=False):
+        tris, rays = _tris(tris), _rays(rays)
+        h = Hits(len(rays))
+        self.lib.orc_brute_closest(tris, len(tris), rays, len(rays), int(leaf_test), int(backface), h.prim, h.t,
+                                   h.u, h.v)
+        return h
+
+    def brute_any(self, tris, rays, leaf_test=0, backface=False):
+        tris, rays = _tris(tris), _rays(rays)
+        occ = np.empty(len(rays), np.uint8)
+        self.lib.orc_brute_any(tris, len(tris), rays, len(rays), int(leaf_test), int(backface), occ)
+        return occ.astype(bool)
+
+    def test_pairs(self, tris, rays, prim, leaf_test=0, backface=False):
+        """Leaf test of each ray against its own triangle prim[r] (t = +inf where prim < 0 or a miss)."""
+        tris, rays = _tris(tris), _rays(rays)
+        prim = np.ascontiguousarray(prim, np.int32)
+        h = Hits(len(rays))
+        h.prim = prim
+        self.lib.orc_test_pairs(tris, rays, len(rays), prim, int(leaf_test), int(backface), h.t, h.u, h.v)
+        return h
+
+    def intersect_f64(self, tris, rays, prim):
+        tris, rays = _tris(tris), _rays(rays)
+        prim = np.ascontiguousarray(prim, np.int32)
+        t, u, v = (np.empty(len(rays)) for _ in range(3))
+        self.lib.orc_intersect_f64(tris, rays, len(rays), prim, t, u, v)
+        return t, u, v
+
+    def brute_f64(self, tris, rays):
+        tris, rays = _tris(tris), _rays(rays)
+        prim = np.empty(len(rays), np.int32)
+        t = np.empty(len(rays))
+        self.lib.orc_brute_closest_f64(tris, len(tris), rays, len(rays), prim, t)
+        return prim, t
+
+    def scene_bounds(self, tris):
+        tris = _tris(tris)
+        out = [np.empty(3, np.float32) for _ in range(4)]
+        self.lib.orc_scene_bounds(tris, len(tris), *out)
+        return out  # cmin, cmax, bmin, bmax
+
+    def morton30(self, tris):
+        tris = _tris(tris)
+        cmin, cmax, _, _ = self.scene_bounds(tris)
+        codes = np.empty(len(tris), np.uint32)
+        self.lib.orc_morton30(tris, len(tris), cmin, cmax, codes)
+        return codes
+
+    def emc60(self, tris):
+        tris = _tris(tris)
+        cmin, cmax, bmin, bmax = self.scene_bounds(tris)
+        diag = self.lib.orc_scene_diag(bmin, bmax)
+        codes = np.empty(len(tris), np.uint64)
+        self.lib.orc_emc60(tris, len(tris), cmin, cmax, diag, codes)
+        return codes
+
+    def emc60_plan(self, tris):
+        cmin, cmax, bmin, bmax = self.scene_bounds(tris)
+        diag = self.lib.orc_scene_diag(bmin, bmax)
+        bits = np.empty(4, np.int32)
+        masks = np.empty(4, np.uint64)
+        self.lib.orc_emc60_plan(cmin, cmax, diag, bits, masks)
+        return bits, masks
+
+    def ploc(self, tris, perm, radius=16, seg=None, nseg=1):
+        """Returns (children (K,2) int32, boxes (K,6) float32, iterations)."""
+        tris = _tris(tris)
+        perm = np.ascontiguousarray(perm, np.int32)
+        n = len(tris)
+        k_max = max(n - nseg, 0)
+        children = np.empty(2 * max(k_max, 1), np.int32)
+        boxes = np.empty(6 * max(k_max, 1), np.float32)
+        it = np.zeros(1, np.int32)
+        seg_arr = None if seg is None else np.ascontiguousarray(seg, np.int32)
+        segp = None if seg_arr is None else seg_arr.ctypes.data_as(C.c_void_p)
+        k = self.lib.orc_ploc(tris, n, perm, segp, int(nseg), int(radius), children, boxes, it)
+        if k < 0:
+            raise ValueError("orc_ploc: bad input")
+        return children[: 2 * k].reshape(-1, 2), boxes[: 6 * k].reshape(-1, 6), int(it[0])
+
+
+def sort_perm(codes, seg=None):
+    """Stable order of the codes (ties keep triangle order), optionally by (segment, code)."""
+    if seg is None:
+        return np.argsort(codes, kind="stable").astype(np.int32)
+    return np.lexsort((codes, seg)).astype(np.int32)
+
+
+def sah_cost_binary(children, boxes, n_leaves, leaf_boxes, max_leaf_exclusive=4):
+    """FP64 SAH cost of a PLOC tree after the leaf rule "a node with < L triangles is a leaf"."""
+    k = len(children)
+    if n_leaves == 1:
+        return 1.0
+    count = np.zeros(k, np.int64)
+    for i in range(k):  # children are created before parents
+        c = 0
+        for ch in children[i]:
+            c += 1 if ch < n_leaves else count[ch - n_leaves]
+        count[i] = c
+
+    def sa(b):
+        d = b[3:6].astype(np.float64) - b[0:3].astype(np.float64)
+        return 2.0 * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0])
+
+    root = n_leaves + k - 1
+    total = 0.0
+    stack = [root]
+    while stack:
+        x = stack.pop()
+        if x < n_leaves:
+            total += sa(leaf_boxes[x])
+            continue
+        i = x - n_leaves
+        if count[i] < max_leaf_exclusive:
+            total += sa(boxes[i]) * count[i]
+            continue
+        total += sa(boxes[i])
+        stack.extend(children[i].tolist())
+    return total / sa(boxes[root - n_leaves])

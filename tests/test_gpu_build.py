@@ -1,0 +1,131 @@
+"""GPU: codes, sort and PLOC topology against the oracle, bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from diplodocus_b200 import _lib as L
+from diplodocus_b200 import accel as A
+from diplodocus_b200 import scenes as S
+from gpu_util import build
+
+pytestmark = pytest.mark.gpu
+
+
+def _meshes():
+    return {
+        "small_scene": S.small_scene(width=4, height=4)[0],
+        "soup_50k": S.soup(50000, seed=11),
+        "sphere_128x64": S.uv_sphere(128, 64, 1.0, (0, 0, 0), displacement=0.05, seed=2),
+        "duplicates": np.repeat(S.open_box(), 300, axis=0),
+    }
+
+
+@pytest.mark.parametrize("name", list(_meshes()))
+def test_morton30_codes_match_oracle(orc, name):
+    tris = _meshes()[name]
+    got = A.compute_codes(tris, L.CODE_MORTON30).cpu().numpy().view(np.uint32)
+    np.testing.assert_array_equal(got, orc.morton30(tris))
+
+
+@pytest.mark.parametrize("name", list(_meshes()))
+def test_emc60_codes_match_oracle(orc, name):
+    tris = _meshes()[name]
+    got = A.compute_codes(tris, L.CODE_EMC60).cpu().numpy().view(np.uint64)
+    np.testing.assert_array_equal(got, orc.emc60(tris))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3839, 3840, 3841, 100_003, 1 << 20])
+@pytest.mark.parametrize("key_bytes,end_bit", [(4, 30), (4, 32), (8, 60), (8, 64)])
+def test_radix_sort_matches_stable_argsort(n, key_bytes, end_bit):
+    rng = np.random.default_rng(n + end_bit)
+    dt = np.uint32 if key_bytes == 4 else np.uint64
+    hi = (1 << min(end_bit, 63)) - 1
+    keys = rng.integers(0, hi, size=n, dtype=np.uint64).astype(dt)
+    keys[: n // 3] = keys[0]  # many duplicates: stability matters
+    kt = torch.from_numpy(keys.view(np.int32 if key_bytes == 4 else np.int64)).cuda()
+    ko, vo = A.radix_sort_pairs(kt, None, 0, end_bit)
+    order = np.argsort(keys & dt(hi if end_bit < 64 else ~0), kind="stable")
+    np.testing.assert_array_equal(vo.cpu().numpy(), order.astype(np.int32))
+    np.testing.assert_array_equal(ko.cpu().numpy().view(dt), keys[order])
+
+
+@pytest.mark.parametrize("digit_bits", [6, 7, 8, 10])
+def test_radix_sort_digit_widths(digit_bits):
+    rng = np.random.default_rng(digit_bits)
+    keys = rng.integers(0, 1 << 30, size=200_000, dtype=np.uint32)
+    ko, vo = A.radix_sort_pairs(torch.from_numpy(keys.view(np.int32)).cuda(), None, 0, 30, digit_bits)
+    np.testing.assert_array_equal(vo.cpu().numpy(), np.argsort(keys, kind="stable").astype(np.int32))
+
+
+def test_radix_sort_rejects_bad_arguments():
+    k = torch.zeros(4, dtype=torch.int32, device="cuda")
+    with pytest.raises(L.DiplError):
+        A.radix_sort_pairs(k, None, 0, 40)
+    with pytest.raises(L.DiplError):
+        A.radix_sort_pairs(k, None, 0, 32, 9)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 31, 32, 33, 1000, 1025, 4097, 30000])
+@pytest.mark.parametrize("radius", [1, 4, 16, 32])
+def test_ploc_topology_matches_oracle(orc, n, radius):
+    tris = S.soup(n, seed=100 + n)
+    bvh = build(tris, nn_search_radius=radius)
+    perm, ch, bx = bvh.download_topology()
+    exp_perm = O.sort_perm(orc.morton30(tris))
+    np.testing.assert_array_equal(perm, exp_perm)
+    if n < 2:
+        return
+    ech, ebx, it = orc.ploc(tris, exp_perm, radius=radius)
+    np.testing.assert_array_equal(ch, ech)
+    np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
+    assert bvh.info().ploc_iterations == it
+
+
+@pytest.mark.parametrize("kind", [A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmc])
+def test_ploc_topology_duplicates_and_emc(orc, kind):
+    tris = np.concatenate([np.repeat(S.open_box(), 200, axis=0), S.soup(3000, seed=4)])
+    bvh = build(tris, kind)
+    perm, ch, bx = bvh.download_topology()
+    codes = orc.morton30(tris) if kind is A.AccelerationStructureType.kPloc else orc.emc60(tris)
+    exp_perm = O.sort_perm(codes)
+    np.testing.assert_array_equal(perm, exp_perm)
+    ech, ebx, it = orc.ploc(tris, exp_perm, radius=16)
+    np.testing.assert_array_equal(ch, ech)
+    np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
+
+
+def test_ploc_topology_1m_displaced_sphere(orc):
+    tris = S.uv_sphere(1024, 512, 1.0, (0, 0, 0), displacement=0.05, seed=2)
+    bvh = build(tris)
+    perm, ch, bx = bvh.download_topology()
+    exp_perm = O.sort_perm(orc.morton30(tris))
+    np.testing.assert_array_equal(perm, exp_perm)
+    ech, ebx, it = orc.ploc(tris, exp_perm, radius=16)
+    np.testing.assert_array_equal(ch, ech)
+    assert bvh.info().ploc_iterations == it
+
+
+def test_sah_cost_matches_oracle_on_same_topology(orc):
+    tris = S.soup(20000, seed=21)
+    bvh = build(tris)
+    perm, ch, bx = bvh.download_topology()
+    leaf_boxes = np.concatenate([tris[perm].min(axis=1), tris[perm].max(axis=1)], axis=1)
+    expect = O.sah_cost_binary(ch, bx, len(tris), leaf_boxes, 4)
+    assert bvh.sah_cost() == pytest.approx(expect, rel=1e-9)
+
+
+def test_build_rejects_bad_options():
+    tris = S.soup(10, seed=1)
+    for kw in (dict(nn_search_radius=0), dict(nn_search_radius=33), dict(max_triangles_per_leaf=1),
+               dict(ploc_block_size=100), dict(sort_digit_bits=9)):
+        with pytest.raises(L.DiplError):
+            build(tris, **kw)
+
+
+def test_empty_and_tiny_builds():
+    for n in (0, 1, 2, 3):
+        tris = S.soup(max(n, 1), seed=3)[:n]
+        bvh = build(tris)
+        info = bvh.info()
+        assert info.num_triangles == n
