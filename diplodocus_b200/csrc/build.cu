@@ -315,11 +315,12 @@ __global__ void __launch_bounds__(256) codes_kernel(const MeshDesc* __restrict__
 // distances (duplicate geometry) still pair up neighbour with neighbour instead of chaining.
 // ------------------------------------------------------------------------------------------------
 struct PlocParams {
-    float4* lo[2];
-    float4* hi[2];
-    int4* child;
-    float4* node_lo;
-    float4* node_hi;
+    float4* lo[2];   // clusters by iteration parity: min xyz, node id bits
+    float4* hi[2];   //                              max xyz, mesh index bits
+    int4* info[2];   //                              triangle count, first sorted position, height, 0
+    int4* child;     // internal node k: left, right, height, 0
+    float4* node_lo; // internal node k: min xyz, triangle count bits
+    float4* node_hi; // internal node k: max xyz, first sorted position bits
     int* parent;
     unsigned long long* status[2];
     PlocCtrl* ctrl;
@@ -329,13 +330,73 @@ struct PlocParams {
     int radius;
 };
 
+// Clusters at most this many are finished by the single-CTA tail kernel, resident in shared memory.
+constexpr int kTailMax = 2048;
+constexpr int kTailThreads = 1024;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Nearest neighbour of every position in [q0, q1) among clusters stored at smem index (position - base).
+// Candidates are visited in the order of the key's tie fields (gap, then parity of the lower index,
+// then side), so a strict "<" on the distance alone yields the minimum of the oracle's 64-bit key.
+template <int NT>
+__device__ __forceinline__ void nn_search(const float4* __restrict__ slo, const float4* __restrict__ shi, int base,
+                                          int n, int q0, int q1, int r, int* __restrict__ nn, int nn_base) {
+    for (int q = q0 + (int)threadIdx.x; q < q1; q += NT) {
+        const float4 a = slo[q - base], b = shi[q - base];
+        const int sg = __float_as_int(b.w);
+        float bestd = __int_as_float(0x7F800000);
+        int bestj = -1;
+        auto consider = [&](int j) {
+            if (j < 0 || j >= n) return;
+            const float4 c = slo[j - base], e = shi[j - base];
+            if (__float_as_int(e.w) != sg) return;
+            const float d = ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, e.x, e.y, e.z);
+            if (d < bestd || bestj < 0) {
+                bestd = d;
+                bestj = j;
+            }
+        };
+#pragma unroll 4
+        for (int k = 1; k <= r; ++k) {
+            // gap k: lower index q-k (backward) or q (forward); an even lower index wins, then backward.
+            const bool fwd_first = (k & 1) && !(q & 1);
+            consider(fwd_first ? q + k : q - k);
+            consider(fwd_first ? q - k : q + k);
+        }
+        nn[q - nn_base] = bestj;
+    }
+}
+
+// Writes internal node `knew` = merge of clusters (la, lb, li) and (ra, rb, ri); returns the merged cluster.
+__device__ __forceinline__ void emit_node(const PlocParams& P, int knew, const float4& la, const float4& lb,
+                                          const int4& li, const float4& ra, const float4& rb, const int4& ri,
+                                          float4& oa, float4& ob, int4& oi) {
+    const int left = __float_as_int(la.w), right = __float_as_int(ra.w);
+    const int node = P.num_leaves + knew;
+    oa = make_float4(fminf(la.x, ra.x), fminf(la.y, ra.y), fminf(la.z, ra.z), __int_as_float(node));
+    ob = make_float4(fmaxf(lb.x, rb.x), fmaxf(lb.y, rb.y), fmaxf(lb.z, rb.z), lb.w);
+    oi = make_int4(li.x + ri.x, min(li.y, ri.y), max(li.z, ri.z) + 1, 0);
+    P.child[knew] = make_int4(left, right, oi.z, 0);
+    P.node_lo[knew] = make_float4(oa.x, oa.y, oa.z, __int_as_float(oi.x));
+    P.node_hi[knew] = make_float4(ob.x, ob.y, ob.z, __int_as_float(oi.y));
+    P.parent[left] = node;
+    P.parent[right] = node;
+}
+
 template <int B>
 struct PlocSmem {
     static constexpr int T = B * kPlocIpt;
     static constexpr int W = T + 4 * kRadiusMax;
-    float lx[W], ly[W], lz[W], hx[W], hy[W], hz[W];
-    int node[W];
-    int seg[W];
+    float4 lo[W];  // min xyz, node id bits
+    float4 hi[W];  // max xyz, mesh index bits
+    int4 info[W];  // count, first position, height
     int nn[T + 2 * kRadiusMax];
     uint32_t warp_sum[B / 32];
     unsigned long long prefix;
@@ -343,62 +404,24 @@ struct PlocSmem {
     int n, mbase;
 };
 
-__device__ __forceinline__ void node_info(const PlocParams& P, int id, int& count, int& pmin, int& height) {
-    if (id < P.num_leaves) {
-        count = 1, pmin = id, height = 0;
-    } else {
-        int k = id - P.num_leaves;
-        count = __float_as_int(P.node_lo[k].w);
-        pmin = __float_as_int(P.node_hi[k].w);
-        height = P.child[k].z;
-    }
-}
-
 template <int B>
 __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int tiles, int n, int mbase, int parity) {
     constexpr int T = PlocSmem<B>::T;
     const int r = P.radius;
     const int s0 = tile * T;
     const int w0 = max(s0 - 2 * r, 0), w1 = min(s0 + T + 2 * r, n);
-    const float4* __restrict__ in_lo = P.lo[parity];
-    const float4* __restrict__ in_hi = P.hi[parity];
+    // window: asynchronous 16-byte copies, all in flight at once (one memory round trip)
     for (int i = threadIdx.x; i < w1 - w0; i += B) {
-        float4 a = in_lo[w0 + i], b = in_hi[w0 + i];
-        s.lx[i] = a.x, s.ly[i] = a.y, s.lz[i] = a.z;
-        s.hx[i] = b.x, s.hy[i] = b.y, s.hz[i] = b.z;
-        s.node[i] = __float_as_int(a.w);
-        s.seg[i] = __float_as_int(b.w);
+        cp_async16(&s.lo[i], P.lo[parity] + w0 + i);
+        cp_async16(&s.hi[i], P.hi[parity] + w0 + i);
+        cp_async16(&s.info[i], P.info[parity] + w0 + i);
     }
     if (threadIdx.x == 0) P.status[parity ^ 1][tile] = 0ull;  // ready for the next iteration
+    cp_async_wait_all();
     __syncthreads();
 
-    // ---- nearest neighbours of [q0, q1) -----------------------------------------------------------
     const int q0 = max(s0 - r, 0), q1 = min(s0 + T + r, n);
-    for (int q = q0 + threadIdx.x; q < q1; q += B) {
-        const int qi = q - w0;
-        const float lx = s.lx[qi], ly = s.ly[qi], lz = s.lz[qi], hx = s.hx[qi], hy = s.hy[qi], hz = s.hz[qi];
-        const int sg = s.seg[qi];
-        unsigned long long best = ~0ull;
-        const int jlo = max(q - r, 0), jhi = min(q + r, n - 1);
-        for (int j = jlo; j <= jhi; ++j) {
-            if (j == q) continue;
-            const int ji = j - w0;
-            if (s.seg[ji] != sg) continue;
-            float d = ploc_distance(lx, ly, lz, hx, hy, hz, s.lx[ji], s.ly[ji], s.lz[ji], s.hx[ji], s.hy[ji], s.hz[ji]);
-            unsigned int gap = (unsigned int)abs(j - q);
-            unsigned int mn = (unsigned int)min(j, q);
-            unsigned long long key = ((unsigned long long)__float_as_uint(d) << 32) |
-                                     (unsigned long long)((gap << 2) | ((mn & 1u) << 1) | (j > q ? 1u : 0u));
-            best = key < best ? key : best;
-        }
-        int nj = -1;
-        if (best != ~0ull) {
-            uint32_t tie = (uint32_t)best;
-            int gap = (int)(tie >> 2);
-            nj = (tie & 1u) ? q + gap : q - gap;
-        }
-        s.nn[q - q0] = nj;
-    }
+    nn_search<B>(s.lo, s.hi, w0, n, q0, q1, r, s.nn, q0);
     __syncthreads();
 
     // ---- merge decisions (blocked: kPlocIpt consecutive positions per thread) ----------------------
@@ -432,42 +455,27 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     }
     const uint32_t excl = woff + x - mine;
 
-    // ---- decoupled look-back over tiles: (kept, merged) prefixes ----------------------------------
-    if (threadIdx.x == 0) {
+    // ---- decoupled look-back over tiles: (kept, merged) prefixes (warp 0) ---------------------------
+    if (threadIdx.x < 32) {
         const unsigned long long agg = ((unsigned long long)(total & 0xFFFFu) << 31) | (total >> 16);
         unsigned long long* st = P.status[parity];
         unsigned long long prefix = 0;
-        int ok = 1;
+        bool ok = true;
         if (tile == 0) {
-            st_release_u64(&st[0], (2ull << 62) | agg);
+            if (threadIdx.x == 0) st_release_u64(&st[0], (2ull << 62) | agg);
         } else {
-            st_release_u64(&st[tile], (1ull << 62) | agg);
-            int j = tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                unsigned long long w = ld_acquire_u64(&st[j]);
-                unsigned long long state = w >> 62;
-                if (state == 0ull) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(P.err, kErrTimeout);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
-                prefix += w & ((1ull << 62) - 1ull);
-                if (state == 2ull) break;
-                --j;
-            }
-            st_release_u64(&st[tile], (2ull << 62) | (prefix + agg));
+            if (threadIdx.x == 0) st_release_u64(&st[tile], (1ull << 62) | agg);
+            prefix = warp_lookback(st, tile, P.err, &ok);
+            if (threadIdx.x == 0 && ok) st_release_u64(&st[tile], (2ull << 62) | (prefix + agg));
         }
-        s.prefix = prefix;
-        s.ok = ok;
-        if (tile == tiles - 1 && ok) {
-            unsigned long long inc = prefix + agg;
-            P.ctrl->n[parity ^ 1] = (uint32_t)(inc >> 31);
-            P.ctrl->merges[parity ^ 1] = (uint32_t)mbase + (uint32_t)(inc & 0x7FFFFFFFull);
+        if (threadIdx.x == 0) {
+            s.prefix = prefix;
+            s.ok = ok ? 1 : 0;
+            if (tile == tiles - 1 && ok) {
+                unsigned long long inc = prefix + agg;
+                P.ctrl->n[parity ^ 1] = (uint32_t)(inc >> 31);
+                P.ctrl->merges[parity ^ 1] = (uint32_t)mbase + (uint32_t)(inc & 0x7FFFFFFFull);
+            }
         }
     }
     __syncthreads();
@@ -478,6 +486,7 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     // ---- write surviving clusters and new nodes ----------------------------------------------------
     float4* __restrict__ out_lo = P.lo[parity ^ 1];
     float4* __restrict__ out_hi = P.hi[parity ^ 1];
+    int4* __restrict__ out_info = P.info[parity ^ 1];
     uint32_t kpos = kept_before + (excl & 0xFFFFu);
     uint32_t mpos = (uint32_t)mbase + merged_before + (excl >> 16);
     const int max_internal = P.num_leaves - P.num_meshes;
@@ -485,44 +494,33 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     for (int k = 0; k < kPlocIpt; ++k) {
         if (!((keep_bits >> k) & 1u)) continue;
         const int i = ib + k, ii = i - w0;
-        float lx = s.lx[ii], ly = s.ly[ii], lz = s.lz[ii], hx = s.hx[ii], hy = s.hy[ii], hz = s.hz[ii];
-        int node = s.node[ii];
+        float4 oa = s.lo[ii], ob = s.hi[ii];
+        int4 oi = s.info[ii];
         if ((merge_bits >> k) & 1u) {
-            const int j = s.nn[i - q0], ji = j - w0;
-            lx = fminf(lx, s.lx[ji]), ly = fminf(ly, s.ly[ji]), lz = fminf(lz, s.lz[ji]);
-            hx = fmaxf(hx, s.hx[ji]), hy = fmaxf(hy, s.hy[ji]), hz = fmaxf(hz, s.hz[ji]);
-            const int left = node, right = s.node[ji];
+            const int ji = s.nn[i - q0] - w0;
             const int knew = (int)mpos++;
             if (knew >= max_internal) {
                 atomicOr(P.err, kErrIterations);
                 continue;
             }
-            int cl, pl, hl, cr, pr, hr;
-            node_info(P, left, cl, pl, hl);
-            node_info(P, right, cr, pr, hr);
-            node = P.num_leaves + knew;
-            P.child[knew] = make_int4(left, right, max(hl, hr) + 1, 0);
-            P.node_lo[knew] = make_float4(lx, ly, lz, __int_as_float(cl + cr));
-            P.node_hi[knew] = make_float4(hx, hy, hz, __int_as_float(min(pl, pr)));
-            P.parent[left] = node;
-            P.parent[right] = node;
+            emit_node(P, knew, s.lo[ii], s.hi[ii], s.info[ii], s.lo[ji], s.hi[ji], s.info[ji], oa, ob, oi);
         }
         if (kpos < (uint32_t)P.num_leaves) {
-            out_lo[kpos] = make_float4(lx, ly, lz, __int_as_float(node));
-            out_hi[kpos] = make_float4(hx, hy, hz, __int_as_float(s.seg[ii]));
+            out_lo[kpos] = oa;
+            out_hi[kpos] = ob;
+            out_info[kpos] = oi;
         }
         ++kpos;
     }
 }
 
-// Every PLOC iteration in one cooperative launch. Iterations are separated by a grid barrier; once a
-// single tile is left, block 0 finishes alone with block barriers.
+// Every PLOC iteration while more than kTailMax clusters remain, in one cooperative launch. Iterations are
+// separated by a grid barrier over the blocks that still have tiles.
 template <int B>
 __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     PlocSmem<B>& s = *reinterpret_cast<PlocSmem<B>*>(s_raw);
     constexpr int T = PlocSmem<B>::T;
-    bool solo = false;
     uint32_t iter = 0;
     for (;;) {
         const int parity = iter & 1;
@@ -535,24 +533,24 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
         const int n = s.n, mbase = s.mbase;
         const bool ok = s.ok != 0;
         __syncthreads();
-        if (!ok || n <= P.num_meshes) break;
+        if (!ok || n <= P.num_meshes || n <= kTailMax) break;
         if (iter >= kMaxPlocIterations) {
             if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
             break;
         }
         const int tiles = (n + T - 1) / T;
-        if (tiles == 1 && !solo) {
-            if (blockIdx.x != 0) break;
-            solo = true;
-        }
-        for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        // Tile counts never grow, so a block past the tile count has no work in any later iteration:
+        // it leaves, and the barrier waits for the blocks that are still active.
+        const int active = min((int)gridDim.x, tiles);
+        if ((int)blockIdx.x >= active) break;
+        for (int t = blockIdx.x; t < tiles; t += active) {
             ploc_tile<B>(P, s, t, tiles, n, mbase, parity);
             __syncthreads();
         }
-        if (solo) {
+        if (active == 1) {
             __threadfence();
             __syncthreads();
-        } else if (!grid_barrier(&P.ctrl->barrier, P.err)) {
+        } else if (!grid_barrier(&P.ctrl->barrier, (uint32_t)active, P.err)) {
             break;
         }
         ++iter;
@@ -560,9 +558,126 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
     if (blockIdx.x == 0 && threadIdx.x == 0) P.ctrl->iterations = iter;
 }
 
+// The last iterations (at most kTailMax clusters) in one CTA of 1024 threads, clusters resident in shared
+// memory and double-buffered; the same rules as ploc_kernel, so the result equals the oracle's loop.
+struct TailSmem {
+    float4 lo[2][kTailMax];
+    float4 hi[2][kTailMax];
+    int4 info[2][kTailMax];
+    int nn[kTailMax];
+    uint32_t warp_sum[kTailThreads / 32];
+};
+
+__global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    TailSmem& s = *reinterpret_cast<TailSmem*>(s_raw);
+    constexpr int IPT = kTailMax / kTailThreads;
+    if (ld_acquire_u32(P.err) != 0u) return;
+    uint32_t iter = P.ctrl->iterations;
+    int n = (int)P.ctrl->n[iter & 1];
+    int mbase = (int)P.ctrl->merges[iter & 1];
+    if (n <= P.num_meshes) return;
+    if (n > kTailMax) {  // cannot happen: the grid kernel runs until n <= kTailMax
+        if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+        return;
+    }
+    const uint32_t first_parity = iter & 1;
+    for (int i = threadIdx.x; i < n; i += kTailThreads) {
+        cp_async16(&s.lo[0][i], P.lo[first_parity] + i);
+        cp_async16(&s.hi[0][i], P.hi[first_parity] + i);
+        cp_async16(&s.info[0][i], P.info[first_parity] + i);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int r = P.radius;
+    const int max_internal = P.num_leaves - P.num_meshes;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int cur = 0;
+    uint32_t tail_iters = 0;
+    while (n > P.num_meshes) {
+        if (iter + tail_iters >= kMaxPlocIterations) {
+            if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+            return;
+        }
+        const float4* __restrict__ lo = s.lo[cur];
+        const float4* __restrict__ hi = s.hi[cur];
+        const int4* __restrict__ info = s.info[cur];
+        nn_search<kTailThreads>(lo, hi, 0, n, 0, n, r, s.nn, 0);
+        __syncthreads();
+        const int ib = threadIdx.x * IPT;
+        uint32_t keep_bits = 0, merge_bits = 0;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int i = ib + k;
+            if (i >= n) break;
+            const int j = s.nn[i];
+            const bool mutual = j >= 0 && s.nn[j] == i;
+            if (!(mutual && i > j)) keep_bits |= 1u << k;
+            if (mutual && i < j) merge_bits |= 1u << k;
+        }
+        const uint32_t mine = (uint32_t)__popc(keep_bits) | ((uint32_t)__popc(merge_bits) << 16);
+        uint32_t x = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s.warp_sum[warp] = x;
+        __syncthreads();
+        uint32_t woff = 0, total = 0;
+        for (int w = 0; w < kTailThreads / 32; ++w) {
+            const uint32_t v = s.warp_sum[w];
+            if (w < warp) woff += v;
+            total += v;
+        }
+        const uint32_t excl = woff + x - mine;
+        uint32_t kpos = excl & 0xFFFFu;
+        uint32_t mpos = (uint32_t)mbase + (excl >> 16);
+        const int nxt = cur ^ 1;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            if (!((keep_bits >> k) & 1u)) continue;
+            const int i = ib + k;
+            float4 oa = lo[i], ob = hi[i];
+            int4 oi = info[i];
+            if ((merge_bits >> k) & 1u) {
+                const int j = s.nn[i];
+                const int knew = (int)mpos++;
+                if (knew >= max_internal) {
+                    atomicOr(P.err, kErrIterations);
+                    continue;
+                }
+                emit_node(P, knew, lo[i], hi[i], info[i], lo[j], hi[j], info[j], oa, ob, oi);
+            }
+            s.lo[nxt][kpos] = oa;
+            s.hi[nxt][kpos] = ob;
+            s.info[nxt][kpos] = oi;
+            ++kpos;
+        }
+        const int kept = (int)(total & 0xFFFFu);
+        mbase += (int)(total >> 16);
+        __syncthreads();
+        if (kept == n) {  // no progress: impossible under a strict total order on pairs
+            if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+            return;
+        }
+        n = kept;
+        cur = nxt;
+        ++tail_iters;
+    }
+    // final clusters (one per mesh) to the buffer of the final parity, for the root pass
+    const uint32_t final_iter = iter + tail_iters;
+    for (int i = threadIdx.x; i < n; i += kTailThreads) {
+        P.lo[final_iter & 1][i] = s.lo[cur][i];
+        P.hi[final_iter & 1][i] = s.hi[cur][i];
+        P.info[final_iter & 1][i] = s.info[cur][i];
+    }
+    if (threadIdx.x == 0) P.ctrl->iterations = final_iter;
+}
+
 __global__ void ploc_init_kernel(const MeshDesc* __restrict__ meshes, const long long* __restrict__ offsets, int m,
                                  long long n, const uint32_t* __restrict__ perm, float4* __restrict__ lo,
-                                 float4* __restrict__ hi, int* __restrict__ parent) {
+                                 float4* __restrict__ hi, int4* __restrict__ info, int* __restrict__ parent) {
     long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (p >= n) return;
     long long g = perm[p];
@@ -572,6 +687,7 @@ __global__ void ploc_init_kernel(const MeshDesc* __restrict__ meshes, const long
     tri_box(t, a, b);
     lo[p] = make_float4(a.x, a.y, a.z, __int_as_float((int)p));
     hi[p] = make_float4(b.x, b.y, b.z, __int_as_float(k));
+    info[p] = make_int4(1, (int)p, 0, 0);
     parent[p] = -1;
 }
 
@@ -694,10 +810,13 @@ __device__ __forceinline__ void child_box(const LayoutParams& P, const MeshDesc*
     }
 }
 
-__global__ void node_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
-                                  const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
-                                  const uint32_t* __restrict__ rev_index, const int* __restrict__ leaf_start_of,
-                                  BNode* __restrict__ nodes, double* __restrict__ sah, const uint32_t* err) {
+__device__ __forceinline__ void node_write_one(const LayoutParams& P, const MeshDesc* __restrict__ meshes,
+                                               const long long* __restrict__ offsets, int m,
+                                               const uint32_t* __restrict__ perm,
+                                               const uint32_t* __restrict__ rev_index,
+                                               const int* __restrict__ leaf_start_of, BNode* __restrict__ nodes,
+                                               double* __restrict__ sah, const uint32_t* err, double& local_sum,
+                                               double& local_count) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= P.num_inner || *err != 0u) return;
     if (__float_as_int(P.node_lo[k].w) < P.L) return;
@@ -727,9 +846,40 @@ __global__ void node_write_kernel(LayoutParams P, const MeshDesc* __restrict__ m
                        pad_up(lo[1].z, hi[1].z));
     nd.d = make_int4(ref[0], ref[1], 0, 0);
     nodes[f] = nd;
-    int mesh = find_mesh(offsets, m, (long long)perm[__float_as_int(P.node_hi[k].w)]);
-    atomicAdd(&sah[2 * mesh], acc);
-    atomicAdd(&sah[2 * mesh + 1], 1.0);
+    const int mesh = find_mesh(offsets, m, (long long)perm[__float_as_int(P.node_hi[k].w)]);
+    if (m == 1) {
+        local_sum = acc;
+        local_count = 1.0;
+    } else {
+        atomicAdd(&sah[2 * mesh], acc);
+        atomicAdd(&sah[2 * mesh + 1], 1.0);
+    }
+}
+
+// Single-mesh builds: one FP64 atomic pair per block instead of one per node.
+__global__ void node_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
+                                  const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
+                                  const uint32_t* __restrict__ rev_index, const int* __restrict__ leaf_start_of,
+                                  BNode* __restrict__ nodes, double* __restrict__ sah, const uint32_t* err) {
+    double local_sum = 0.0, local_count = 0.0;
+    node_write_one(P, meshes, offsets, m, perm, rev_index, leaf_start_of, nodes, sah, err, local_sum, local_count);
+    if (m != 1) return;
+    __shared__ double s_sum[32], s_cnt[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        local_sum += __shfl_xor_sync(0xffffffffu, local_sum, o);
+        local_count += __shfl_xor_sync(0xffffffffu, local_count, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_sum[warp] = local_sum, s_cnt[warp] = local_count;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += s_sum[w], c += s_cnt[w];
+        if (c > 0.0) {
+            atomicAdd(&sah[0], a);
+            atomicAdd(&sah[1], c);
+        }
+    }
 }
 
 // Roots of every mesh: the final clusters (one per mesh, in mesh order).
@@ -794,6 +944,15 @@ dipl_status launch_ploc(const PlocParams& P, int initial_tiles, cudaStream_t str
     void* args[] = {const_cast<PlocParams*>(&P)};
     DIPL_CUDA(cudaLaunchCooperativeKernel((const void*)ploc_kernel<B>, dim3(grid), dim3(B), args, smem, stream));
     note_launches();
+    return DIPL_OK;
+}
+
+dipl_status launch_ploc_tail(const PlocParams& P, cudaStream_t stream) {
+    const size_t smem = sizeof(TailSmem);
+    DIPL_CUDA(cudaFuncSetAttribute(ploc_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ploc_tail_kernel<<<1, kTailThreads, smem, stream>>>(P);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
     return DIPL_OK;
 }
 
@@ -954,12 +1113,14 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     int* parent;
     unsigned long long* status;
     float4 *c_lo0, *c_hi0, *c_lo1, *c_hi1;
+    int4 *c_in0, *c_in1;
     const long long Kalloc = std::max<long long>(K, 1);
     if ((st = scratch.alloc(&d_ctrl, 1)) != DIPL_OK || (st = storage->alloc(&child, Kalloc)) != DIPL_OK ||
         (st = storage->alloc(&nlo, Kalloc)) != DIPL_OK || (st = storage->alloc(&nhi, Kalloc)) != DIPL_OK ||
         (st = scratch.alloc(&parent, N + Kalloc)) != DIPL_OK || (st = scratch.alloc(&status, 2 * tiles0 + 2)) != DIPL_OK ||
         (st = scratch.alloc(&c_lo0, N)) != DIPL_OK || (st = scratch.alloc(&c_hi0, N)) != DIPL_OK ||
-        (st = scratch.alloc(&c_lo1, N)) != DIPL_OK || (st = scratch.alloc(&c_hi1, N)) != DIPL_OK)
+        (st = scratch.alloc(&c_lo1, N)) != DIPL_OK || (st = scratch.alloc(&c_hi1, N)) != DIPL_OK ||
+        (st = scratch.alloc(&c_in0, N)) != DIPL_OK || (st = scratch.alloc(&c_in1, N)) != DIPL_OK)
         return st;
     PlocCtrl hctrl{};
     hctrl.n[0] = (uint32_t)N;
@@ -967,14 +1128,17 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     DIPL_CUDA(cudaMemcpyAsync(d_ctrl, &hctrl, sizeof(PlocCtrl), cudaMemcpyHostToDevice, stream));
     DIPL_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (2 * tiles0 + 2), stream));
     fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(parent, N + K, -1); note_launches();
-    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, m, N, perm, c_lo0, c_hi0, parent); note_launches();
+    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, m, N, perm, c_lo0, c_hi0, c_in0,
+                                                             parent);
+    note_launches();
     DIPL_CUDA(cudaGetLastError());
     P.lo[0] = c_lo0, P.hi[0] = c_hi0, P.lo[1] = c_lo1, P.hi[1] = c_hi1;
+    P.info[0] = c_in0, P.info[1] = c_in1;
     P.child = child, P.node_lo = nlo, P.node_hi = nhi, P.parent = parent;
     P.status[0] = status, P.status[1] = status + tiles0 + 1;
     P.ctrl = d_ctrl, P.err = d_err;
     P.num_leaves = (int)N, P.num_meshes = m, P.radius = d0.nn_search_radius;
-    if (N > m) {
+    if (N > m && N > kTailMax) {
         switch (B) {
             case 128: st = launch_ploc<128>(P, tiles0, stream); break;
             case 512: st = launch_ploc<512>(P, tiles0, stream); break;
@@ -982,6 +1146,7 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
         }
         if (st != DIPL_OK) return st;
     }
+    if (N > m && (st = launch_ploc_tail(P, stream)) != DIPL_OK) return st;
 
     // ---- layout -------------------------------------------------------------------------------------
     LayoutParams LP{child, nlo, nhi, parent, (int)N, (int)K, L};

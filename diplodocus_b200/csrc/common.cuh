@@ -6,7 +6,7 @@
 
 #include <string>
 
-#include "../../include/dipl_bvh.h"
+#include "dipl_bvh.h"
 
 #if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
 #error "libdipl_bvh is built for sm_100a (B200) only"
@@ -109,7 +109,8 @@ struct GridBarrier {
     uint32_t generation;
 };
 
-__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t* err) {
+// `expected` = number of blocks taking part (the same value in every participating block).
+__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t expected, uint32_t* err) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -117,7 +118,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t* err) {
         uint32_t gen = ld_acquire_u32(&bar->generation);
         __threadfence();
         uint32_t arrived = atomicAdd(&bar->count, 1u);
-        if (arrived == gridDim.x - 1) {
+        if (arrived == expected - 1) {
             atomicExch(&bar->count, 0u);
             __threadfence();
             st_release_u32(&bar->generation, gen + 1u);
@@ -136,6 +137,45 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t* err) {
     }
     __syncthreads();
     return ok != 0;
+}
+
+// Warp-parallel decoupled look-back (call with all 32 lanes of one warp). `status[j]` holds a 64-bit word:
+// state in the top two bits (0 = not ready, 1 = aggregate of tile j, 2 = inclusive prefix through tile j)
+// and a value in the low 62 bits; values add without carries between packed fields. Returns the exclusive
+// prefix of `tile`, reading 32 predecessors per round trip. Bounded: on timeout sets *err and *ok = false.
+__device__ __forceinline__ unsigned long long warp_lookback(const unsigned long long* status, long long tile,
+                                                            uint32_t* err, bool* ok) {
+    constexpr unsigned long long kVal = (1ull << 62) - 1ull;
+    const int lane = threadIdx.x & 31;
+    unsigned long long prefix = 0;
+    long long j = tile - 1;
+    uint32_t spins = 0;
+    *ok = true;
+    while (j >= 0) {
+        const long long idx = j - lane;
+        const unsigned long long w = idx >= 0 ? ld_acquire_u64(status + idx) : (2ull << 62);
+        const unsigned long long state = w >> 62;
+        const uint32_t inc = __ballot_sync(0xffffffffu, state == 2ull);
+        const uint32_t zero = __ballot_sync(0xffffffffu, state == 0ull);
+        const int lim = inc ? __ffs(inc) - 1 : 31;
+        const uint32_t upto = lim == 31 ? 0xffffffffu : ((2u << lim) - 1u);
+        if (zero & upto) {
+            if (++spins > kSpinLimit) {
+                if (lane == 0) atomicOr(err, kErrTimeout);
+                *ok = false;
+                return 0ull;
+            }
+            __nanosleep(20);
+            continue;
+        }
+        unsigned long long v = lane <= lim ? (w & kVal) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        prefix += v;
+        if (inc) break;
+        j -= 32;
+    }
+    return prefix;
 }
 
 // Surface-area-like distance of PLOC: half the area of the union box, evaluated with fixed FMAs so

@@ -10,7 +10,6 @@ constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr unsigned long long kAgg = 1ull << 62;
 constexpr unsigned long long kInc = 2ull << 62;
-constexpr unsigned long long kValMask = (1ull << 62) - 1ull;
 
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(const uint32_t* in, uint32_t* out,
                                                             int64_t n, unsigned long long* __restrict__ status,
@@ -46,35 +45,20 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const uint32_t* in, 
         if (w < warp) woff += t;
         total += t;
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         unsigned long long prefix = 0;
         bool ok = true;
         if (tile == 0) {
-            st_release_u64(&status[0], kInc | total);
+            if (threadIdx.x == 0) st_release_u64(&status[0], kInc | total);
         } else {
-            st_release_u64(&status[tile], kAgg | total);
-            int64_t j = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                unsigned long long w = ld_acquire_u64(&status[j]);
-                unsigned long long st = w & ~kValMask;
-                if (st == 0ull) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(err, kErrTimeout);
-                        ok = false;
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
-                prefix += w & kValMask;
-                if (st == kInc) break;
-                --j;
-            }
-            st_release_u64(&status[tile], kInc | (prefix + total));
+            if (threadIdx.x == 0) st_release_u64(&status[tile], kAgg | total);
+            prefix = warp_lookback(status, tile, err, &ok);
+            if (threadIdx.x == 0 && ok) st_release_u64(&status[tile], kInc | (prefix + total));
         }
-        s_prefix = ok ? prefix : 0ull;
-        if (d_total && (int64_t)(tile + 1) * kScanTile >= n) *d_total = (uint32_t)(prefix + total);
+        if (threadIdx.x == 0) {
+            s_prefix = ok ? prefix : 0ull;
+            if (d_total && (int64_t)(tile + 1) * kScanTile >= n) *d_total = (uint32_t)(prefix + total);
+        }
     }
     __syncthreads();
     unsigned long long run = s_prefix + woff + (x - local);

@@ -45,7 +45,8 @@ def test_radix_sort_matches_stable_argsort(n, key_bytes, end_bit):
     keys[: n // 3] = keys[0]  # many duplicates: stability matters
     kt = torch.from_numpy(keys.view(np.int32 if key_bytes == 4 else np.int64)).cuda()
     ko, vo = A.radix_sort_pairs(kt, None, 0, end_bit)
-    order = np.argsort(keys & dt(hi if end_bit < 64 else ~0), kind="stable")
+    mask = dt(hi) if end_bit < 64 else np.iinfo(dt).max
+    order = np.argsort(keys & mask, kind="stable")
     np.testing.assert_array_equal(vo.cpu().numpy(), order.astype(np.int32))
     np.testing.assert_array_equal(ko.cpu().numpy().view(dt), keys[order])
 
