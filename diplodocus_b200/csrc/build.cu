@@ -405,8 +405,9 @@ struct PlocSmem {
 };
 
 template <int B>
-__device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int tiles, int n, int mbase, int parity) {
-    constexpr int T = PlocSmem<B>::T;
+__device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int tiles, int n, int mbase, int parity,
+                          int ipt) {
+    const int T = B * ipt;  // positions of this tile (ipt <= kPlocIpt)
     const int r = P.radius;
     const int s0 = tile * T;
     const int w0 = max(s0 - 2 * r, 0), w1 = min(s0 + T + 2 * r, n);
@@ -416,7 +417,6 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
         cp_async16(&s.hi[i], P.hi[parity] + w0 + i);
         cp_async16(&s.info[i], P.info[parity] + w0 + i);
     }
-    if (threadIdx.x == 0) P.status[parity ^ 1][tile] = 0ull;  // ready for the next iteration
     cp_async_wait_all();
     __syncthreads();
 
@@ -425,12 +425,12 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     __syncthreads();
 
     // ---- merge decisions (blocked: kPlocIpt consecutive positions per thread) ----------------------
-    const int ib = s0 + threadIdx.x * kPlocIpt;
+    const int ib = s0 + threadIdx.x * ipt;
     uint32_t keep_bits = 0, merge_bits = 0;
 #pragma unroll
     for (int k = 0; k < kPlocIpt; ++k) {
         int i = ib + k;
-        if (i >= n) break;
+        if (k >= ipt || i >= n) break;
         int j = s.nn[i - q0];
         bool mutual = j >= 0 && s.nn[j - q0] == i;
         if (!(mutual && i > j)) keep_bits |= 1u << k;
@@ -492,7 +492,7 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     const int max_internal = P.num_leaves - P.num_meshes;
 #pragma unroll
     for (int k = 0; k < kPlocIpt; ++k) {
-        if (!((keep_bits >> k) & 1u)) continue;
+        if (!((keep_bits >> k) & 1u)) continue;  // also 0 for k >= ipt
         const int i = ib + k, ii = i - w0;
         float4 oa = s.lo[ii], ob = s.hi[ii];
         int4 oi = s.info[ii];
@@ -520,8 +520,8 @@ template <int B>
 __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     PlocSmem<B>& s = *reinterpret_cast<PlocSmem<B>*>(s_raw);
-    constexpr int T = PlocSmem<B>::T;
     uint32_t iter = 0;
+    int active_prev = (int)gridDim.x;
     for (;;) {
         const int parity = iter & 1;
         if (threadIdx.x == 0) {
@@ -538,13 +538,23 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
             if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
             break;
         }
+        // Items per thread shrink with the cluster count so that small iterations still spread over many
+        // SMs; the same rule in every block.
+        const long long cap = (long long)B * gridDim.x;
+        const int ipt = n >= 4 * cap ? 4 : (n >= 2 * cap ? 2 : 1);
+        const int T = B * ipt;
         const int tiles = (n + T - 1) / T;
-        // Tile counts never grow, so a block past the tile count has no work in any later iteration:
-        // it leaves, and the barrier waits for the blocks that are still active.
-        const int active = min((int)gridDim.x, tiles);
+        // The set of active blocks only shrinks: a block that leaves never comes back, and the barrier
+        // waits for exactly the blocks still active (the same count in every block).
+        const int active = min(active_prev, tiles);
+        active_prev = active;
         if ((int)blockIdx.x >= active) break;
+        // Clear the other parity's look-back words for the next iteration: it has at most n / B tiles.
+        // Nobody reads that array during this iteration.
+        const int next_words = (n + B - 1) / B;
+        for (int t = blockIdx.x * B + threadIdx.x; t < next_words; t += active * B) P.status[parity ^ 1][t] = 0ull;
         for (int t = blockIdx.x; t < tiles; t += active) {
-            ploc_tile<B>(P, s, t, tiles, n, mbase, parity);
+            ploc_tile<B>(P, s, t, tiles, n, mbase, parity, ipt);
             __syncthreads();
         }
         if (active == 1) {
@@ -1106,6 +1116,7 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     const int B = ploc_block_for(d0.ploc_block_size);
     const int T = B * kPlocIpt;
     const int tiles0 = (int)((N + T - 1) / T);
+    const int tiles_max = (int)((N + B - 1) / B);  // tiles of one item per thread
     PlocParams P{};
     PlocCtrl* d_ctrl;
     int4* child;
@@ -1117,7 +1128,7 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     const long long Kalloc = std::max<long long>(K, 1);
     if ((st = scratch.alloc(&d_ctrl, 1)) != DIPL_OK || (st = storage->alloc(&child, Kalloc)) != DIPL_OK ||
         (st = storage->alloc(&nlo, Kalloc)) != DIPL_OK || (st = storage->alloc(&nhi, Kalloc)) != DIPL_OK ||
-        (st = scratch.alloc(&parent, N + Kalloc)) != DIPL_OK || (st = scratch.alloc(&status, 2 * tiles0 + 2)) != DIPL_OK ||
+        (st = scratch.alloc(&parent, N + Kalloc)) != DIPL_OK || (st = scratch.alloc(&status, 2 * tiles_max + 2)) != DIPL_OK ||
         (st = scratch.alloc(&c_lo0, N)) != DIPL_OK || (st = scratch.alloc(&c_hi0, N)) != DIPL_OK ||
         (st = scratch.alloc(&c_lo1, N)) != DIPL_OK || (st = scratch.alloc(&c_hi1, N)) != DIPL_OK ||
         (st = scratch.alloc(&c_in0, N)) != DIPL_OK || (st = scratch.alloc(&c_in1, N)) != DIPL_OK)
@@ -1126,7 +1137,7 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     hctrl.n[0] = (uint32_t)N;
     hctrl.merges[0] = 0;
     DIPL_CUDA(cudaMemcpyAsync(d_ctrl, &hctrl, sizeof(PlocCtrl), cudaMemcpyHostToDevice, stream));
-    DIPL_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (2 * tiles0 + 2), stream));
+    DIPL_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (2 * tiles_max + 2), stream));
     fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(parent, N + K, -1); note_launches();
     ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, m, N, perm, c_lo0, c_hi0, c_in0,
                                                              parent);
@@ -1135,7 +1146,7 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     P.lo[0] = c_lo0, P.hi[0] = c_hi0, P.lo[1] = c_lo1, P.hi[1] = c_hi1;
     P.info[0] = c_in0, P.info[1] = c_in1;
     P.child = child, P.node_lo = nlo, P.node_hi = nhi, P.parent = parent;
-    P.status[0] = status, P.status[1] = status + tiles0 + 1;
+    P.status[0] = status, P.status[1] = status + tiles_max + 1;
     P.ctrl = d_ctrl, P.err = d_err;
     P.num_leaves = (int)N, P.num_meshes = m, P.radius = d0.nn_search_radius;
     if (N > m && N > kTailMax) {

@@ -71,34 +71,67 @@ __device__ __forceinline__ float leaf_test(float3 a, float3 b, float3 c, const R
     return wt_test(a, b, c, r.o, w, backface, b1, b2);
 }
 
+// Persistent traversal: each warp owns a contiguous chunk of rays and advances every lane by one node or
+// one leaf per step; a lane whose ray finished takes the next ray of the chunk at the following step, so
+// lanes do not idle behind the warp's longest ray (most rays of a batch may finish at the root while a few
+// descend to the leaves).
 template <int LEAF, bool ANY, bool COUNT, int STACK>
-__device__ __forceinline__ void trace_one(const BNode* __restrict__ nodes, const float4* __restrict__ tris, int root,
-                                          int num_nodes, const dipl_ray* __restrict__ rays, int64_t i,
-                                          dipl_hit* __restrict__ hits, uint8_t* __restrict__ occluded, uint32_t flags,
-                                          uint32_t* __restrict__ err, unsigned& visits, unsigned& tests) {
-    const RayState r = load_ray(rays, i);
+__global__ void __launch_bounds__(kTraceThreads) trace_kernel(const BNode* __restrict__ nodes,
+                                                              const float4* __restrict__ tris, int root,
+                                                              int num_nodes, const dipl_ray* __restrict__ rays,
+                                                              int64_t n, int64_t chunk, dipl_hit* __restrict__ hits,
+                                                              uint8_t* __restrict__ occluded, uint32_t flags,
+                                                              unsigned long long* __restrict__ counters,
+                                                              uint32_t* __restrict__ err) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t beg = warp_id * chunk;
+    const int64_t end = min(n, beg + chunk);
     const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
+    const uint32_t lt_mask = lanemask_lt();
+    const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+    int64_t next = beg;  // next ray of the chunk (warp-uniform)
+    int64_t my = -1;     // this lane's ray, -1 when idle
+    RayState r{};
     WtRay w{};
-    if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(r.d);
-    float best_t = r.tmax, best_u = 0.0f, best_v = 0.0f;
+    float best_t = 0.0f, best_u = 0.0f, best_v = 0.0f;
     int best_prim = -1;
     bool found = false;
-    Stack<STACK> st;
-    int cur = (num_nodes >= 0) ? root : 0x7FFFFFFF;  // num_nodes < 0 marks an empty BVH
-    bool bad = false;
-    // Each node is entered at most once per ray; the limit only guards against a corrupted tree.
-    const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+    int cur = 0;
     uint32_t steps = 0;
-    while (cur != 0x7FFFFFFF) {
-        if (++steps > step_limit) {
-            bad = true;
-            break;
-        }
-        if (cur >= 0) {
-            if (cur >= num_nodes) {
-                bad = true;
-                break;
+    Stack<STACK> st;
+    unsigned visits = 0, tests = 0;
+    bool bad = false;
+    for (;;) {
+        // ---- refill idle lanes from the chunk --------------------------------------------------------
+        const bool idle = my < 0;
+        const uint32_t idle_mask = __ballot_sync(0xffffffffu, idle);
+        if (idle_mask) {
+            if (idle) {
+                const int64_t cand = next + __popc(idle_mask & lt_mask);
+                if (cand < end) {
+                    my = cand;
+                    r = load_ray(rays, my);
+                    if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(r.d);
+                    best_t = r.tmax, best_u = 0.0f, best_v = 0.0f, best_prim = -1, found = false;
+                    cur = num_nodes >= 0 ? root : 0x7FFFFFFF;
+                    st.sp = 0;
+                    steps = 0;
+                }
             }
+            next = min(end, next + (int64_t)__popc(idle_mask));
+        }
+        if (__all_sync(0xffffffffu, my < 0)) break;
+        if (my < 0) continue;
+
+        // ---- one step: an inner node or a leaf --------------------------------------------------------
+        bool finished = false;
+        if (cur == 0x7FFFFFFF) {
+            finished = true;  // empty BVH
+        } else if (++steps > step_limit || (cur >= 0 && cur >= num_nodes)) {
+            bad = true;       // only a corrupted tree gets here
+            finished = true;
+        } else if (cur >= 0) {
             const float4* np = reinterpret_cast<const float4*>(nodes + cur);
             const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
             const int4 d = __ldg(reinterpret_cast<const int4*>(np + 3));
@@ -111,23 +144,21 @@ __device__ __forceinline__ void trace_one(const BNode* __restrict__ nodes, const
                 const bool first0 = t0 <= t1;
                 if (st.sp >= STACK) {
                     bad = true;
-                    break;
+                    finished = true;
+                } else {
+                    st.ref[st.sp] = first0 ? d.y : d.x;
+                    st.t[st.sp] = first0 ? t1 : t0;
+                    ++st.sp;
+                    cur = first0 ? d.x : d.y;
                 }
-                st.ref[st.sp] = first0 ? d.y : d.x;
-                st.t[st.sp] = first0 ? t1 : t0;
-                ++st.sp;
-                cur = first0 ? d.x : d.y;
-                continue;
-            }
-            if (h0) {
+            } else if (h0) {
                 cur = d.x;
-                continue;
-            }
-            if (h1) {
+            } else if (h1) {
                 cur = d.y;
-                continue;
+            } else {
+                cur = -0x7FFFFFFF - 1;  // pop below
             }
-        } else {
+        } else if (cur != -0x7FFFFFFF - 1) {
             const int first = leaf_first(cur), cnt = leaf_count(cur);
             for (int k = 0; k < cnt; ++k) {
                 const float4* tp = tris + 3 * (int64_t)(first + k);
@@ -143,7 +174,8 @@ __device__ __forceinline__ void trace_one(const BNode* __restrict__ nodes, const
                         found = true;
                         break;
                     }
-                } else if (t > r.tmin && t < kInfinity && (t < best_t || (t == best_t && found && prim < best_prim))) {
+                } else if (t > r.tmin && t < kInfinity &&
+                           (t < best_t || (t == best_t && found && prim < best_prim))) {
                     best_t = t;
                     best_prim = prim;
                     best_u = b1;
@@ -151,72 +183,84 @@ __device__ __forceinline__ void trace_one(const BNode* __restrict__ nodes, const
                     found = true;
                 }
             }
-            if (ANY && found) break;
+            if (ANY && found) finished = true;
+            else cur = -0x7FFFFFFF - 1;  // pop below
         }
-        // pop the next entry that can still hold a better hit
-        cur = 0x7FFFFFFF;
-        const float lim = prune_limit(best_t);
-        while (st.sp > 0) {
-            --st.sp;
-            if (st.t[st.sp] <= lim) {
-                cur = st.ref[st.sp];
-                break;
+        if (!finished && cur == -0x7FFFFFFF - 1) {
+            // pop the next entry that can still hold a better hit
+            const float lim = prune_limit(best_t);
+            cur = 0x7FFFFFFF;
+            while (st.sp > 0) {
+                --st.sp;
+                if (st.t[st.sp] <= lim) {
+                    cur = st.ref[st.sp];
+                    break;
+                }
             }
+            if (cur == 0x7FFFFFFF) finished = true;
+        }
+        if (finished) {
+            if (ANY) {
+                occluded[my] = found ? 1 : 0;
+            } else {
+                int4 out;
+                out.x = found ? best_prim : -1;
+                out.y = __float_as_int(found ? best_t : __int_as_float(0x7F800000));
+                out.z = __float_as_int(found ? best_u : 0.0f);
+                out.w = __float_as_int(found ? best_v : 0.0f);
+                reinterpret_cast<int4*>(hits)[my] = out;
+            }
+            my = -1;
         }
     }
     if (bad) atomicOr(err, kErrStack);
-    if (ANY) {
-        occluded[i] = found ? 1 : 0;
-    } else {
-        int4 out;
-        out.x = found ? best_prim : -1;
-        out.y = __float_as_int(found ? best_t : __int_as_float(0x7F800000));
-        out.z = __float_as_int(found ? best_u : 0.0f);
-        out.w = __float_as_int(found ? best_v : 0.0f);
-        reinterpret_cast<int4*>(hits)[i] = out;
-    }
-}
-
-template <int LEAF, bool ANY, bool COUNT, int STACK>
-__global__ void __launch_bounds__(kTraceThreads) trace_kernel(const BNode* __restrict__ nodes,
-                                                              const float4* __restrict__ tris, int root,
-                                                              int num_nodes, const dipl_ray* __restrict__ rays,
-                                                              int64_t n, dipl_hit* __restrict__ hits,
-                                                              uint8_t* __restrict__ occluded, uint32_t flags,
-                                                              unsigned long long* __restrict__ counters,
-                                                              uint32_t* __restrict__ err) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    unsigned visits = 0, tests = 0;
-    if (i < n) trace_one<LEAF, ANY, COUNT, STACK>(nodes, tris, root, num_nodes, rays, i, hits, occluded, flags, err,
-                                                   visits, tests);
     if (COUNT) {
-        // every lane of the (full) warp reaches this point
         const unsigned v = __reduce_add_sync(0xffffffffu, visits);
         const unsigned t = __reduce_add_sync(0xffffffffu, tests);
-        if ((threadIdx.x & 31) == 0) {
+        if (lane == 0) {
             atomicAdd(&counters[0], (unsigned long long)v);
             atomicAdd(&counters[1], (unsigned long long)t);
         }
     }
 }
 
+template <typename K>
+int persistent_grid(K kernel) {
+    static int grid = 0;  // per instantiation
+    if (grid == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceThreads, 0);
+        grid = std::max(1, sms * std::max(1, per_sm));
+    }
+    return grid;
+}
+
+template <int LEAF, bool ANY, bool COUNT, int STACK>
+dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
+                         uint32_t flags, unsigned long long* counters, cudaStream_t s) {
+    auto kernel = trace_kernel<LEAF, ANY, COUNT, STACK>;
+    const int max_grid = persistent_grid(kernel);
+    const int64_t warps_needed = (n + 31) / 32;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(max_grid, (warps_needed * 32 + kTraceThreads - 1) /
+                                                                               kTraceThreads));
+    const int64_t warps = grid * (kTraceThreads / 32);
+    const int64_t chunk = (n + warps - 1) / warps;
+    const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
+    kernel<<<(unsigned)grid, kTraceThreads, 0, s>>>(static_cast<const BNode*>(b->nodes), b->tris, b->root, num_nodes,
+                                                   rays, n, chunk, hits, occ, flags, counters, b->d_err);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return DIPL_OK;
+}
+
 template <int LEAF, bool ANY, bool COUNT>
 dipl_status launch_trace_stack(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
                                uint32_t flags, unsigned long long* counters, cudaStream_t s) {
-    const unsigned grid = (unsigned)((n + kTraceThreads - 1) / kTraceThreads);
-    const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
-    const BNode* nodes = static_cast<const BNode*>(b->nodes);
-    if (b->depth < 64)
-        trace_kernel<LEAF, ANY, COUNT, 64><<<grid, kTraceThreads, 0, s>>>(nodes, b->tris, b->root, num_nodes, rays, n,
-                                                                          hits, occ, flags, counters, b->d_err);
-    else if (b->depth < 128)
-        trace_kernel<LEAF, ANY, COUNT, 128><<<grid, kTraceThreads, 0, s>>>(nodes, b->tris, b->root, num_nodes, rays,
-                                                                           n, hits, occ, flags, counters, b->d_err);
-    else
-        trace_kernel<LEAF, ANY, COUNT, 512><<<grid, kTraceThreads, 0, s>>>(nodes, b->tris, b->root, num_nodes, rays,
-                                                                           n, hits, occ, flags, counters, b->d_err); note_launches();
-    DIPL_CUDA(cudaGetLastError());
-    return DIPL_OK;
+    if (b->depth < 64) return launch_trace<LEAF, ANY, COUNT, 64>(b, rays, n, hits, occ, flags, counters, s);
+    if (b->depth < 128) return launch_trace<LEAF, ANY, COUNT, 128>(b, rays, n, hits, occ, flags, counters, s);
+    return launch_trace<LEAF, ANY, COUNT, 512>(b, rays, n, hits, occ, flags, counters, s);
 }
 
 }  // namespace
