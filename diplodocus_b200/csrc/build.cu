@@ -374,6 +374,107 @@ __device__ __forceinline__ void nn_search(const float4* __restrict__ slo, const 
     }
 }
 
+// Symmetric variant for the grid tiles: each pair (p, p+k) is evaluated once by the thread of its lower
+// position; the lower side keeps its running minimum in registers, the upper side receives its key by a
+// 64-bit shared-memory atomicMin. Keys are the oracle's (distance bits << 32 | gap << 2 | parity << 1 | side);
+// positions [q0, q1) get their nearest neighbour in nn[q - q0]; key is scratch of the same extent.
+template <int NT>
+__device__ __forceinline__ void nn_search_sym(const float4* __restrict__ slo, const float4* __restrict__ shi, int base,
+                                              int n, int q0, int q1, int r, int* __restrict__ nn,
+                                              unsigned long long* __restrict__ key) {
+    for (int q = q0 + (int)threadIdx.x; q < q1; q += NT) key[q - q0] = ~0ull;
+    __syncthreads();
+    const int p0 = max(q0 - r, 0);
+    for (int p = p0 + (int)threadIdx.x; p < q1; p += NT) {
+        const float4 a = slo[p - base], b = shi[p - base];
+        const int sg = __float_as_int(b.w);
+        const bool own = p >= q0;
+        const unsigned long long par = (unsigned long long)((p & 1) << 1);
+        unsigned long long best = ~0ull;
+        const int kmax = min(r, n - 1 - p);
+#pragma unroll 4
+        for (int k = 1; k <= kmax; ++k) {
+            const int j = p + k;
+            const float4 c = slo[j - base], e = shi[j - base];
+            if (__float_as_int(e.w) != sg) continue;
+            const float d = ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, e.x, e.y, e.z);
+            const unsigned long long kd = ((unsigned long long)__float_as_uint(d) << 32) |
+                                          ((unsigned long long)k << 2) | par;
+            const unsigned long long kp = kd | 1ull;  // seen from p: partner above (side 1)
+            best = kp < best ? kp : best;
+            if (j >= q0 && j < q1) atomicMin(&key[j - q0], kd);  // seen from j: partner below (side 0)
+        }
+        if (own && best != ~0ull) atomicMin(&key[p - q0], best);
+    }
+    __syncthreads();
+    for (int q = q0 + (int)threadIdx.x; q < q1; q += NT) {
+        const unsigned long long kq = key[q - q0];
+        int j = -1;
+        if (kq != ~0ull) {
+            const unsigned tie = (unsigned)kq;
+            const int gap = (int)(tie >> 2);
+            j = (tie & 1u) ? q + gap : q - gap;
+        }
+        nn[q - q0] = j;
+    }
+}
+
+// Tail variant: every position's candidates are split over P consecutive threads (P a power of two, up to
+// 16) when there are few clusters, then the per-thread minima are combined with a 64-bit min over the
+// oracle's key (distance bits << 32 | gap << 2 | parity << 1 | side). Each thread visits its own gaps in
+// increasing order, so its local strict-"<" minimum is its subset's key minimum.
+template <int NT>
+__device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, const float4* __restrict__ shi, int n,
+                                                int r, int* __restrict__ nn) {
+    int P = 1;
+    while (P < 16 && 2 * P * n <= NT) P *= 2;
+    const int sub = (int)threadIdx.x & (P - 1);
+    for (int base = (int)threadIdx.x / P; base < ((n + (NT / P) - 1) / (NT / P)) * (NT / P); base += NT / P) {
+        const int q = base;
+        unsigned long long key = ~0ull;
+        if (q < n) {
+            const float4 a = slo[q], b = shi[q];
+            const int sg = __float_as_int(b.w);
+            float bestd = __int_as_float(0x7F800000);
+            int bestj = -1;
+            auto consider = [&](int j) {
+                if (j < 0 || j >= n) return;
+                const float4 c = slo[j], e = shi[j];
+                if (__float_as_int(e.w) != sg) return;
+                const float d = ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, e.x, e.y, e.z);
+                if (d < bestd || bestj < 0) {
+                    bestd = d;
+                    bestj = j;
+                }
+            };
+            for (int k = 1 + sub; k <= r; k += P) {
+                const bool fwd_first = (k & 1) && !(q & 1);
+                consider(fwd_first ? q + k : q - k);
+                consider(fwd_first ? q - k : q + k);
+            }
+            if (bestj >= 0) {
+                const unsigned gap = (unsigned)abs(bestj - q);
+                const unsigned mn = (unsigned)min(bestj, q);
+                key = ((unsigned long long)__float_as_uint(bestd) << 32) |
+                      (unsigned long long)((gap << 2) | ((mn & 1u) << 1) | (bestj > q ? 1u : 0u));
+            }
+        }
+        for (int o = P / 2; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+            key = other < key ? other : key;
+        }
+        if (q < n && sub == 0) {
+            int j = -1;
+            if (key != ~0ull) {
+                const unsigned tie = (unsigned)key;
+                const int gap = (int)(tie >> 2);
+                j = (tie & 1u) ? q + gap : q - gap;
+            }
+            nn[q] = j;
+        }
+    }
+}
+
 // Writes internal node `knew` = merge of clusters (la, lb, li) and (ra, rb, ri); returns the merged cluster.
 __device__ __forceinline__ void emit_node(const PlocParams& P, int knew, const float4& la, const float4& lb,
                                           const int4& li, const float4& ra, const float4& rb, const int4& ri,
@@ -398,6 +499,7 @@ struct PlocSmem {
     float4 hi[W];  // max xyz, mesh index bits
     int4 info[W];  // count, first position, height
     int nn[T + 2 * kRadiusMax];
+    unsigned long long key[T + 2 * kRadiusMax];
     uint32_t warp_sum[B / 32];
     unsigned long long prefix;
     int ok;
@@ -421,7 +523,7 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     __syncthreads();
 
     const int q0 = max(s0 - r, 0), q1 = min(s0 + T + r, n);
-    nn_search<B>(s.lo, s.hi, w0, n, q0, q1, r, s.nn, q0);
+    nn_search_sym<B>(s.lo, s.hi, w0, n, q0, q1, r, s.nn, s.key);
     __syncthreads();
 
     // ---- merge decisions (blocked: kPlocIpt consecutive positions per thread) ----------------------
@@ -612,7 +714,7 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
         const float4* __restrict__ lo = s.lo[cur];
         const float4* __restrict__ hi = s.hi[cur];
         const int4* __restrict__ info = s.info[cur];
-        nn_search<kTailThreads>(lo, hi, 0, n, 0, n, r, s.nn, 0);
+        nn_search_split<kTailThreads>(lo, hi, n, r, s.nn);
         __syncthreads();
         const int ib = threadIdx.x * IPT;
         uint32_t keep_bits = 0, merge_bits = 0;
