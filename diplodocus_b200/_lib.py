@@ -26,7 +26,7 @@ EXPORTS = [
     "dipl_build_desc_init", "dipl_bvh_build", "dipl_bvh_build_batched", "dipl_bvh_trace_closest",
     "dipl_bvh_trace_closest_counted", "dipl_bvh_trace_any", "dipl_bvh_sah_cost", "dipl_bvh_get_info",
     "dipl_bvh_download_topology", "dipl_bvh_download_layout", "dipl_bvh_check_errors", "dipl_bvh_destroy", "dipl_compute_codes",
-    "dipl_radix_sort_pairs", "dipl_reintersect_f64", "dipl_trace_adjoint", "dipl_status_string",
+    "dipl_radix_sort_pairs", "dipl_radix_sort_pairs_noalloc", "dipl_reintersect_f64", "dipl_trace_adjoint", "dipl_status_string",
     "dipl_last_error", "dipl_abi_version", "dipl_kernel_launch_count",
 ]
 
@@ -79,6 +79,7 @@ def load(path: str = LIB_PATH):
         "dipl_bvh_destroy": (i32, [vp]),
         "dipl_compute_codes": (i32, [C.POINTER(BuildDesc), vp, vp]),
         "dipl_radix_sort_pairs": (i32, [vp, vp, vp, vp, i64, i32, i32, i32, i32, vp]),
+        "dipl_radix_sort_pairs_noalloc": (i32, [vp, vp, vp, vp, i64, i32, i32, i32, i32, vp]),
         "dipl_reintersect_f64": (i32, [vp, vp, vp, vp, vp, i64, vp, vp]),
         "dipl_trace_adjoint": (i32, [vp, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]),
         "dipl_status_string": (C.c_char_p, [i32]),

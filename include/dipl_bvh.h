@@ -190,6 +190,19 @@ DIPL_API dipl_status dipl_radix_sort_pairs(const void* d_keys_in, const uint32_t
                                   uint32_t* d_vals_out, int64_t n, int32_t key_bytes, int32_t begin_bit,
                                   int32_t end_bit, int32_t digit_bits, void* stream);
 
+/* No counterpart in the reference. The same sort as dipl_radix_sort_pairs for callers that may not
+ * allocate device memory (a host application that owns the whole GPU heap and gives plug-ins fixed
+ * buffers, or a loop that must not stall on cudaMalloc). Its scratch is one fixed array in the library's
+ * device image (about 5 MB on every GPU that loads the library, held until the process exits); no memory is
+ * allocated per call. At most 262,144 pairs (larger n: DIPL_ERR_INVALID_ARGUMENT). The first call on a
+ * device looks up the array's address, so make it before any stream capture. All calls on a device share
+ * the array: the call clears what must start at zero, but calls whose GPU work overlaps race on it, so
+ * order them. Synchronises `stream` at the end, like dipl_radix_sort_pairs. */
+DIPL_API dipl_status dipl_radix_sort_pairs_noalloc(const void* d_keys_in, const uint32_t* d_vals_in, void* d_keys_out,
+                                                   uint32_t* d_vals_out, int64_t n, int32_t key_bytes,
+                                                   int32_t begin_bit, int32_t end_bit, int32_t digit_bits,
+                                                   void* stream);
+
 /* FP64 oracle re-intersection (checking only): for each hit, t/u/v of the ray against triangle `prim`
  * of the original vertex arrays, in double precision (d_tuv: 3 doubles per ray; misses give +inf,0,0). */
 DIPL_API dipl_status dipl_reintersect_f64(const float* d_v0, const float* d_v1, const float* d_v2, const dipl_ray* d_rays,
