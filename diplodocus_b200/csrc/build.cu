@@ -998,8 +998,8 @@ __global__ void node_write_kernel(LayoutParams P, const MeshDesc* __restrict__ m
 struct RootInfo {
     int root_ref;
     int depth;
-    int num_leaves;
-    int pad;
+    int num_leaves;  // triangles under the root
+    int root_id;     // PLOC node id of the root
     double root_area;
     double leaf_cost;  // SAH cost contribution when the root itself is a leaf
 };
@@ -1032,6 +1032,7 @@ __global__ void roots_kernel(LayoutParams P, const float4* __restrict__ lo0, con
         ri.leaf_cost = ri.root_area * cnt;
     }
     ri.num_leaves = cnt;
+    ri.root_id = id;
     roots[k] = ri;
 }
 
@@ -1088,10 +1089,10 @@ static dipl_status validate_desc(const dipl_build_desc& d) {
     DIPL_CHECK_ARG(d.ploc_block_size == 0 || d.ploc_block_size == 128 || d.ploc_block_size == 256 ||
                        d.ploc_block_size == 512,
                    "ploc_block_size must be 0, 128, 256 or 512");
-    if (d.bv_type != DIPL_BV_AABB || d.layout != DIPL_LAYOUT_BINARY) {
-        set_last_error("SOBB and 8-wide layouts are not available in this build");
-        return DIPL_ERR_UNSUPPORTED;
-    }
+    DIPL_CHECK_ARG(d.bv_type == DIPL_BV_AABB || d.layout == DIPL_LAYOUT_BINARY,
+                   "SOBB bounding volumes use the binary layout");
+    DIPL_CHECK_ARG(d.layout != DIPL_LAYOUT_WIDE8_Q8 || d.max_triangles_per_leaf <= 5,
+                   "the 8-wide layout needs max_triangles_per_leaf <= 5 (at most 32 leaf triangles per node)");
     DIPL_CHECK_ARG(d.sort_digit_bits == 0 || d.sort_digit_bits == 6 || d.sort_digit_bits == 7 ||
                        d.sort_digit_bits == 8 || d.sort_digit_bits == 10,
                    "sort_digit_bits must be 0, 6, 7, 8 or 10");
@@ -1323,6 +1324,28 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     const int64_t inner_total = (int64_t)h_tail[0];
     const int iterations = (int)h_tail[1];
 
+    // ---- SOBB form: skewed oriented child boxes over the same layout ---------------------------------
+    SNode* snodes = nullptr;
+    if (d0.bv_type == DIPL_BV_SOBB) {
+        st = build_sobb(child, nlo, nhi, parent, leaf_start_of, owner_leaf, tris, nodes, rev_flags, (int)N, (int)K, L,
+                        d0.kdop_size, *storage, stream, d_err, &snodes);
+        if (st != DIPL_OK) return st;
+        if ((st = check_device_error(d_err, stream, "SOBB refit")) != DIPL_OK) return st;
+    }
+
+    // ---- precision form: 8-wide quantised layout over the same clustering ---------------------------
+    WNode* wnodes = nullptr;
+    float4* wtris = nullptr;
+    int64_t wcount = 0;
+    std::vector<int> wroots, wlevels;
+    if (d0.layout == DIPL_LAYOUT_WIDE8_Q8) {
+        std::vector<int> root_ids(m), root_counts(m);
+        for (int k = 0; k < m; ++k) root_ids[k] = h_roots[k].root_id, root_counts[k] = h_roots[k].num_leaves;
+        st = build_wide(child, nlo, nhi, leaf_start_of, tris, (int)N, L, root_ids, root_counts, *storage, stream,
+                        d_err, &wnodes, &wtris, &wcount, wroots, wlevels);
+        if (st != DIPL_OK) return st;
+    }
+
     std::vector<dipl_bvh*> made;
     for (int i = 0; i < count; ++i) {
         dipl_bvh* h = make_handle(i);
@@ -1345,6 +1368,18 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
             h->sah_area = ri.root_area;
             h->sah_sum = h_sah[2 * k] + ri.leaf_cost;
             h->num_leaves = 0;
+            if (d0.layout == DIPL_LAYOUT_WIDE8_Q8) {
+                h->root = wroots[k];
+                h->depth = wlevels[k];
+            }
+        }
+        if (d0.bv_type == DIPL_BV_SOBB) h->nodes = snodes;
+        if (d0.layout == DIPL_LAYOUT_WIDE8_Q8) {
+            h->nodes = wnodes;
+            h->tris = wtris;
+            h->node_size = sizeof(WNode);
+            h->node_capacity = wcount;
+            h->num_nodes = wcount;
         }
         out[i] = h;
         made.push_back(h);

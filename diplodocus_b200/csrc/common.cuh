@@ -46,16 +46,15 @@ struct __align__(16) BNode {
 };
 static_assert(sizeof(BNode) == 64, "BNode must be 64 bytes");
 
-// Binary SOBB node (80 bytes): per child three slab directions (indices into the direction table)
+// Binary SOBB node (64 bytes): per child three slab directions (indices into the direction table)
 // and the slab intervals along them.
 struct __align__(16) SNode {
     float4 a;  // left  lo0 hi0 lo1 hi1
     float4 b;  // left  lo2 hi2, right lo0 hi0
     float4 c;  // right lo1 hi1 lo2 hi2
     int4 d;    // left ref, right ref, left axes (3 x 8 bits), right axes (3 x 8 bits)
-    int4 e;    // unused padding to 80 bytes
 };
-static_assert(sizeof(SNode) == 80, "SNode must be 80 bytes");
+static_assert(sizeof(SNode) == 64, "SNode must be 64 bytes");
 
 // 8-wide node with 8-bit quantised child bounds (80 bytes), after Ylitie, Karras & Laine (HPG 2017).
 struct __align__(16) WNode {

@@ -1,15 +1,20 @@
-// Traversal of the SOBB and 8-wide quantised layouts (filled in by sobb.cu / wide.cu when built).
+// Dispatch of the traversals that are not the binary FP32-AABB one.
 #include "internal.h"
 
 namespace dipl {
 
-dipl_status trace_closest_ext(const dipl_bvh*, const dipl_ray*, int64_t, dipl_hit*, int, uint32_t,
-                              unsigned long long*, cudaStream_t) {
+dipl_status trace_closest_ext(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, int leaf_test,
+                              uint32_t flags, unsigned long long* counters, cudaStream_t s) {
+    if (b->layout == DIPL_LAYOUT_WIDE8_Q8) return trace_wide(b, rays, n, hits, nullptr, leaf_test, flags, counters, false, s);
+    if (b->bv_type == DIPL_BV_SOBB) return trace_sobb(b, rays, n, hits, nullptr, leaf_test, flags, counters, false, s);
     set_last_error("this layout is not available in this build");
     return DIPL_ERR_UNSUPPORTED;
 }
 
-dipl_status trace_any_ext(const dipl_bvh*, const dipl_ray*, int64_t, uint8_t*, int, uint32_t, cudaStream_t) {
+dipl_status trace_any_ext(const dipl_bvh* b, const dipl_ray* rays, int64_t n, uint8_t* occluded, int leaf_test,
+                          uint32_t flags, cudaStream_t s) {
+    if (b->layout == DIPL_LAYOUT_WIDE8_Q8) return trace_wide(b, rays, n, nullptr, occluded, leaf_test, flags, nullptr, true, s);
+    if (b->bv_type == DIPL_BV_SOBB) return trace_sobb(b, rays, n, nullptr, occluded, leaf_test, flags, nullptr, true, s);
     set_last_error("this layout is not available in this build");
     return DIPL_ERR_UNSUPPORTED;
 }

@@ -123,6 +123,23 @@ dipl_status trace_adjoint(const float* v0, const float* v1, const float* v2, con
                           const dipl_hit* hits, const float* dtuv, int64_t n, float* dv0, float* dv1, float* dv2,
                           float* dorig, float* ddir, cudaStream_t stream);
 
+// Precision form (wide.cu): 8-wide quantised layout built from the binary clustering, and its traversal.
+dipl_status build_wide(const int4* child, const float4* node_lo, const float4* node_hi, const int* leaf_start_of,
+                       const float4* btris, int N, int L, const std::vector<int>& root_ids,
+                       const std::vector<int>& root_counts, Storage& storage, cudaStream_t s, uint32_t* d_err,
+                       WNode** out_nodes, float4** out_tris, int64_t* out_num_nodes, std::vector<int>& out_root_refs,
+                       std::vector<int>& out_levels);
+dipl_status trace_wide(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, int leaf_test,
+                       uint32_t flags, unsigned long long* counters, bool any, cudaStream_t s);
+
+// SOBB form (sobb.cu): skewed oriented child boxes refitted over the binary layout, and their traversal.
+dipl_status build_sobb(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
+                       const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
+                       const uint32_t* rev_index, int N, int K, int L, int kdop_size, Storage& storage,
+                       cudaStream_t s, uint32_t* d_err, SNode** out_nodes);
+dipl_status trace_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, int leaf_test,
+                       uint32_t flags, unsigned long long* counters, bool any, cudaStream_t s);
+
 // Process-wide count of kernels this library has launched (for launch-count reporting).
 void note_launches(int n = 1);
 

@@ -1,0 +1,420 @@
+// SOBB form: skewed oriented bounding boxes (after Kacerik et al., "SOBB: Skewed Oriented Bounding Boxes
+// for Ray Tracing", 2025) refitted over the finished PLOC topology.
+//
+// Each child box is the intersection of three slabs along directions taken from a fixed table of up to 16
+// directions (kdop_size / 2 of them: the axes, the 4 corner diagonals, the 6 edge diagonals, 3 more). The
+// refit computes every node's k-DOP (the interval of projections on all table directions) bottom-up with
+// one thread per leaf (the second thread to reach a parent continues upwards), then each child keeps the
+// direction triple whose parallelepiped has the least surface area,
+//   SA(a, b, c) = 2 (w_a w_b + w_b w_c + w_c w_a) / |det(n_a, n_b, n_c)|,  w = interval width.
+// With the axes only (kdop_size 6) this is the AABB. Intervals are padded by 2^-20 of the subtree's
+// coordinate magnitude (more than the rounding of an FP32 projection), and the traversal widens each slab by
+// a bound on the rounding of the ray's own projection, so no hit of an exact test can be lost.
+#include <cmath>
+#include <mutex>
+
+#include "internal.h"
+#include "intersect.cuh"
+
+namespace dipl {
+
+namespace {
+
+constexpr int kDirs = 16;
+
+// Direction table (unnormalised components are fine: the same float values are used to build and to trace).
+__constant__ float c_dir[kDirs][3] = {
+    {1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f},
+    {0.57735026f, 0.57735026f, 0.57735026f}, {0.57735026f, 0.57735026f, -0.57735026f},
+    {0.57735026f, -0.57735026f, 0.57735026f}, {-0.57735026f, 0.57735026f, 0.57735026f},
+    {0.70710677f, 0.70710677f, 0.f}, {0.70710677f, -0.70710677f, 0.f}, {0.70710677f, 0.f, 0.70710677f},
+    {0.70710677f, 0.f, -0.70710677f}, {0.f, 0.70710677f, 0.70710677f}, {0.f, 0.70710677f, -0.70710677f},
+    {0.f, 0.52573111f, 0.85065081f}, {0.52573111f, 0.85065081f, 0.f}, {0.85065081f, 0.f, 0.52573111f},
+};
+
+// Triples of directions with |det| > 0.2 and 1/|det|, filled by the host once.
+constexpr int kMaxTriples = 560;
+__constant__ unsigned char c_triple[kMaxTriples][3];
+__constant__ float c_inv_det[kMaxTriples];
+
+struct Kdop {
+    float lo[kDirs], hi[kDirs];
+};
+
+__device__ __forceinline__ float proj(int i, float x, float y, float z) {
+    return __fmaf_rn(c_dir[i][0], x, __fmaf_rn(c_dir[i][1], y, __fmul_rn(c_dir[i][2], z)));
+}
+
+struct SobbIn {
+    const int4* child;
+    const float4* node_lo;
+    const float4* node_hi;
+    const int* parent;
+    const int* leaf_start_of;
+    const float4* btris;
+    int N;
+    int L;
+    int dirs;
+};
+
+__device__ __forceinline__ int scount(const SobbIn& S, int id) {
+    return id < S.N ? 1 : __float_as_int(S.node_lo[id - S.N].w);
+}
+
+// k-DOP of a final leaf from its triangles, then up the tree: the second arriver at a parent merges.
+__global__ void kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf, Kdop* __restrict__ kdop,
+                                  float* __restrict__ mag, unsigned* __restrict__ arrivals, const uint32_t* err) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.N || *err != 0u) return;
+    int x = owner_leaf[p];
+    if (x < 0) return;
+    const int cnt = scount(S, x);
+    const float4* t = S.btris + 3 * (long long)S.leaf_start_of[x];
+    Kdop k;
+    float m = 0.0f;
+    for (int i = 0; i < S.dirs; ++i) k.lo[i] = __int_as_float(0x7F800000), k.hi[i] = __int_as_float(0xFF800000);
+    for (int v = 0; v < 3 * cnt; ++v) {
+        const float4 q = t[v];
+        m = fmaxf(m, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
+        for (int i = 0; i < S.dirs; ++i) {
+            const float d = proj(i, q.x, q.y, q.z);
+            k.lo[i] = fminf(k.lo[i], d);
+            k.hi[i] = fmaxf(k.hi[i], d);
+        }
+    }
+    kdop[x] = k;
+    mag[x] = m;
+    for (int guard = 0; guard < 4096; ++guard) {
+        __threadfence();
+        const int par = S.parent[x];
+        if (par < 0) return;
+        if (atomicAdd(&arrivals[par - S.N], 1u) == 0u) return;  // the sibling is not done yet
+        __threadfence();
+        const int4 c = S.child[par - S.N];
+        // the sibling's k-DOP was written by another SM: read through L2 (no stale L1 lines)
+        const float* a = reinterpret_cast<const float*>(kdop + c.x);
+        const float* b = reinterpret_cast<const float*>(kdop + c.y);
+        for (int i = 0; i < S.dirs; ++i) {
+            k.lo[i] = fminf(__ldcg(a + i), __ldcg(b + i));
+            k.hi[i] = fmaxf(__ldcg(a + kDirs + i), __ldcg(b + kDirs + i));
+        }
+        m = fmaxf(__ldcg(mag + c.x), __ldcg(mag + c.y));
+        kdop[par] = k;
+        mag[par] = m;
+        x = par;
+    }
+}
+
+__device__ __forceinline__ void best_sobb(const Kdop& k, float m, int dirs, int triples, int axes[3], float lo[3],
+                                          float hi[3]) {
+    float best = __int_as_float(0x7F800000);
+    int bt = 0;
+    for (int t = 0; t < triples; ++t) {
+        const int a = c_triple[t][0], b = c_triple[t][1], c = c_triple[t][2];
+        if (a >= dirs || b >= dirs || c >= dirs) continue;
+        const float wa = k.hi[a] - k.lo[a], wb = k.hi[b] - k.lo[b], wc = k.hi[c] - k.lo[c];
+        const float sa = (wa * wb + wb * wc + wc * wa) * c_inv_det[t];
+        if (sa < best) {
+            best = sa;
+            bt = t;
+        }
+    }
+    const float pad = m * 9.5367431640625e-07f + 1e-30f;
+    for (int j = 0; j < 3; ++j) {
+        axes[j] = c_triple[bt][j];
+        lo[j] = k.lo[axes[j]] - pad;
+        hi[j] = k.hi[axes[j]] + pad;
+    }
+}
+
+__global__ void sobb_node_kernel(SobbIn S, const BNode* __restrict__ bnodes, const uint32_t* __restrict__ rev_index,
+                                 int num_inner, const Kdop* __restrict__ kdop, const float* __restrict__ mag,
+                                 int triples, SNode* __restrict__ snodes, const uint32_t* err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= num_inner || *err != 0u) return;
+    if (__float_as_int(S.node_lo[k].w) < S.L) return;
+    const int f = (int)rev_index[num_inner - 1 - k];
+    const int4 c = S.child[k];
+    int ax[2][3];
+    float lo[2][3], hi[2][3];
+    for (int s = 0; s < 2; ++s) {
+        const int id = s == 0 ? c.x : c.y;
+        best_sobb(kdop[id], mag[id], S.dirs, triples, ax[s], lo[s], hi[s]);
+    }
+    SNode nd;
+    nd.a = make_float4(lo[0][0], hi[0][0], lo[0][1], hi[0][1]);
+    nd.b = make_float4(lo[0][2], hi[0][2], lo[1][0], hi[1][0]);
+    nd.c = make_float4(lo[1][1], hi[1][1], lo[1][2], hi[1][2]);
+    const int4 refs = bnodes[f].d;  // the same references as the binary layout
+    nd.d = make_int4(refs.x, refs.y, ax[0][0] | (ax[0][1] << 8) | (ax[0][2] << 16),
+                     ax[1][0] | (ax[1][1] << 8) | (ax[1][2] << 16));
+    snodes[f] = nd;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Traversal: the ray's projections on the table directions are computed once per ray into shared memory.
+// ------------------------------------------------------------------------------------------------
+constexpr int kSThreads = 128;
+constexpr float kSSlabWiden = 1e-6f;
+constexpr float kSPruneSlack = 1e-5f;
+
+template <int LEAF>
+__device__ __forceinline__ float sleaf_test(float3 a, float3 b, float3 c, float3 o, float3 d, const WtRay& w,
+                                            bool backface, float& b1, float& b2) {
+    if (LEAF == DIPL_LEAF_REF_MT) return mt_ref(a, b, c, o, d, backface, b1, b2);
+    return wt_test(a, b, c, o, w, backface, b1, b2);
+}
+
+template <int LEAF, bool ANY, bool COUNT, int STACK>
+__global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __restrict__ nodes,
+                                                               const float4* __restrict__ tris, int root,
+                                                               int num_nodes, int dirs, const dipl_ray* __restrict__ rays,
+                                                               int64_t n, dipl_hit* __restrict__ hits,
+                                                               uint8_t* __restrict__ occluded, uint32_t flags,
+                                                               unsigned long long* __restrict__ counters,
+                                                               uint32_t* __restrict__ err) {
+    __shared__ float s_o[kDirs][kSThreads];
+    __shared__ float s_inv[kDirs][kSThreads];
+    __shared__ float s_tol[kDirs][kSThreads];
+    __shared__ float s_rel[kDirs][kSThreads];
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    unsigned visits = 0, tests = 0;
+    if (i < n) {
+        const int tid = threadIdx.x;
+        const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * i;
+        const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
+        const float3 o = make_float3(ra.x, ra.y, ra.z), d = make_float3(rb.x, rb.y, rb.z);
+        const float tmin = ra.w, tmax = rb.w;
+        const float omag = fabsf(o.x) + fabsf(o.y) + fabsf(o.z);
+        const float dmag = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+        for (int k = 0; k < dirs; ++k) {
+            const float dk = proj(k, d.x, d.y, d.z);
+            const float inv = __frcp_rn(fabsf(dk) < 1e-20f ? copysignf(1e-20f, dk) : dk);
+            s_o[k][tid] = proj(k, o.x, o.y, o.z);
+            s_inv[k][tid] = inv;
+            // rounding of the projected origin as a distance along the ray (absolute), and of the projected
+            // direction as a relative error of every distance on this slab (large for grazing slabs)
+            s_tol[k][tid] = omag * 4.0e-7f * fabsf(inv);
+            s_rel[k][tid] = kSSlabWiden + dmag * 4.0e-7f * fabsf(inv);
+        }
+        const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
+        WtRay w{};
+        if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(d);
+        float best_t = tmax, best_u = 0.0f, best_v = 0.0f;
+        int best_prim = -1;
+        bool found = false, bad = false;
+        int sref[STACK];
+        float st[STACK];
+        int sp = 0;
+        int cur = num_nodes >= 0 ? root : 0x7FFFFFFF;
+        uint32_t steps = 0;
+        const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+        auto slab_box = [&](int axes, float l0, float h0, float l1, float h1, float l2, float h2, float lim) {
+            float tn = __int_as_float(0xFF800000), tf = __int_as_float(0x7F800000);
+            const float ls[3] = {l0, l1, l2}, hs[3] = {h0, h1, h2};
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int k = (axes >> (8 * j)) & 0xFF;
+                const float ok = s_o[k][tid], inv = s_inv[k][tid], tol = s_tol[k][tid], rel = s_rel[k][tid];
+                const float t0 = __fmul_rn(__fsub_rn(ls[j], ok), inv), t1 = __fmul_rn(__fsub_rn(hs[j], ok), inv);
+                const float a0 = fminf(t0, t1), a1 = fmaxf(t0, t1);
+                tn = fmaxf(tn, a0 - fabsf(a0) * rel - tol);
+                tf = fminf(tf, a1 + fabsf(a1) * rel + tol);
+            }
+            return (tn <= tf && tf >= tmin && tn <= lim) ? tn : __int_as_float(0x7F800000);
+        };
+        while (cur != 0x7FFFFFFF) {
+            if (++steps > step_limit) {
+                bad = true;
+                break;
+            }
+            if (cur >= 0) {
+                if (cur >= num_nodes) {
+                    bad = true;
+                    break;
+                }
+                const float4* np = reinterpret_cast<const float4*>(nodes + cur);
+                const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+                const int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
+                if (COUNT) ++visits;
+                const float lim = best_t + fabsf(best_t) * kSPruneSlack;
+                const float t0 = slab_box(dd.z, a.x, a.y, a.z, a.w, b.x, b.y, lim);
+                const float t1 = slab_box(dd.w, b.z, b.w, c.x, c.y, c.z, c.w, lim);
+                const bool h0 = t0 != __int_as_float(0x7F800000), h1 = t1 != __int_as_float(0x7F800000);
+                if (h0 && h1) {
+                    const bool first0 = t0 <= t1;
+                    if (sp >= STACK) {
+                        bad = true;
+                        break;
+                    }
+                    sref[sp] = first0 ? dd.y : dd.x;
+                    st[sp] = first0 ? t1 : t0;
+                    ++sp;
+                    cur = first0 ? dd.x : dd.y;
+                    continue;
+                }
+                if (h0) {
+                    cur = dd.x;
+                    continue;
+                }
+                if (h1) {
+                    cur = dd.y;
+                    continue;
+                }
+            } else {
+                const int first = leaf_first(cur), cnt = leaf_count(cur);
+                for (int k = 0; k < cnt; ++k) {
+                    const float4* tp = tris + 3 * (int64_t)(first + k);
+                    const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+                    const int prim = __float_as_int(p0.w);
+                    float b1 = 0.0f, b2 = 0.0f;
+                    const float t = sleaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
+                                                     make_float3(p2.x, p2.y, p2.z), o, d, w, backface, b1, b2);
+                    if (COUNT) ++tests;
+                    if (ANY) {
+                        if (t > tmin && t < tmax && t < kInfinity) {
+                            found = true;
+                            break;
+                        }
+                    } else if (t > tmin && t < kInfinity && (t < best_t || (t == best_t && found && prim < best_prim))) {
+                        best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
+                    }
+                }
+                if (ANY && found) break;
+            }
+            cur = 0x7FFFFFFF;
+            const float lim = best_t + fabsf(best_t) * kSPruneSlack;
+            while (sp > 0) {
+                --sp;
+                if (st[sp] <= lim) {
+                    cur = sref[sp];
+                    break;
+                }
+            }
+        }
+        if (bad) atomicOr(err, kErrStack);
+        if (ANY) {
+            occluded[i] = found ? 1 : 0;
+        } else {
+            int4 out;
+            out.x = found ? best_prim : -1;
+            out.y = __float_as_int(found ? best_t : __int_as_float(0x7F800000));
+            out.z = __float_as_int(found ? best_u : 0.0f);
+            out.w = __float_as_int(found ? best_v : 0.0f);
+            reinterpret_cast<int4*>(hits)[i] = out;
+        }
+    }
+    if (COUNT) {
+        const unsigned v = __reduce_add_sync(0xffffffffu, visits);
+        const unsigned t = __reduce_add_sync(0xffffffffu, tests);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&counters[0], (unsigned long long)v);
+            atomicAdd(&counters[1], (unsigned long long)t);
+        }
+    }
+}
+
+template <int LEAF, bool ANY, bool COUNT, int STACK>
+dipl_status launch_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
+                        uint32_t flags, unsigned long long* counters, cudaStream_t s) {
+    const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
+    sobb_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kSThreads - 1) / kSThreads), kSThreads, 0, s>>>(
+        static_cast<const SNode*>(b->nodes), b->tris, b->root, num_nodes, b->kdop / 2, rays, n, hits, occ, flags,
+        counters, b->d_err);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return DIPL_OK;
+}
+
+template <int LEAF, bool ANY, bool COUNT>
+dipl_status launch_sobb_stack(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
+                              uint32_t flags, unsigned long long* counters, cudaStream_t s) {
+    if (b->depth < 64) return launch_sobb<LEAF, ANY, COUNT, 64>(b, rays, n, hits, occ, flags, counters, s);
+    if (b->depth < 128) return launch_sobb<LEAF, ANY, COUNT, 128>(b, rays, n, hits, occ, flags, counters, s);
+    return launch_sobb<LEAF, ANY, COUNT, 512>(b, rays, n, hits, occ, flags, counters, s);
+}
+
+std::once_flag g_triples_once;
+int g_triples = 0;
+
+dipl_status upload_triples() {
+    static const float dirs[kDirs][3] = {
+        {1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f},
+        {0.57735026f, 0.57735026f, 0.57735026f}, {0.57735026f, 0.57735026f, -0.57735026f},
+        {0.57735026f, -0.57735026f, 0.57735026f}, {-0.57735026f, 0.57735026f, 0.57735026f},
+        {0.70710677f, 0.70710677f, 0.f}, {0.70710677f, -0.70710677f, 0.f}, {0.70710677f, 0.f, 0.70710677f},
+        {0.70710677f, 0.f, -0.70710677f}, {0.f, 0.70710677f, 0.70710677f}, {0.f, 0.70710677f, -0.70710677f},
+        {0.f, 0.52573111f, 0.85065081f}, {0.52573111f, 0.85065081f, 0.f}, {0.85065081f, 0.f, 0.52573111f},
+    };
+    unsigned char tri[kMaxTriples][3];
+    float inv[kMaxTriples];
+    int nt = 0;
+    for (int a = 0; a < kDirs; ++a)
+        for (int b = a + 1; b < kDirs; ++b)
+            for (int c = b + 1; c < kDirs; ++c) {
+                const float* A = dirs[a];
+                const float* B = dirs[b];
+                const float* Cc = dirs[c];
+                const double det = (double)A[0] * (B[1] * Cc[2] - B[2] * Cc[1]) -
+                                   (double)A[1] * (B[0] * Cc[2] - B[2] * Cc[0]) +
+                                   (double)A[2] * (B[0] * Cc[1] - B[1] * Cc[0]);
+                if (std::fabs(det) < 0.2) continue;
+                tri[nt][0] = (unsigned char)a, tri[nt][1] = (unsigned char)b, tri[nt][2] = (unsigned char)c;
+                inv[nt] = (float)(1.0 / std::fabs(det));
+                ++nt;
+            }
+    DIPL_CUDA(cudaMemcpyToSymbol(c_triple, tri, sizeof(tri)));
+    DIPL_CUDA(cudaMemcpyToSymbol(c_inv_det, inv, sizeof(inv)));
+    g_triples = nt;
+    return DIPL_OK;
+}
+
+}  // namespace
+
+// Refits SOBB child boxes over the binary layout (bnodes, final inner indices rev_index) into snodes.
+dipl_status build_sobb(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
+                       const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
+                       const uint32_t* rev_index, int N, int K, int L, int kdop_size, Storage& storage,
+                       cudaStream_t s, uint32_t* d_err, SNode** out_nodes) {
+    dipl_status st = DIPL_OK;
+    std::call_once(g_triples_once, [&] { st = upload_triples(); });
+    if (st != DIPL_OK) return st;
+    ScratchArena scratch(s);
+    Kdop* kdop;
+    float* mag;
+    unsigned* arrivals;
+    SNode* snodes;
+    const int Kalloc = std::max(K, 1);
+    if ((st = scratch.alloc(&kdop, (size_t)N + Kalloc)) != DIPL_OK || (st = scratch.alloc(&mag, (size_t)N + Kalloc)) != DIPL_OK ||
+        (st = scratch.alloc(&arrivals, Kalloc)) != DIPL_OK || (st = storage.alloc(&snodes, Kalloc)) != DIPL_OK)
+        return st;
+    DIPL_CUDA(cudaMemsetAsync(arrivals, 0, sizeof(unsigned) * Kalloc, s));
+    SobbIn S{child, node_lo, node_hi, parent, leaf_start_of, btris, N, L, kdop_size / 2};
+    kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, kdop, mag, arrivals, d_err);
+    note_launches();
+    if (K > 0) {
+        sobb_node_kernel<<<(unsigned)((K + 255) / 256), 256, 0, s>>>(S, bnodes, rev_index, K, kdop, mag, g_triples,
+                                                                      snodes, d_err);
+        note_launches();
+    }
+    DIPL_CUDA(cudaGetLastError());
+    *out_nodes = snodes;
+    return DIPL_OK;
+}
+
+dipl_status trace_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, int leaf_test,
+                       uint32_t flags, unsigned long long* counters, bool any, cudaStream_t s) {
+    if (any)
+        return leaf_test == DIPL_LEAF_REF_MT
+                   ? launch_sobb_stack<DIPL_LEAF_REF_MT, true, false>(b, rays, n, nullptr, occ, flags, nullptr, s)
+                   : launch_sobb_stack<DIPL_LEAF_WATERTIGHT, true, false>(b, rays, n, nullptr, occ, flags, nullptr, s);
+    if (counters)
+        return leaf_test == DIPL_LEAF_REF_MT
+                   ? launch_sobb_stack<DIPL_LEAF_REF_MT, false, true>(b, rays, n, hits, nullptr, flags, counters, s)
+                   : launch_sobb_stack<DIPL_LEAF_WATERTIGHT, false, true>(b, rays, n, hits, nullptr, flags, counters, s);
+    return leaf_test == DIPL_LEAF_REF_MT
+               ? launch_sobb_stack<DIPL_LEAF_REF_MT, false, false>(b, rays, n, hits, nullptr, flags, nullptr, s)
+               : launch_sobb_stack<DIPL_LEAF_WATERTIGHT, false, false>(b, rays, n, hits, nullptr, flags, nullptr, s);
+}
+
+}  // namespace dipl

@@ -1,0 +1,500 @@
+// Precision form: 8-wide BVH with 8-bit conservatively quantised child bounds (80-byte nodes, after Ylitie,
+// Karras & Laine, "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017) and
+// FP32 triangles re-tested at the leaves.
+//
+// Collapse: every wide node starts from one binary PLOC node with at least L triangles and repeatedly opens
+// its child of largest surface area that is itself such a node, until it has 8 children or only leaves.
+// Levels are built breadth first (one collapse kernel, two scans and one write kernel per level), so the
+// inner children of a node are contiguous (child_base + rank) and its leaves' triangles are contiguous
+// (tri_base + offset).
+//
+// Quantisation: per node an origin p (the min corner of the padded children) and per axis a power-of-two
+// scale 2^e with extent / 2^e <= 255; child bounds q_lo = floor, q_hi = ceil, then adjusted until the FP32
+// decode fmaf(q, 2^e, p) lies outside the padded child box. The traversal decodes with the same fmaf, so
+// every decoded box contains its (already padded) child box: no ray can lose a hit against the FP32 nodes.
+#include "internal.h"
+#include "intersect.cuh"
+
+namespace dipl {
+namespace {
+
+constexpr int kWideThreads = 256;
+
+struct WideIn {
+    const int4* child;
+    const float4* node_lo;
+    const float4* node_hi;
+    const int* leaf_start_of;  // binary leaf range start by node id
+    const float4* btris;       // binary leaf triangles
+    int N;
+    int L;
+};
+
+__device__ __forceinline__ int wcount(const WideIn& W, int id) {
+    return id < W.N ? 1 : __float_as_int(W.node_lo[id - W.N].w);
+}
+
+__device__ __forceinline__ void wbox(const WideIn& W, int id, float3& lo, float3& hi) {
+    if (id < W.N) {
+        const float4* t = W.btris + 3 * (long long)W.leaf_start_of[id];
+        const float4 a = t[0], b = t[1], c = t[2];
+        lo = make_float3(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z));
+        hi = make_float3(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z));
+    } else {
+        const float4 a = W.node_lo[id - W.N], b = W.node_hi[id - W.N];
+        lo = make_float3(a.x, a.y, a.z);
+        hi = make_float3(b.x, b.y, b.z);
+    }
+}
+
+__device__ __forceinline__ float wpad_down(float lo, float hi) {
+    const float m = fmaxf(fabsf(lo), fabsf(hi));
+    return lo - (m * 9.5367431640625e-07f + 1e-30f);
+}
+__device__ __forceinline__ float wpad_up(float lo, float hi) {
+    const float m = fmaxf(fabsf(lo), fabsf(hi));
+    return hi + (m * 9.5367431640625e-07f + 1e-30f);
+}
+
+// One thread per frontier node: the collapsed child list (binary node ids, inner ones first in list order).
+__global__ void wide_collapse_kernel(WideIn W, const int* __restrict__ frontier, int n_front,
+                                     int* __restrict__ kids /*8 per entry*/, uint32_t* __restrict__ n_inner,
+                                     uint32_t* __restrict__ n_tris, const uint32_t* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_front) return;
+    if (*err != 0u) {
+        n_inner[i] = 0;
+        n_tris[i] = 0;
+        return;
+    }
+    const int x = frontier[i];
+    const int4 c = W.child[x - W.N];
+    int list[8];
+    int cnt = 2;
+    list[0] = c.x;
+    list[1] = c.y;
+    while (cnt < 8) {
+        int best = -1;
+        double best_area = -1.0;
+        for (int k = 0; k < cnt; ++k) {
+            const int id = list[k];
+            if (id < W.N || wcount(W, id) < W.L) continue;
+            float3 lo, hi;
+            wbox(W, id, lo, hi);
+            const double dx = (double)hi.x - lo.x, dy = (double)hi.y - lo.y, dz = (double)hi.z - lo.z;
+            const double area = dx * dy + dy * dz + dz * dx;
+            if (area > best_area) {
+                best_area = area;
+                best = k;
+            }
+        }
+        if (best < 0) break;
+        const int4 cc = W.child[list[best] - W.N];
+        list[best] = cc.x;
+        list[cnt++] = cc.y;
+    }
+    uint32_t ni = 0, nt = 0;
+    for (int k = 0; k < 8; ++k) {
+        const int id = k < cnt ? list[k] : -1;
+        kids[8 * i + k] = id;
+        if (id < 0) continue;
+        const int n = wcount(W, id);
+        if (n >= W.L) ++ni;
+        else nt += (uint32_t)n;
+    }
+    n_inner[i] = ni;
+    n_tris[i] = nt;
+}
+
+__device__ __forceinline__ void quantise_axis(float p, float ext, const float* lo, const float* hi, int cnt,
+                                              unsigned char* qlo, unsigned char* qhi, unsigned char& ebiased) {
+    int e = -126;
+    if (ext > 0.0f) {
+        int ex = 0;
+        frexpf(ext / 255.0f, &ex);  // ext/255 = m * 2^ex, m in [0.5, 1)
+        e = max(-126, min(127, ex));
+    }
+    for (int attempt = 0; attempt < 4; ++attempt, e = min(127, e + 1)) {
+        const float scale = ldexpf(1.0f, e);
+        bool ok = true;
+        for (int k = 0; k < 8; ++k) {
+            if (k >= cnt) {
+                qlo[k] = 0, qhi[k] = 0;
+                continue;
+            }
+            float a = floorf((lo[k] - p) / scale);
+            float b = ceilf((hi[k] - p) / scale);
+            a = fminf(fmaxf(a, 0.0f), 255.0f);
+            b = fminf(fmaxf(b, 0.0f), 255.0f);
+            while (a > 0.0f && __fmaf_rn(a, scale, p) > lo[k]) a -= 1.0f;
+            while (b < 255.0f && __fmaf_rn(b, scale, p) < hi[k]) b += 1.0f;
+            if (__fmaf_rn(a, scale, p) > lo[k] || __fmaf_rn(b, scale, p) < hi[k]) ok = false;
+            qlo[k] = (unsigned char)a;
+            qhi[k] = (unsigned char)b;
+        }
+        if (ok) break;
+    }
+    ebiased = (unsigned char)(e + 127);
+}
+
+__global__ void wide_write_kernel(WideIn W, const int* __restrict__ frontier, int n_front,
+                                  const int* __restrict__ kids, const uint32_t* __restrict__ inner_prefix,
+                                  const uint32_t* __restrict__ tri_prefix, int base, int next_base, int tri_next,
+                                  WNode* __restrict__ nodes, float4* __restrict__ tris, int* __restrict__ frontier_out,
+                                  const uint32_t* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_front || *err != 0u) return;
+    const int child_base = next_base + (int)inner_prefix[i];
+    const int tri_base = tri_next + (int)tri_prefix[i];
+    float lo[3][8], hi[3][8];
+    int cnt = 0;
+    int ids[8];
+    for (int k = 0; k < 8; ++k) {
+        ids[k] = kids[8 * i + k];
+        if (ids[k] >= 0) cnt = k + 1;
+    }
+    float3 p = make_float3(__int_as_float(0x7F800000), __int_as_float(0x7F800000), __int_as_float(0x7F800000));
+    float3 q = make_float3(-p.x, -p.y, -p.z);
+    for (int k = 0; k < cnt; ++k) {
+        float3 l, h;
+        wbox(W, ids[k], l, h);
+        lo[0][k] = wpad_down(l.x, h.x), hi[0][k] = wpad_up(l.x, h.x);
+        lo[1][k] = wpad_down(l.y, h.y), hi[1][k] = wpad_up(l.y, h.y);
+        lo[2][k] = wpad_down(l.z, h.z), hi[2][k] = wpad_up(l.z, h.z);
+        p = make_float3(fminf(p.x, lo[0][k]), fminf(p.y, lo[1][k]), fminf(p.z, lo[2][k]));
+        q = make_float3(fmaxf(q.x, hi[0][k]), fmaxf(q.y, hi[1][k]), fmaxf(q.z, hi[2][k]));
+    }
+    WNode nd;
+    nd.px = p.x, nd.py = p.y, nd.pz = p.z;
+    quantise_axis(p.x, q.x - p.x, lo[0], hi[0], cnt, nd.qlox, nd.qhix, nd.ex);
+    quantise_axis(p.y, q.y - p.y, lo[1], hi[1], cnt, nd.qloy, nd.qhiy, nd.ey);
+    quantise_axis(p.z, q.z - p.z, lo[2], hi[2], cnt, nd.qloz, nd.qhiz, nd.ez);
+    nd.child_base = child_base;
+    nd.tri_base = tri_base;
+    unsigned char imask = 0;
+    int rank = 0, toff = 0;
+    for (int k = 0; k < 8; ++k) {
+        nd.meta[k] = 0;
+        if (k >= cnt) continue;
+        const int id = ids[k];
+        const int n = wcount(W, id);
+        if (n >= W.L) {
+            imask |= (unsigned char)(1u << k);
+            frontier_out[(int)inner_prefix[i] + rank] = id;
+            nd.meta[k] = (unsigned char)rank;
+            ++rank;
+        } else {
+            nd.meta[k] = (unsigned char)((n << 5) | toff);
+            const float4* src = W.btris + 3 * (long long)W.leaf_start_of[id];
+            float4* dst = tris + 3 * (long long)(tri_base + toff);
+            for (int t = 0; t < 3 * n; ++t) dst[t] = src[t];
+            toff += n;
+        }
+    }
+    nd.imask = imask;
+    nodes[base + i] = nd;
+}
+
+__global__ void copy_tris_kernel(const float4* __restrict__ src, float4* __restrict__ dst, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 3 * count) dst[i] = src[i];
+}
+
+// ------------------------------------------------------------------------------------------------
+// Traversal.
+// ------------------------------------------------------------------------------------------------
+constexpr int kWTraceThreads = 128;
+constexpr float kWSlabWiden = 1e-6f;
+constexpr float kWPruneSlack = 1e-5f;
+
+struct WRay {
+    float3 o, d, inv;
+    float tmin, tmax;
+};
+
+template <int LEAF>
+__device__ __forceinline__ float wleaf_test(float3 a, float3 b, float3 c, const WRay& r, const WtRay& w, bool backface,
+                                            float& b1, float& b2) {
+    if (LEAF == DIPL_LEAF_REF_MT) return mt_ref(a, b, c, r.o, r.d, backface, b1, b2);
+    return wt_test(a, b, c, r.o, w, backface, b1, b2);
+}
+
+template <int LEAF, bool ANY, bool COUNT, int STACK>
+__global__ void __launch_bounds__(kWTraceThreads) wide_trace_kernel(
+    const WNode* __restrict__ nodes, const float4* __restrict__ tris, int root, int num_nodes,
+    const dipl_ray* __restrict__ rays, int64_t n, dipl_hit* __restrict__ hits, uint8_t* __restrict__ occluded,
+    uint32_t flags, unsigned long long* __restrict__ counters, uint32_t* __restrict__ err) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    unsigned visits = 0, tests = 0;
+    if (i < n) {
+        const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * i;
+        const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
+        WRay r;
+        r.o = make_float3(ra.x, ra.y, ra.z);
+        r.d = make_float3(rb.x, rb.y, rb.z);
+        r.tmin = ra.w;
+        r.tmax = rb.w;
+        auto safe = [](float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; };
+        r.inv = make_float3(__frcp_rn(safe(r.d.x)), __frcp_rn(safe(r.d.y)), __frcp_rn(safe(r.d.z)));
+        const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
+        WtRay w{};
+        if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(r.d);
+        float best_t = r.tmax, best_u = 0.0f, best_v = 0.0f;
+        int best_prim = -1;
+        bool found = false, bad = false;
+        int sref[STACK];
+        float st[STACK];
+        int sp = 0;
+        int cur = num_nodes >= 0 ? root : 0x7FFFFFFF;
+        uint32_t steps = 0;
+        const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+        auto test_range = [&](int first, int count) {
+            for (int k = 0; k < count; ++k) {
+                const float4* tp = tris + 3 * (int64_t)(first + k);
+                const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+                const int prim = __float_as_int(p0.w);
+                float b1 = 0.0f, b2 = 0.0f;
+                const float t = wleaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
+                                                 make_float3(p2.x, p2.y, p2.z), r, w, backface, b1, b2);
+                if (COUNT) ++tests;
+                if (ANY) {
+                    if (t > r.tmin && t < r.tmax && t < kInfinity) {
+                        found = true;
+                        return;
+                    }
+                } else if (t > r.tmin && t < kInfinity &&
+                           (t < best_t || (t == best_t && found && prim < best_prim))) {
+                    best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
+                }
+            }
+        };
+        while (cur != 0x7FFFFFFF) {
+            if (++steps > step_limit) {
+                bad = true;
+                break;
+            }
+            if (cur < 0) {
+                test_range(leaf_first(cur), leaf_count(cur));
+                if (ANY && found) break;
+            } else {
+                if (cur >= num_nodes) {
+                    bad = true;
+                    break;
+                }
+                const float4* np = reinterpret_cast<const float4*>(nodes + cur);
+                const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2), f3 = __ldg(np + 3),
+                             f4 = __ldg(np + 4);
+                if (COUNT) ++visits;
+                const uint32_t eb = __float_as_uint(f0.w);
+                const float sx = __uint_as_float((eb & 0xFFu) << 23), sy = __uint_as_float(((eb >> 8) & 0xFFu) << 23),
+                            sz = __uint_as_float(((eb >> 16) & 0xFFu) << 23);
+                const uint32_t imask = eb >> 24;
+                const int child_base = __float_as_int(f1.x), tri_base = __float_as_int(f1.y);
+                const uint32_t meta_lo = __float_as_uint(f1.z), meta_hi = __float_as_uint(f1.w);
+                const uint32_t qw[12] = {__float_as_uint(f2.x), __float_as_uint(f2.y), __float_as_uint(f2.z),
+                                         __float_as_uint(f2.w), __float_as_uint(f3.x), __float_as_uint(f3.y),
+                                         __float_as_uint(f3.z), __float_as_uint(f3.w), __float_as_uint(f4.x),
+                                         __float_as_uint(f4.y), __float_as_uint(f4.z), __float_as_uint(f4.w)};
+                const float lim = best_t + fabsf(best_t) * kWPruneSlack;
+                // children hit, nearest last on the stack
+                int hit_ref[8];
+                float hit_t[8];
+                int nh = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const uint32_t meta = ((k < 4 ? meta_lo : meta_hi) >> (8 * (k & 3))) & 0xFFu;
+                    const bool inner = (imask >> k) & 1u;
+                    if (!inner && meta == 0u) continue;
+                    auto qb = [&](int arr) { return (float)((qw[2 * arr + (k >> 2)] >> (8 * (k & 3))) & 0xFFu); };
+                    const float lx = __fmaf_rn(qb(0), sx, f0.x), ly = __fmaf_rn(qb(1), sy, f0.y),
+                                lz = __fmaf_rn(qb(2), sz, f0.z);
+                    const float hx = __fmaf_rn(qb(3), sx, f0.x), hy = __fmaf_rn(qb(4), sy, f0.y),
+                                hz = __fmaf_rn(qb(5), sz, f0.z);
+                    const float tx0 = __fmul_rn(__fsub_rn(lx, r.o.x), r.inv.x), tx1 = __fmul_rn(__fsub_rn(hx, r.o.x), r.inv.x);
+                    const float ty0 = __fmul_rn(__fsub_rn(ly, r.o.y), r.inv.y), ty1 = __fmul_rn(__fsub_rn(hy, r.o.y), r.inv.y);
+                    const float tz0 = __fmul_rn(__fsub_rn(lz, r.o.z), r.inv.z), tz1 = __fmul_rn(__fsub_rn(hz, r.o.z), r.inv.z);
+                    float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+                    float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+                    tn = tn - fabsf(tn) * kWSlabWiden;
+                    tf = tf + fabsf(tf) * kWSlabWiden;
+                    if (!(tn <= tf && tf >= r.tmin && tn <= lim)) continue;
+                    const int ref = inner ? child_base + (int)meta
+                                          : make_leaf_ref(tri_base + (int)(meta & 31u), (int)(meta >> 5));
+                    // insertion by descending t: the nearest ends last
+                    int pos = nh++;
+                    while (pos > 0 && hit_t[pos - 1] < tn) {
+                        hit_t[pos] = hit_t[pos - 1];
+                        hit_ref[pos] = hit_ref[pos - 1];
+                        --pos;
+                    }
+                    hit_t[pos] = tn;
+                    hit_ref[pos] = ref;
+                }
+                if (sp + nh > STACK) {
+                    bad = true;
+                    break;
+                }
+                for (int k = 0; k < nh; ++k) {
+                    sref[sp] = hit_ref[k];
+                    st[sp] = hit_t[k];
+                    ++sp;
+                }
+            }
+            cur = 0x7FFFFFFF;
+            const float lim = best_t + fabsf(best_t) * kWPruneSlack;
+            while (sp > 0) {
+                --sp;
+                if (st[sp] <= lim) {
+                    cur = sref[sp];
+                    break;
+                }
+            }
+        }
+        if (bad) atomicOr(err, kErrStack);
+        if (ANY) {
+            occluded[i] = found ? 1 : 0;
+        } else {
+            int4 out;
+            out.x = found ? best_prim : -1;
+            out.y = __float_as_int(found ? best_t : __int_as_float(0x7F800000));
+            out.z = __float_as_int(found ? best_u : 0.0f);
+            out.w = __float_as_int(found ? best_v : 0.0f);
+            reinterpret_cast<int4*>(hits)[i] = out;
+        }
+    }
+    if (COUNT) {
+        const unsigned v = __reduce_add_sync(0xffffffffu, visits);
+        const unsigned t = __reduce_add_sync(0xffffffffu, tests);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&counters[0], (unsigned long long)v);
+            atomicAdd(&counters[1], (unsigned long long)t);
+        }
+    }
+}
+
+template <int LEAF, bool ANY, bool COUNT, int STACK>
+dipl_status launch_wide(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, uint32_t flags,
+                        unsigned long long* counters, cudaStream_t s) {
+    const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
+    wide_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kWTraceThreads - 1) / kWTraceThreads), kWTraceThreads,
+                                                  0, s>>>(static_cast<const WNode*>(b->nodes), b->tris, b->root,
+                                                          num_nodes, rays, n, hits, occ, flags, counters, b->d_err);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return DIPL_OK;
+}
+
+template <int LEAF, bool ANY, bool COUNT>
+dipl_status launch_wide_stack(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
+                              uint32_t flags, unsigned long long* counters, cudaStream_t s) {
+    const int need = 7 * b->depth + 8;
+    if (need <= 64) return launch_wide<LEAF, ANY, COUNT, 64>(b, rays, n, hits, occ, flags, counters, s);
+    if (need <= 192) return launch_wide<LEAF, ANY, COUNT, 192>(b, rays, n, hits, occ, flags, counters, s);
+    return launch_wide<LEAF, ANY, COUNT, 512>(b, rays, n, hits, occ, flags, counters, s);
+}
+
+}  // namespace
+
+// Builds the wide layout of every mesh of a batch from the binary PLOC tree. root_ids[k] = PLOC node id of
+// mesh k's root, root_counts[k] its triangle count. Outputs the wide nodes/triangles (in `storage`), each
+// mesh's root reference (wide node index or leaf reference), the number of wide levels per mesh, and the
+// node count.
+dipl_status build_wide(const int4* child, const float4* node_lo, const float4* node_hi, const int* leaf_start_of,
+                       const float4* btris, int N, int L, const std::vector<int>& root_ids,
+                       const std::vector<int>& root_counts, Storage& storage, cudaStream_t s, uint32_t* d_err,
+                       WNode** out_nodes, float4** out_tris, int64_t* out_num_nodes, std::vector<int>& out_root_refs,
+                       std::vector<int>& out_levels) {
+    const int m = (int)root_ids.size();
+    const int K = std::max(N - m, 1);
+    ScratchArena scratch(s);
+    WNode* nodes;
+    float4* tris;
+    int *front0, *front1, *kids;
+    uint32_t *ninner, *ntris, *totals;
+    unsigned char* scan_scratch;
+    dipl_status st;
+    if ((st = storage.alloc(&nodes, K)) != DIPL_OK || (st = storage.alloc(&tris, 3 * (size_t)std::max(N, 1))) != DIPL_OK ||
+        (st = scratch.alloc(&front0, K)) != DIPL_OK || (st = scratch.alloc(&front1, K)) != DIPL_OK ||
+        (st = scratch.alloc(&kids, 8 * (size_t)K)) != DIPL_OK || (st = scratch.alloc(&ninner, K)) != DIPL_OK ||
+        (st = scratch.alloc(&ntris, K)) != DIPL_OK || (st = scratch.alloc(&totals, 4)) != DIPL_OK ||
+        (st = scratch.alloc(&scan_scratch, scan_scratch_bytes(K))) != DIPL_OK)
+        return st;
+    WideIn W{child, node_lo, node_hi, leaf_start_of, btris, N, L};
+    out_root_refs.assign(m, 0);
+    out_levels.assign(m, 0);
+    // meshes whose root is a leaf: copy their triangles first
+    int tri_next = 0;
+    std::vector<int> inner_roots;
+    for (int k = 0; k < m; ++k) {
+        if (root_counts[k] < L) {
+            // the binary leaf range of the root: its leaf_start_of entry
+            int start = 0;
+            DIPL_CUDA(cudaMemcpyAsync(&start, leaf_start_of + root_ids[k], 4, cudaMemcpyDeviceToHost, s));
+            DIPL_CUDA(cudaStreamSynchronize(s));
+            copy_tris_kernel<<<1, 32, 0, s>>>(btris + 3 * (long long)start, tris + 3 * (long long)tri_next,
+                                              root_counts[k]);
+            note_launches();
+            out_root_refs[k] = make_leaf_ref(tri_next, root_counts[k]);
+            tri_next += root_counts[k];
+        } else {
+            out_root_refs[k] = (int)inner_roots.size();
+            inner_roots.push_back(root_ids[k]);
+        }
+    }
+    int n_front = (int)inner_roots.size();
+    if (n_front > 0)
+        DIPL_CUDA(cudaMemcpyAsync(front0, inner_roots.data(), 4 * n_front, cudaMemcpyHostToDevice, s));
+    int base = 0, levels = 0;
+    int* fin = front0;
+    int* fout = front1;
+    while (n_front > 0) {
+        const unsigned grid = (unsigned)((n_front + kWideThreads - 1) / kWideThreads);
+        wide_collapse_kernel<<<grid, kWideThreads, 0, s>>>(W, fin, n_front, kids, ninner, ntris, d_err);
+        note_launches();
+        if ((st = exclusive_scan_u32(ninner, ninner, n_front, totals, scan_scratch, s, d_err)) != DIPL_OK) return st;
+        if ((st = exclusive_scan_u32(ntris, ntris, n_front, totals + 1, scan_scratch, s, d_err)) != DIPL_OK) return st;
+        wide_write_kernel<<<grid, kWideThreads, 0, s>>>(W, fin, n_front, kids, ninner, ntris, base, base + n_front,
+                                                        tri_next, nodes, tris, fout, d_err);
+        note_launches();
+        DIPL_CUDA(cudaGetLastError());
+        uint32_t h[3] = {0, 0, 0};
+        DIPL_CUDA(cudaMemcpyAsync(h, totals, 8, cudaMemcpyDeviceToHost, s));
+        DIPL_CUDA(cudaMemcpyAsync(h + 2, d_err, 4, cudaMemcpyDeviceToHost, s));
+        DIPL_CUDA(cudaStreamSynchronize(s));
+        if (h[2] != 0u) {
+            set_last_error("wide build: device error");
+            return (h[2] & kErrTimeout) ? DIPL_ERR_TIMEOUT : DIPL_ERR_INTERNAL;
+        }
+        base += n_front;
+        tri_next += (int)h[1];
+        n_front = (int)h[0];
+        std::swap(fin, fout);
+        ++levels;
+        if (base + n_front > K) {
+            set_last_error("wide build: node capacity exceeded (internal)");
+            return DIPL_ERR_INTERNAL;
+        }
+    }
+    for (int k = 0; k < m; ++k) out_levels[k] = levels;
+    *out_nodes = nodes;
+    *out_tris = tris;
+    *out_num_nodes = base;
+    return DIPL_OK;
+}
+
+dipl_status trace_wide(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, int leaf_test,
+                       uint32_t flags, unsigned long long* counters, bool any, cudaStream_t s) {
+    if (any)
+        return leaf_test == DIPL_LEAF_REF_MT
+                   ? launch_wide_stack<DIPL_LEAF_REF_MT, true, false>(b, rays, n, nullptr, occ, flags, nullptr, s)
+                   : launch_wide_stack<DIPL_LEAF_WATERTIGHT, true, false>(b, rays, n, nullptr, occ, flags, nullptr, s);
+    if (counters)
+        return leaf_test == DIPL_LEAF_REF_MT
+                   ? launch_wide_stack<DIPL_LEAF_REF_MT, false, true>(b, rays, n, hits, nullptr, flags, counters, s)
+                   : launch_wide_stack<DIPL_LEAF_WATERTIGHT, false, true>(b, rays, n, hits, nullptr, flags, counters, s);
+    return leaf_test == DIPL_LEAF_REF_MT
+               ? launch_wide_stack<DIPL_LEAF_REF_MT, false, false>(b, rays, n, hits, nullptr, flags, nullptr, s)
+               : launch_wide_stack<DIPL_LEAF_WATERTIGHT, false, false>(b, rays, n, hits, nullptr, flags, nullptr, s);
+}
+
+}  // namespace dipl

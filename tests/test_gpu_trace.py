@@ -13,12 +13,13 @@ pytestmark = pytest.mark.gpu
 KINDS = [A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmc]
 
 
+@pytest.mark.parametrize("layout", ["binary", "wide8_q8"])
 @pytest.mark.parametrize("kind", KINDS)
 @pytest.mark.parametrize("name", GOLDEN_NAMES)
-def test_ref_mt_hits_bit_exact_with_reference_brute_force(name, kind):
+def test_ref_mt_hits_bit_exact_with_reference_brute_force(name, kind, layout):
     """Class E/T of the parity protocol: id, t, u, v bit-equal to DummyAccelerationStucture::Intersect."""
     g = load_golden(name)
-    bvh = build(g["tris"], kind)
+    bvh = build(g["tris"], kind, layout=layout)
     prim, t, u, v = trace(bvh, g["rays"], leaf_test="ref_mt")
     np.testing.assert_array_equal(prim, g["brute_prim"])
     np.testing.assert_array_equal(fbits(t), fbits(g["brute_t"]))
@@ -39,10 +40,11 @@ def test_agreement_classes_against_reference_sbvh(name):
     assert (sb_t[diff] >= t[diff]).all()
 
 
+@pytest.mark.parametrize("layout", ["binary", "wide8_q8"])
 @pytest.mark.parametrize("name", GOLDEN_NAMES)
-def test_watertight_matches_restatement(orc, name):
+def test_watertight_matches_restatement(orc, name, layout):
     g = load_golden(name)
-    prim, t, u, v = trace(build(g["tris"]), g["rays"], leaf_test="watertight")
+    prim, t, u, v = trace(build(g["tris"], layout=layout), g["rays"], leaf_test="watertight")
     h = orc.brute(g["tris"], g["rays"], leaf_test=1)
     np.testing.assert_array_equal(prim, h.prim)
     np.testing.assert_array_equal(fbits(t), fbits(h.t))
@@ -60,12 +62,13 @@ def test_backface_culling(orc, leaf_test):
     np.testing.assert_array_equal(fbits(t), fbits(h.t))
 
 
+@pytest.mark.parametrize("layout", ["binary", "wide8_q8"])
 @pytest.mark.parametrize("name", ["small_scene", "soup_2k", "duplicates_ties"])
-def test_any_hit_matches_oracle(orc, name):
+def test_any_hit_matches_oracle(orc, name, layout):
     g = load_golden(name)
     rays = g["rays"].copy()
     rays[:, 7] = np.where(np.arange(len(rays)) % 2 == 0, rays[:, 7], 0.5)  # half the rays: short shadow rays
-    bvh = build(g["tris"])
+    bvh = build(g["tris"], layout=layout)
     occ = bvh.IntersectAny(A.Stats(), torch.from_numpy(rays)).cpu().numpy()
     np.testing.assert_array_equal(occ, orc.brute_any(g["tris"], rays))
 
@@ -134,3 +137,124 @@ def test_displaced_sphere_1m_hits_verified(orc):
     h = orc.brute(tris, rays[sample])
     np.testing.assert_array_equal(prim[sample], h.prim)
     np.testing.assert_array_equal(fbits(t[sample]), fbits(h.t))
+
+
+def _decode_wide(nodes_bytes):
+    """Numpy view of the 80-byte wide nodes and their decoded child boxes (FP32 fma emulated exactly)."""
+    rec = np.frombuffer(nodes_bytes, dtype=np.dtype([
+        ("p", "<f4", 3), ("e", "u1", 3), ("imask", "u1"), ("child_base", "<i4"), ("tri_base", "<i4"),
+        ("meta", "u1", 8), ("qlo", "u1", (3, 8)), ("qhi", "u1", (3, 8))]))
+    scale = np.ldexp(1.0, rec["e"].astype(np.int64) - 127)  # (M, 3)
+    p = rec["p"].astype(np.float64)
+    lo = (rec["qlo"] * scale[:, :, None] + p[:, :, None]).astype(np.float32)
+    hi = (rec["qhi"] * scale[:, :, None] + p[:, :, None]).astype(np.float32)
+    return rec, lo, hi
+
+
+@pytest.mark.parametrize("name", ["small_scene_full_mesh", "soup_2k", "displaced_sphere_64x32"])
+def test_wide_quantised_bounds_are_conservative(name):
+    """Every triangle under a wide child slot lies inside that slot's decoded 8-bit box."""
+    g = load_golden(name)
+    bvh = build(g["tris"], layout="wide8_q8")
+    nodes, tris, root = bvh.download_layout()
+    rec, lo, hi = _decode_wide(nodes.tobytes())
+    binfo = build(g["tris"]).info()
+    assert bvh.info().node_bytes < binfo.node_bytes  # the compression the form exists for
+
+    def subtree_tris(node):
+        out = []
+        r = rec[node]
+        inner_rank = 0
+        for k in range(8):
+            if (r["imask"] >> k) & 1:
+                out += subtree_tris(r["child_base"] + r["meta"][k])
+            elif r["meta"][k]:
+                first = r["tri_base"] + (r["meta"][k] & 31)
+                out += list(range(first, first + (r["meta"][k] >> 5)))
+        return out
+
+    checked = 0
+    for node in range(len(rec)):
+        r = rec[node]
+        for k in range(8):
+            if (r["imask"] >> k) & 1:
+                ids = subtree_tris(r["child_base"] + r["meta"][k])
+            elif r["meta"][k]:
+                first = r["tri_base"] + (r["meta"][k] & 31)
+                ids = list(range(first, first + (r["meta"][k] >> 5)))
+            else:
+                continue
+            v = tris[ids][:, :, :3].reshape(-1, 3)
+            assert (v >= lo[node, :, k]).all() and (v <= hi[node, :, k]).all(), (node, k)
+            checked += 1
+            if checked > 3000:
+                return
+
+
+SOBB_KINDS = [A.AccelerationStructureType.kPlocSobb, A.AccelerationStructureType.kPlocEmcSobb]
+
+
+@pytest.mark.parametrize("kind", SOBB_KINDS)
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_sobb_hits_bit_exact_with_reference_brute_force(name, kind):
+    g = load_golden(name)
+    prim, t, u, v = trace(build(g["tris"], kind), g["rays"])
+    np.testing.assert_array_equal(prim, g["brute_prim"])
+    np.testing.assert_array_equal(fbits(t), fbits(g["brute_t"]))
+    np.testing.assert_array_equal(fbits(u), fbits(g["brute_u"]))
+
+
+@pytest.mark.parametrize("kdop", [6, 14, 26, 32])
+def test_sobb_direction_sets(orc, kdop):
+    g = load_golden("soup_2k")
+    bvh = build(g["tris"], A.AccelerationStructureType.kPlocSobb, kdop_size=kdop)
+    prim, t, _, _ = trace(bvh, g["rays"])
+    np.testing.assert_array_equal(prim, g["brute_prim"])
+    occ = bvh.IntersectAny(A.Stats(), torch.from_numpy(g["rays"])).cpu().numpy()
+    np.testing.assert_array_equal(occ, orc.brute_any(g["tris"], g["rays"]))
+
+
+SOBB_DIRS = np.array([
+    [1, 0, 0], [0, 1, 0], [0, 0, 1],
+    [0.57735026, 0.57735026, 0.57735026], [0.57735026, 0.57735026, -0.57735026],
+    [0.57735026, -0.57735026, 0.57735026], [-0.57735026, 0.57735026, 0.57735026],
+    [0.70710677, 0.70710677, 0], [0.70710677, -0.70710677, 0], [0.70710677, 0, 0.70710677],
+    [0.70710677, 0, -0.70710677], [0, 0.70710677, 0.70710677], [0, 0.70710677, -0.70710677],
+    [0, 0.52573111, 0.85065081], [0.52573111, 0.85065081, 0], [0.85065081, 0, 0.52573111]], np.float32)
+
+
+@pytest.mark.parametrize("name", ["small_scene_full_mesh", "soup_2k"])
+def test_sobb_slabs_contain_their_subtrees(name):
+    """Every vertex under a child lies inside that child's three slabs (exact FP64 projections)."""
+    g = load_golden(name)
+    bvh = build(g["tris"], A.AccelerationStructureType.kPlocSobb)
+    nodes, tris, root = bvh.download_layout()
+    rec = np.frombuffer(nodes.tobytes(), dtype=np.dtype([("f", "<f4", 12), ("ref", "<i4", 2), ("ax", "<i4", 2)]))
+    dirs = SOBB_DIRS.astype(np.float64)
+
+    def leaf_range(ref):
+        x = ~int(ref)
+        return list(range(x >> 3, (x >> 3) + (x & 7)))
+
+    def subtree(ref):
+        if ref < 0:
+            return leaf_range(ref)
+        r = rec[ref]
+        return subtree(r["ref"][0]) + subtree(r["ref"][1])
+
+    n_checked = 0
+    for k in range(len(rec)):
+        f = rec[k]["f"]
+        slabs = [(f[0:6], rec[k]["ax"][0]), (np.concatenate([f[6:12]]), rec[k]["ax"][1])]
+        for side in range(2):
+            vals, ax = slabs[side]
+            ids = subtree(rec[k]["ref"][side])
+            v = tris[ids][:, :, :3].reshape(-1, 3).astype(np.float64)
+            for j in range(3):
+                a = (int(ax) >> (8 * j)) & 0xFF
+                pr = v @ dirs[a]
+                assert (pr >= vals[2 * j]).all() and (pr <= vals[2 * j + 1]).all(), (k, side, j)
+            n_checked += 1
+        if n_checked > 2000:
+            break
+    assert n_checked > 0
