@@ -425,14 +425,17 @@ __device__ __forceinline__ void nn_search_sym(const float4* __restrict__ slo, co
 // increasing order, so its local strict-"<" minimum is its subset's key minimum.
 template <int NT>
 __device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, const float4* __restrict__ shi, int n,
-                                                int r, int* __restrict__ nn) {
+                                                int q0, int q1, int r, int* __restrict__ nn) {
+    const int m = q1 - q0;
     int P = 1;
-    while (P < 16 && 2 * P * n <= NT) P *= 2;
+    while (P < 16 && 2 * P * m <= NT) P *= 2;
     const int sub = (int)threadIdx.x & (P - 1);
-    for (int base = (int)threadIdx.x / P; base < ((n + (NT / P) - 1) / (NT / P)) * (NT / P); base += NT / P) {
-        const int q = base;
+    const int lanes = NT / P;
+    const int rounds = (m + lanes - 1) / lanes;
+    for (int rd = 0; rd < rounds; ++rd) {
+        const int q = q0 + (int)threadIdx.x / P + rd * lanes;
         unsigned long long key = ~0ull;
-        if (q < n) {
+        if (q < q1) {
             const float4 a = slo[q], b = shi[q];
             const int sg = __float_as_int(b.w);
             float bestd = __int_as_float(0x7F800000);
@@ -463,7 +466,7 @@ __device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, 
             const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
             key = other < key ? other : key;
         }
-        if (q < n && sub == 0) {
+        if (q < q1 && sub == 0) {
             int j = -1;
             if (key != ~0ull) {
                 const unsigned tie = (unsigned)key;
@@ -670,27 +673,38 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
     if (blockIdx.x == 0 && threadIdx.x == 0) P.ctrl->iterations = iter;
 }
 
-// The last iterations (at most kTailMax clusters) in one CTA of 1024 threads, clusters resident in shared
-// memory and double-buffered; the same rules as ploc_kernel, so the result equals the oracle's loop.
+// The last iterations (at most kTailMax clusters) in one thread-block cluster of kTailCtas CTAs of 1024 threads.
+// Every CTA keeps all clusters in its shared memory (double-buffered); per iteration each CTA finds the nearest
+// neighbours of its slice of positions and stores them into every CTA's neighbour array through distributed
+// shared memory; after one cluster barrier every CTA runs the same merge and compaction over all positions, so
+// all copies stay identical without exchanging them (only CTA 0 writes the new nodes). Same rules as
+// ploc_kernel, so the result still equals the oracle's loop.
+constexpr int kTailCtasMax = 8;
+
 struct TailSmem {
     float4 lo[2][kTailMax];
     float4 hi[2][kTailMax];
     int4 info[2][kTailMax];
-    int nn[kTailMax];
+    int nn[2][kTailMax];  // by iteration parity: peers write slice k+1 while slice k may still be read
     uint32_t warp_sum[kTailThreads / 32];
 };
 
 __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     TailSmem& s = *reinterpret_cast<TailSmem*>(s_raw);
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int ctas = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
     constexpr int IPT = kTailMax / kTailThreads;
-    if (ld_acquire_u32(P.err) != 0u) return;
+    // every CTA reads the same control words: the decisions below are identical across the cluster
+    const bool err0 = ld_acquire_u32(P.err) != 0u;
     uint32_t iter = P.ctrl->iterations;
     int n = (int)P.ctrl->n[iter & 1];
     int mbase = (int)P.ctrl->merges[iter & 1];
-    if (n <= P.num_meshes) return;
+    if (err0 || n <= P.num_meshes) return;
     if (n > kTailMax) {  // cannot happen: the grid kernel runs until n <= kTailMax
-        if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+        if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
         return;
     }
     const uint32_t first_parity = iter & 1;
@@ -701,29 +715,43 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     }
     cp_async_wait_all();
     __syncthreads();
+    cluster.sync();  // all CTAs are running before anyone stores into a peer's shared memory
     const int r = P.radius;
     const int max_internal = P.num_leaves - P.num_meshes;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int cur = 0;
     uint32_t tail_iters = 0;
+    bool failed = false;
     while (n > P.num_meshes) {
         if (iter + tail_iters >= kMaxPlocIterations) {
-            if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
-            return;
+            if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+            failed = true;
+            break;
         }
+        const int par = (int)(tail_iters & 1);
         const float4* __restrict__ lo = s.lo[cur];
         const float4* __restrict__ hi = s.hi[cur];
         const int4* __restrict__ info = s.info[cur];
-        nn_search_split<kTailThreads>(lo, hi, n, r, s.nn);
+        // ---- neighbours of this CTA's slice, then broadcast to the peers ------------------------------
+        const int slice = (n + ctas - 1) / ctas;
+        const int q0 = min(n, rank * slice), q1 = min(n, q0 + slice);
+        nn_search_split<kTailThreads>(lo, hi, n, q0, q1, r, s.nn[par]);
         __syncthreads();
+        for (int peer = 1; peer < ctas; ++peer) {
+            int* remote = cluster.map_shared_rank(s.nn[par], (rank + peer) % ctas);
+            for (int q = q0 + (int)threadIdx.x; q < q1; q += kTailThreads) remote[q] = s.nn[par][q];
+        }
+        cluster.sync();  // release our stores, acquire the peers'
+        const int* __restrict__ nn = s.nn[par];
+        // ---- merge decisions and compaction over all positions (identical in every CTA) --------------
         const int ib = threadIdx.x * IPT;
         uint32_t keep_bits = 0, merge_bits = 0;
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int i = ib + k;
             if (i >= n) break;
-            const int j = s.nn[i];
-            const bool mutual = j >= 0 && s.nn[j] == i;
+            const int j = nn[i];
+            const bool mutual = j >= 0 && nn[j] == i;
             if (!(mutual && i > j)) keep_bits |= 1u << k;
             if (mutual && i < j) merge_bits |= 1u << k;
         }
@@ -731,17 +759,21 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
         uint32_t x = mine;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
         if (lane == 31) s.warp_sum[warp] = x;
         __syncthreads();
-        uint32_t woff = 0, total = 0;
-        for (int w = 0; w < kTailThreads / 32; ++w) {
-            const uint32_t v = s.warp_sum[w];
-            if (w < warp) woff += v;
-            total += v;
+        // scan of the 32 warp sums with shuffles (every warp, redundantly)
+        const uint32_t ws = s.warp_sum[lane];
+        uint32_t wx = ws;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wx, o);
+            if (lane >= o) wx += y;
         }
+        const uint32_t total = __shfl_sync(0xffffffffu, wx, 31);
+        const uint32_t woff = __shfl_sync(0xffffffffu, wx - ws, warp);
         const uint32_t excl = woff + x - mine;
         uint32_t kpos = excl & 0xFFFFu;
         uint32_t mpos = (uint32_t)mbase + (excl >> 16);
@@ -753,13 +785,22 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
             float4 oa = lo[i], ob = hi[i];
             int4 oi = info[i];
             if ((merge_bits >> k) & 1u) {
-                const int j = s.nn[i];
+                const int j = nn[i];
                 const int knew = (int)mpos++;
                 if (knew >= max_internal) {
-                    atomicOr(P.err, kErrIterations);
+                    if (rank == 0) atomicOr(P.err, kErrIterations);
                     continue;
                 }
-                emit_node(P, knew, lo[i], hi[i], info[i], lo[j], hi[j], info[j], oa, ob, oi);
+                if (rank == 0) {
+                    emit_node(P, knew, lo[i], hi[i], info[i], lo[j], hi[j], info[j], oa, ob, oi);
+                } else {
+                    const float4 ja = lo[j], jb = hi[j];
+                    const int4 ji = info[j];
+                    oa = make_float4(fminf(oa.x, ja.x), fminf(oa.y, ja.y), fminf(oa.z, ja.z),
+                                     __int_as_float(P.num_leaves + knew));
+                    ob = make_float4(fmaxf(ob.x, jb.x), fmaxf(ob.y, jb.y), fmaxf(ob.z, jb.z), ob.w);
+                    oi = make_int4(oi.x + ji.x, min(oi.y, ji.y), max(oi.z, ji.z) + 1, 0);
+                }
             }
             s.lo[nxt][kpos] = oa;
             s.hi[nxt][kpos] = ob;
@@ -770,13 +811,16 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
         mbase += (int)(total >> 16);
         __syncthreads();
         if (kept == n) {  // no progress: impossible under a strict total order on pairs
-            if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
-            return;
+            if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+            failed = true;
+            break;
         }
         n = kept;
         cur = nxt;
         ++tail_iters;
     }
+    cluster.sync();  // no CTA leaves while a peer may still store into its shared memory
+    if (failed || rank != 0) return;
     // final clusters (one per mesh) to the buffer of the final parity, for the root pass
     const uint32_t final_iter = iter + tail_iters;
     for (int i = threadIdx.x; i < n; i += kTailThreads) {
@@ -1063,9 +1107,32 @@ dipl_status launch_ploc(const PlocParams& P, int initial_tiles, cudaStream_t str
 dipl_status launch_ploc_tail(const PlocParams& P, cudaStream_t stream) {
     const size_t smem = sizeof(TailSmem);
     DIPL_CUDA(cudaFuncSetAttribute(ploc_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ploc_tail_kernel<<<1, kTailThreads, smem, stream>>>(P);
+    static int ctas = 0;  // the largest cluster size the device can schedule with this footprint
+    if (ctas == 0) {
+        for (int c = kTailCtasMax; c >= 1; c /= 2) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = c, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(c), cfg.blockDim = dim3(kTailThreads), cfg.dynamicSmemBytes = smem;
+            cfg.attrs = attr, cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, ploc_tail_kernel, &cfg) == cudaSuccess && clusters > 0) {
+                ctas = c;
+                break;
+            }
+            (void)cudaGetLastError();
+        }
+        if (ctas == 0) ctas = 1;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ctas, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(ctas), cfg.blockDim = dim3(kTailThreads), cfg.dynamicSmemBytes = smem, cfg.stream = stream;
+    cfg.attrs = attr, cfg.numAttrs = 1;
+    DIPL_CUDA(cudaLaunchKernelEx(&cfg, ploc_tail_kernel, P));
     note_launches();
-    DIPL_CUDA(cudaGetLastError());
     return DIPL_OK;
 }
 
