@@ -23,7 +23,9 @@ TRACE_BACKFACE_CULLING = 1
 
 # Every entry point include/dipl_bvh.h declares.
 EXPORTS = [
-    "dipl_build_desc_init", "dipl_bvh_build", "dipl_bvh_build_batched", "dipl_bvh_trace_closest",
+    "dipl_build_desc_init", "dipl_bvh_build", "dipl_bvh_build_batched", "dipl_build_plan_create",
+    "dipl_build_plan_launch", "dipl_build_plan_get_bvhs", "dipl_build_plan_destroy", "dipl_autotune_build",
+    "dipl_bvh_trace_closest",
     "dipl_bvh_trace_closest_counted", "dipl_bvh_trace_any", "dipl_bvh_sah_cost", "dipl_bvh_get_info",
     "dipl_bvh_download_topology", "dipl_bvh_download_layout", "dipl_bvh_check_errors", "dipl_bvh_destroy", "dipl_compute_codes",
     "dipl_radix_sort_pairs", "dipl_radix_sort_pairs_noalloc", "dipl_reintersect_f64", "dipl_trace_adjoint", "dipl_status_string",
@@ -68,6 +70,11 @@ def load(path: str = LIB_PATH):
         "dipl_build_desc_init": (None, [C.POINTER(BuildDesc)]),
         "dipl_bvh_build": (i32, [C.POINTER(BuildDesc), C.POINTER(vp), vp]),
         "dipl_bvh_build_batched": (i32, [C.POINTER(BuildDesc), i32, C.POINTER(vp), vp]),
+        "dipl_build_plan_create": (i32, [C.POINTER(BuildDesc), i32, C.POINTER(vp), vp]),
+        "dipl_build_plan_launch": (i32, [vp, vp]),
+        "dipl_build_plan_get_bvhs": (i32, [vp, C.POINTER(vp), vp]),
+        "dipl_build_plan_destroy": (i32, [vp]),
+        "dipl_autotune_build": (i32, [C.POINTER(BuildDesc), i32, C.c_char_p, C.POINTER(BuildDesc), C.POINTER(i32), vp]),
         "dipl_bvh_trace_closest": (i32, [vp, vp, i64, vp, i32, u32, vp]),
         "dipl_bvh_trace_closest_counted": (i32, [vp, vp, i64, vp, i32, u32, vp, vp]),
         "dipl_bvh_trace_any": (i32, [vp, vp, i64, vp, i32, u32, vp]),

@@ -341,3 +341,54 @@ def trace_adjoint(v, rays: torch.Tensor, hits: Hits, dtuv: torch.Tensor):
                                    _ptr(dv[0]), _ptr(dv[1]), _ptr(dv[2]), _ptr(dorig), _ptr(ddir), _stream()),
             "dipl_trace_adjoint")
     return dv[0], dv[1], dv[2], dorig, ddir
+
+
+class BuildPlan:
+    """A batch of meshes captured once into a CUDA graph (dipl_build_plan_*); ``launch`` rebuilds every BVH from
+    the current vertex contents; ``bvhs`` waits and returns one GpuPlocBvh per mesh for the latest build."""
+
+    def __init__(self, config: AccelerationStructureConfig, meshes, tuned_descs=None):
+        self._lib = L.load()
+        self.config = config
+        self.verts = [soa_vertices(m) for m in meshes]
+        n = len(self.verts)
+        self.descs = (L.BuildDesc * n)()
+        for i, v in enumerate(self.verts):
+            self.descs[i] = tuned_descs[i] if tuned_descs is not None else make_desc(*v, config)
+        self._h = C.c_void_p(0)
+        L.check(self._lib.dipl_build_plan_create(self.descs, n, C.byref(self._h), _stream()), "dipl_build_plan_create")
+
+    def launch(self):
+        L.check(self._lib.dipl_build_plan_launch(self._h, _stream()), "dipl_build_plan_launch")
+
+    def bvhs(self):
+        n = len(self.verts)
+        handles = (C.c_void_p * n)()
+        L.check(self._lib.dipl_build_plan_get_bvhs(self._h, handles, _stream()), "dipl_build_plan_get_bvhs")
+        return [GpuPlocBvh.from_handle(C.c_void_p(handles[i]), self.verts[i], self.config) for i in range(n)]
+
+    def close(self):
+        if self._h.value:
+            self._lib.dipl_build_plan_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(config: AccelerationStructureConfig, meshes, cache_path=None):
+    """dipl_autotune_build over these meshes; returns (tuned descs array, from_cache)."""
+    lib = L.load()
+    verts = [soa_vertices(m) for m in meshes]
+    n = len(verts)
+    descs = (L.BuildDesc * n)()
+    for i, v in enumerate(verts):
+        descs[i] = make_desc(*v, config)
+    tuned = (L.BuildDesc * n)()
+    fc = C.c_int32(0)
+    path = cache_path.encode() if cache_path else None
+    L.check(lib.dipl_autotune_build(descs, n, path, tuned, C.byref(fc), _stream()), "dipl_autotune_build")
+    return tuned, bool(fc.value), verts

@@ -143,6 +143,23 @@ dipl_status dipl_bvh_build_batched(const dipl_build_desc* descs, int32_t count, 
     return build_batched(descs, count, out, static_cast<cudaStream_t>(stream));
 }
 
+dipl_status dipl_build_plan_create(const dipl_build_desc* descs, int32_t count, dipl_build_plan** out, void* stream) {
+    return plan_create(descs, count, out, static_cast<cudaStream_t>(stream));
+}
+
+dipl_status dipl_build_plan_launch(dipl_build_plan* plan, void* stream) {
+    return plan_launch(plan, static_cast<cudaStream_t>(stream));
+}
+
+dipl_status dipl_build_plan_get_bvhs(dipl_build_plan* plan, dipl_bvh** out, void* stream) {
+    return plan_get_bvhs(plan, out, static_cast<cudaStream_t>(stream));
+}
+
+dipl_status dipl_build_plan_destroy(dipl_build_plan* plan) {
+    plan_destroy(plan);
+    return DIPL_OK;
+}
+
 dipl_status dipl_bvh_trace_closest(const dipl_bvh* bvh, const dipl_ray* d_rays, int64_t n, dipl_hit* d_hits,
                                    int32_t leaf_test, uint32_t flags, void* stream) {
     return trace_closest(bvh, d_rays, n, d_hits, leaf_test, flags, nullptr, static_cast<cudaStream_t>(stream));

@@ -847,6 +847,10 @@ __global__ void ploc_init_kernel(const MeshDesc* __restrict__ meshes, const long
     parent[p] = -1;
 }
 
+__global__ void ploc_ctrl_init_kernel(PlocCtrl* ctrl, uint32_t n) {
+    ctrl->n[0] = n;  // the rest was cleared by a memset
+}
+
 __global__ void fill_int_kernel(int* p, long long n, int v) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
@@ -1098,8 +1102,14 @@ dipl_status launch_ploc(const PlocParams& P, int initial_tiles, cudaStream_t str
         return DIPL_ERR_CUDA;
     }
     int grid = std::max(1, std::min(initial_tiles, sms * per_sm));
-    void* args[] = {const_cast<PlocParams*>(&P)};
-    DIPL_CUDA(cudaLaunchCooperativeKernel((const void*)ploc_kernel<B>, dim3(grid), dim3(B), args, smem, stream));
+    // cooperative launch (all blocks co-resident, required by the grid barrier); capturable into a graph
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.gridDim = dim3(grid), cfg.blockDim = dim3(B), cfg.dynamicSmemBytes = smem, cfg.stream = stream;
+    cfg.attrs = attr, cfg.numAttrs = 1;
+    DIPL_CUDA(cudaLaunchKernelEx(&cfg, ploc_kernel<B>, P));
     note_launches();
     return DIPL_OK;
 }
@@ -1166,222 +1176,304 @@ static dipl_status validate_desc(const dipl_build_desc& d) {
     return DIPL_OK;
 }
 
-dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** out, cudaStream_t stream) {
-    DIPL_CHECK_ARG(descs && out && count >= 1, "descs/out must be non-NULL and count >= 1");
+// ------------------------------------------------------------------------------------------------
+// A build in three phases: prepare (validation, every allocation, uploads), enqueue (only kernels, memsets
+// and device copies on the stream, ending with one copy of the per-mesh summary to pinned host memory:
+// capturable into a CUDA graph) and finish (read the summary after the stream synchronised, make handles).
+// ------------------------------------------------------------------------------------------------
+struct BuildPlan {
+    std::vector<dipl_build_desc> descs;
+    std::vector<int> mesh_of_desc;
+    std::vector<MeshDesc> meshes;
+    std::vector<long long> offsets;
+    dipl_build_desc d0{};
+    int count = 0, m = 0, L = 4;
+    long long N = 0, K = 0, Kalloc = 1;
+    int code_bits = 30, mesh_bits = 0, key_bits = 30, code_shift = 0, mesh_shift = 0, key_bytes = 4;
+    int digit_bits = 8, B = 256, tiles0 = 1, tiles_max = 1;
+    cudaStream_t stream = nullptr;
+    std::shared_ptr<Storage> out;   // arrays the handles keep
+    std::shared_ptr<Storage> work;  // scratch of the pipeline
+    uint32_t* d_err = nullptr;
+    MeshDesc* d_meshes = nullptr;
+    long long* d_offsets = nullptr;
+    Bounds* d_bounds = nullptr;
+    CodeParams* d_params = nullptr;
+    void *keys = nullptr, *keys_sorted = nullptr, *keys_alt = nullptr;
+    uint32_t *perm = nullptr, *perm_alt = nullptr;
+    unsigned char* sort_scratch = nullptr;
+    PlocCtrl* d_ctrl = nullptr;
+    int4* child = nullptr;
+    float4 *nlo = nullptr, *nhi = nullptr;
+    int* parent = nullptr;
+    unsigned long long* status = nullptr;
+    float4 *c_lo[2] = {nullptr, nullptr}, *c_hi[2] = {nullptr, nullptr};
+    int4* c_in[2] = {nullptr, nullptr};
+    uint32_t *rev_flags = nullptr, *contrib = nullptr, *d_counts = nullptr;
+    int *owner_leaf = nullptr, *leaf_start_of = nullptr;
+    unsigned char* scan_scratch = nullptr;
+    BNode* nodes = nullptr;
+    float4* tris = nullptr;
+    double* d_sah = nullptr;
+    RootInfo* d_roots = nullptr;
+    SobbScratch sobb{};
+    SNode* snodes = nullptr;
+    unsigned char* h_summary = nullptr;  // pinned
+    bool owns_summary = false;
+    size_t summary_bytes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_kernels = 0;
+    ~BuildPlan() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (h_summary && owns_summary) cudaFreeHost(h_summary);
+    }
+};
+
+static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int count, cudaStream_t stream,
+                                bool own_summary) {
+    DIPL_CHECK_ARG(descs && count >= 1, "descs must be non-NULL and count >= 1");
     for (int i = 0; i < count; ++i) {
         dipl_status st = validate_desc(descs[i]);
         if (st != DIPL_OK) return st;
-        out[i] = nullptr;
     }
     const dipl_build_desc& d0 = descs[0];
     for (int i = 1; i < count; ++i) {
         DIPL_CHECK_ARG(descs[i].code_type == d0.code_type && descs[i].bv_type == d0.bv_type &&
                            descs[i].layout == d0.layout && descs[i].max_triangles_per_leaf == d0.max_triangles_per_leaf &&
-                           descs[i].nn_search_radius == d0.nn_search_radius && descs[i].kdop_size == d0.kdop_size,
+                           descs[i].nn_search_radius == d0.nn_search_radius && descs[i].kdop_size == d0.kdop_size &&
+                           descs[i].ploc_block_size == d0.ploc_block_size &&
+                           descs[i].sort_digit_bits == d0.sort_digit_bits,
                        "batched builds need one set of build options");
     }
-    // Meshes with triangles take part in the pipeline; empty meshes get empty handles.
-    std::vector<MeshDesc> meshes;
-    std::vector<long long> offsets;
-    std::vector<int> mesh_of_desc(count, -1);
+    P.descs.assign(descs, descs + count);
+    P.count = count;
+    P.d0 = d0;
+    P.stream = stream;
+    P.mesh_of_desc.assign(count, -1);
     long long total = 0;
     for (int i = 0; i < count; ++i) {
         if (descs[i].num_triangles == 0) continue;
-        mesh_of_desc[i] = (int)meshes.size();
-        meshes.push_back(MeshDesc{descs[i].d_v0, descs[i].d_v1, descs[i].d_v2, total, descs[i].num_triangles});
-        offsets.push_back(total);
+        P.mesh_of_desc[i] = (int)P.meshes.size();
+        P.meshes.push_back(MeshDesc{descs[i].d_v0, descs[i].d_v1, descs[i].d_v2, total, descs[i].num_triangles});
+        P.offsets.push_back(total);
         total += descs[i].num_triangles;
     }
     DIPL_CHECK_ARG(total < (1ll << 27), "total triangles of a build must be < 2^27");
-    const int m = (int)meshes.size();
-    offsets.push_back(total);
-
-    auto storage = std::make_shared<Storage>();
-    storage->stream = stream;
-    uint32_t* d_err = nullptr;
-    dipl_status st = storage->alloc(&d_err, 4);
-    if (st != DIPL_OK) return st;
-    DIPL_CUDA(cudaMemsetAsync(d_err, 0, 4, stream));
-
-    auto make_handle = [&](int i) {
-        auto* h = new dipl_bvh();
-        h->storage = storage;
-        h->num_triangles = descs[i].num_triangles;
-        h->code_type = descs[i].code_type;
-        h->bv_type = descs[i].bv_type;
-        h->layout = descs[i].layout;
-        h->max_leaf = descs[i].max_triangles_per_leaf;
-        h->radius = descs[i].nn_search_radius;
-        h->kdop = descs[i].kdop_size;
-        h->d_err = d_err;
-        h->root = 0;
-        return h;
-    };
-
-    if (m == 0) {
-        for (int i = 0; i < count; ++i) out[i] = make_handle(i);
-        return DIPL_OK;
-    }
-
-    const long long N = total;
-    const long long K = N - m;  // internal nodes
-    const int L = d0.max_triangles_per_leaf;
-    ScratchArena scratch(stream);
-
-    MeshDesc* d_meshes;
-    long long* d_offsets;
-    Bounds* d_bounds;
-    CodeParams* d_params;
-    if ((st = scratch.alloc(&d_meshes, m)) != DIPL_OK || (st = scratch.alloc(&d_offsets, m + 1)) != DIPL_OK ||
-        (st = scratch.alloc(&d_bounds, m)) != DIPL_OK || (st = scratch.alloc(&d_params, m)) != DIPL_OK)
+    P.m = (int)P.meshes.size();
+    P.offsets.push_back(total);
+    P.N = total;
+    P.K = total - P.m;
+    P.Kalloc = std::max<long long>(P.K, 1);
+    P.L = d0.max_triangles_per_leaf;
+    P.out = std::make_shared<Storage>();
+    P.out->stream = stream;
+    P.work = std::make_shared<Storage>();
+    P.work->stream = stream;
+    dipl_status st;
+    if ((st = P.out->alloc(&P.d_err, 4)) != DIPL_OK) return st;
+    if (P.m == 0) return DIPL_OK;
+    const int m = P.m;
+    const long long N = P.N, K = P.K, Kalloc = P.Kalloc;
+    Storage& W = *P.work;
+    Storage& O = *P.out;
+    if ((st = W.alloc(&P.d_meshes, m)) != DIPL_OK || (st = W.alloc(&P.d_offsets, m + 1)) != DIPL_OK ||
+        (st = W.alloc(&P.d_bounds, m)) != DIPL_OK || (st = W.alloc(&P.d_params, m)) != DIPL_OK)
         return st;
-    DIPL_CUDA(cudaMemcpyAsync(d_meshes, meshes.data(), sizeof(MeshDesc) * m, cudaMemcpyHostToDevice, stream));
-    DIPL_CUDA(cudaMemcpyAsync(d_offsets, offsets.data(), sizeof(long long) * (m + 1), cudaMemcpyHostToDevice, stream));
+    DIPL_CUDA(cudaMemcpyAsync(P.d_meshes, P.meshes.data(), sizeof(MeshDesc) * m, cudaMemcpyHostToDevice, stream));
+    DIPL_CUDA(cudaMemcpyAsync(P.d_offsets, P.offsets.data(), sizeof(long long) * (m + 1), cudaMemcpyHostToDevice,
+                              stream));
+    P.code_bits = d0.code_type == DIPL_CODE_MORTON30 ? 30 : 60;
+    while ((1ll << P.mesh_bits) < m) ++P.mesh_bits;
+    P.key_bits = P.code_bits + P.mesh_bits;
+    if (P.key_bits > 64) {
+        P.code_shift = P.key_bits - 64;
+        P.key_bits = 64;
+    }
+    P.mesh_shift = P.mesh_bits > 0 ? P.code_bits - P.code_shift : 0;
+    P.key_bytes = P.key_bits <= 32 ? 4 : 8;
+    P.digit_bits = d0.sort_digit_bits > 0 ? d0.sort_digit_bits : 8;
+    if ((st = W.alloc((unsigned char**)&P.keys, N * P.key_bytes)) != DIPL_OK ||
+        (st = W.alloc((unsigned char**)&P.keys_sorted, N * P.key_bytes)) != DIPL_OK ||
+        (st = W.alloc((unsigned char**)&P.keys_alt, N * P.key_bytes)) != DIPL_OK ||
+        (st = O.alloc(&P.perm, N)) != DIPL_OK || (st = W.alloc(&P.perm_alt, N)) != DIPL_OK ||
+        (st = W.alloc(&P.sort_scratch, radix_sort_scratch_bytes(N, 0, P.key_bits, P.digit_bits))) != DIPL_OK)
+        return st;
+    P.B = ploc_block_for(d0.ploc_block_size);
+    P.tiles0 = (int)((N + P.B * kPlocIpt - 1) / (P.B * kPlocIpt));
+    P.tiles_max = (int)((N + P.B - 1) / P.B);
+    if ((st = W.alloc(&P.d_ctrl, 1)) != DIPL_OK || (st = O.alloc(&P.child, Kalloc)) != DIPL_OK ||
+        (st = O.alloc(&P.nlo, Kalloc)) != DIPL_OK || (st = O.alloc(&P.nhi, Kalloc)) != DIPL_OK ||
+        (st = W.alloc(&P.parent, N + Kalloc)) != DIPL_OK || (st = W.alloc(&P.status, 2 * P.tiles_max + 2)) != DIPL_OK)
+        return st;
+    for (int k = 0; k < 2; ++k)
+        if ((st = W.alloc(&P.c_lo[k], N)) != DIPL_OK || (st = W.alloc(&P.c_hi[k], N)) != DIPL_OK ||
+            (st = W.alloc(&P.c_in[k], N)) != DIPL_OK)
+            return st;
+    if ((st = W.alloc(&P.rev_flags, Kalloc)) != DIPL_OK || (st = W.alloc(&P.contrib, N)) != DIPL_OK ||
+        (st = W.alloc(&P.owner_leaf, N)) != DIPL_OK || (st = W.alloc(&P.leaf_start_of, N + Kalloc)) != DIPL_OK ||
+        (st = W.alloc(&P.scan_scratch, scan_scratch_bytes(std::max(N, Kalloc)))) != DIPL_OK ||
+        (st = W.alloc(&P.d_counts, 4)) != DIPL_OK || (st = O.alloc(&P.nodes, Kalloc)) != DIPL_OK ||
+        (st = O.alloc(&P.tris, 3 * N)) != DIPL_OK || (st = W.alloc(&P.d_sah, 2 * m)) != DIPL_OK ||
+        (st = W.alloc(&P.d_roots, m)) != DIPL_OK)
+        return st;
+    if (d0.bv_type == DIPL_BV_SOBB) {
+        if ((st = sobb_prepare(N, K, W, O, &P.sobb, &P.snodes)) != DIPL_OK) return st;
+    }
+    P.summary_bytes = sizeof(RootInfo) * m + sizeof(double) * 2 * m + 16;
+    if (own_summary) {  // a plan replays into its own pinned buffer
+        if (cudaMallocHost(&P.h_summary, P.summary_bytes) != cudaSuccess) {
+            P.h_summary = nullptr;
+            set_last_error("pinned host allocation failed");
+            return DIPL_ERR_OUT_OF_MEMORY;
+        }
+        P.owns_summary = true;
+    } else {  // a one-shot build reads it back right away: the calling thread's staging buffer
+        P.h_summary = pinned_host_buffer(P.summary_bytes);
+        if (!P.h_summary) {
+            set_last_error("pinned host allocation failed");
+            return DIPL_ERR_OUT_OF_MEMORY;
+        }
+    }
+    return DIPL_OK;
+}
 
-    // ---- bounds + code parameters ------------------------------------------------------------------
-    bounds_init_kernel<<<blocks_for(m, 128), 128, 0, stream>>>(d_bounds, m); note_launches();
+template <int B>
+static dipl_status launch_ploc_any(const PlocParams& p, int tiles0, cudaStream_t s) {
+    return launch_ploc<B>(p, tiles0, s);
+}
+
+// Everything on the stream, nothing else: no allocation, no host copy from pageable memory, no synchronisation.
+static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
+    DIPL_CUDA(cudaMemsetAsync(P.d_err, 0, 4, stream));
+    if (P.m == 0) return DIPL_OK;
+    const int m = P.m;
+    const long long N = P.N, K = P.K;
+    const dipl_build_desc& d0 = P.d0;
+    dipl_status st;
+    bounds_init_kernel<<<blocks_for(m, 128), 128, 0, stream>>>(P.d_bounds, m);
+    note_launches();
     {
-        long long grid = std::min<long long>((N + 1023) / 1024, 148 * 16);
-        grid = std::max<long long>(grid, 1);
+        long long grid = std::max<long long>(1, std::min<long long>((N + 1023) / 1024, 148 * 16));
         long long chunk = (N + grid - 1) / grid;
-        bounds_kernel<<<(unsigned)grid, 256, 0, stream>>>(d_meshes, d_offsets, m, N, chunk, d_bounds); note_launches();
+        bounds_kernel<<<(unsigned)grid, 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, chunk, P.d_bounds);
+        note_launches();
     }
-    code_params_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(d_bounds, m, d0.code_type, d_params); note_launches();
-    DIPL_CUDA(cudaGetLastError());
-
-    // ---- codes + sort --------------------------------------------------------------------------------
-    const int code_bits = d0.code_type == DIPL_CODE_MORTON30 ? 30 : 60;
-    int mesh_bits = 0;
-    while ((1ll << mesh_bits) < m) ++mesh_bits;
-    int key_bits = code_bits + mesh_bits, code_shift = 0;
-    if (key_bits > 64) {
-        code_shift = key_bits - 64;
-        key_bits = 64;
-    }
-    const int mesh_shift = mesh_bits > 0 ? code_bits - code_shift : 0;
-    const int key_bytes = key_bits <= 32 ? 4 : 8;
-    const int digit_bits = d0.sort_digit_bits > 0 ? d0.sort_digit_bits : 8;
-    void *keys, *keys_sorted, *keys_alt;
-    uint32_t *perm, *perm_alt;
-    unsigned char* sort_scratch;
-    if ((st = scratch.alloc((unsigned char**)&keys, N * key_bytes)) != DIPL_OK ||
-        (st = scratch.alloc((unsigned char**)&keys_sorted, N * key_bytes)) != DIPL_OK ||
-        (st = scratch.alloc((unsigned char**)&keys_alt, N * key_bytes)) != DIPL_OK ||
-        (st = storage->alloc(&perm, N)) != DIPL_OK || (st = scratch.alloc(&perm_alt, N)) != DIPL_OK ||
-        (st = scratch.alloc(&sort_scratch, radix_sort_scratch_bytes(N, 0, key_bits, digit_bits))) != DIPL_OK)
-        return st;
-    if (key_bytes == 4)
-        codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, m, N, d_params,
-                                                                       d0.code_type, code_shift, mesh_shift,
-                                                                       (uint32_t*)keys);
+    code_params_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(P.d_bounds, m, d0.code_type, P.d_params);
+    note_launches();
+    if (P.key_bytes == 4)
+        codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.d_params,
+                                                                       d0.code_type, P.code_shift, P.mesh_shift,
+                                                                       (uint32_t*)P.keys);
     else
         codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
-            d_meshes, d_offsets, m, N, d_params, d0.code_type, code_shift, mesh_shift, (unsigned long long*)keys); note_launches();
+            P.d_meshes, P.d_offsets, m, N, P.d_params, d0.code_type, P.code_shift, P.mesh_shift,
+            (unsigned long long*)P.keys);
+    note_launches();
     DIPL_CUDA(cudaGetLastError());
-    st = radix_sort_pairs(keys, nullptr, keys_sorted, perm, keys_alt, perm_alt, N, key_bytes, 0, key_bits, digit_bits,
-                          sort_scratch, stream, d_err);
+    st = radix_sort_pairs(P.keys, nullptr, P.keys_sorted, P.perm, P.keys_alt, P.perm_alt, N, P.key_bytes, 0,
+                          P.key_bits, P.digit_bits, P.sort_scratch, stream, P.d_err);
     if (st != DIPL_OK) return st;
 
     // ---- PLOC ------------------------------------------------------------------------------------------
-    const int B = ploc_block_for(d0.ploc_block_size);
-    const int T = B * kPlocIpt;
-    const int tiles0 = (int)((N + T - 1) / T);
-    const int tiles_max = (int)((N + B - 1) / B);  // tiles of one item per thread
-    PlocParams P{};
-    PlocCtrl* d_ctrl;
-    int4* child;
-    float4 *nlo, *nhi;
-    int* parent;
-    unsigned long long* status;
-    float4 *c_lo0, *c_hi0, *c_lo1, *c_hi1;
-    int4 *c_in0, *c_in1;
-    const long long Kalloc = std::max<long long>(K, 1);
-    if ((st = scratch.alloc(&d_ctrl, 1)) != DIPL_OK || (st = storage->alloc(&child, Kalloc)) != DIPL_OK ||
-        (st = storage->alloc(&nlo, Kalloc)) != DIPL_OK || (st = storage->alloc(&nhi, Kalloc)) != DIPL_OK ||
-        (st = scratch.alloc(&parent, N + Kalloc)) != DIPL_OK || (st = scratch.alloc(&status, 2 * tiles_max + 2)) != DIPL_OK ||
-        (st = scratch.alloc(&c_lo0, N)) != DIPL_OK || (st = scratch.alloc(&c_hi0, N)) != DIPL_OK ||
-        (st = scratch.alloc(&c_lo1, N)) != DIPL_OK || (st = scratch.alloc(&c_hi1, N)) != DIPL_OK ||
-        (st = scratch.alloc(&c_in0, N)) != DIPL_OK || (st = scratch.alloc(&c_in1, N)) != DIPL_OK)
-        return st;
-    PlocCtrl hctrl{};
-    hctrl.n[0] = (uint32_t)N;
-    hctrl.merges[0] = 0;
-    DIPL_CUDA(cudaMemcpyAsync(d_ctrl, &hctrl, sizeof(PlocCtrl), cudaMemcpyHostToDevice, stream));
-    DIPL_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (2 * tiles_max + 2), stream));
-    fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(parent, N + K, -1); note_launches();
-    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, m, N, perm, c_lo0, c_hi0, c_in0,
-                                                             parent);
+    PlocParams pp{};
+    DIPL_CUDA(cudaMemsetAsync(P.d_ctrl, 0, sizeof(PlocCtrl), stream));
+    ploc_ctrl_init_kernel<<<1, 1, 0, stream>>>(P.d_ctrl, (uint32_t)N);
+    note_launches();
+    DIPL_CUDA(cudaMemsetAsync(P.status, 0, sizeof(unsigned long long) * (2 * P.tiles_max + 2), stream));
+    fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(P.parent, N + K, -1);
+    note_launches();
+    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.perm, P.c_lo[0],
+                                                             P.c_hi[0], P.c_in[0], P.parent);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
-    P.lo[0] = c_lo0, P.hi[0] = c_hi0, P.lo[1] = c_lo1, P.hi[1] = c_hi1;
-    P.info[0] = c_in0, P.info[1] = c_in1;
-    P.child = child, P.node_lo = nlo, P.node_hi = nhi, P.parent = parent;
-    P.status[0] = status, P.status[1] = status + tiles_max + 1;
-    P.ctrl = d_ctrl, P.err = d_err;
-    P.num_leaves = (int)N, P.num_meshes = m, P.radius = d0.nn_search_radius;
+    pp.lo[0] = P.c_lo[0], pp.hi[0] = P.c_hi[0], pp.lo[1] = P.c_lo[1], pp.hi[1] = P.c_hi[1];
+    pp.info[0] = P.c_in[0], pp.info[1] = P.c_in[1];
+    pp.child = P.child, pp.node_lo = P.nlo, pp.node_hi = P.nhi, pp.parent = P.parent;
+    pp.status[0] = P.status, pp.status[1] = P.status + P.tiles_max + 1;
+    pp.ctrl = P.d_ctrl, pp.err = P.d_err;
+    pp.num_leaves = (int)N, pp.num_meshes = m, pp.radius = d0.nn_search_radius;
     if (N > m && N > kTailMax) {
-        switch (B) {
-            case 128: st = launch_ploc<128>(P, tiles0, stream); break;
-            case 512: st = launch_ploc<512>(P, tiles0, stream); break;
-            default: st = launch_ploc<256>(P, tiles0, stream); break;
+        switch (P.B) {
+            case 128: st = launch_ploc_any<128>(pp, P.tiles0, stream); break;
+            case 512: st = launch_ploc_any<512>(pp, P.tiles0, stream); break;
+            default: st = launch_ploc_any<256>(pp, P.tiles0, stream); break;
         }
         if (st != DIPL_OK) return st;
     }
-    if (N > m && (st = launch_ploc_tail(P, stream)) != DIPL_OK) return st;
+    if (N > m && (st = launch_ploc_tail(pp, stream)) != DIPL_OK) return st;
 
     // ---- layout -------------------------------------------------------------------------------------
-    LayoutParams LP{child, nlo, nhi, parent, (int)N, (int)K, L};
-    uint32_t *rev_flags, *contrib;
-    int *owner_leaf, *leaf_start_of;
-    unsigned char* scan_scratch;
-    uint32_t* d_counts;  // [0] = inner nodes of the layout
-    BNode* nodes;
-    float4* tris;
-    double* d_sah;
-    RootInfo* d_roots;
-    if ((st = scratch.alloc(&rev_flags, Kalloc)) != DIPL_OK || (st = scratch.alloc(&contrib, N)) != DIPL_OK ||
-        (st = scratch.alloc(&owner_leaf, N)) != DIPL_OK || (st = scratch.alloc(&leaf_start_of, N + Kalloc)) != DIPL_OK ||
-        (st = scratch.alloc(&scan_scratch, scan_scratch_bytes(std::max(N, Kalloc)))) != DIPL_OK ||
-        (st = scratch.alloc(&d_counts, 4)) != DIPL_OK || (st = storage->alloc(&nodes, Kalloc)) != DIPL_OK ||
-        (st = storage->alloc(&tris, 3 * N)) != DIPL_OK || (st = scratch.alloc(&d_sah, 2 * m)) != DIPL_OK ||
-        (st = scratch.alloc(&d_roots, m)) != DIPL_OK)
-        return st;
-    DIPL_CUDA(cudaMemsetAsync(d_sah, 0, sizeof(double) * 2 * m, stream));
-    DIPL_CUDA(cudaMemsetAsync(d_counts, 0, 16, stream));
+    LayoutParams LP{P.child, P.nlo, P.nhi, P.parent, (int)N, (int)K, P.L};
+    DIPL_CUDA(cudaMemsetAsync(P.d_sah, 0, sizeof(double) * 2 * m, stream));
+    DIPL_CUDA(cudaMemsetAsync(P.d_counts, 0, 16, stream));
     if (K > 0) {
-        inner_flags_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, rev_flags, d_err); note_launches();
-        if ((st = exclusive_scan_u32(rev_flags, rev_flags, K, d_counts, scan_scratch, stream, d_err)) != DIPL_OK)
+        inner_flags_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.rev_flags, P.d_err);
+        note_launches();
+        if ((st = exclusive_scan_u32(P.rev_flags, P.rev_flags, K, P.d_counts, P.scan_scratch, stream, P.d_err)) !=
+            DIPL_OK)
             return st;
     }
-    leaf_owner_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, contrib, owner_leaf, d_err); note_launches();
-    if ((st = exclusive_scan_u32(contrib, contrib, N, nullptr, scan_scratch, stream, d_err)) != DIPL_OK) return st;
-    leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, d_meshes, d_offsets, m, perm, contrib, owner_leaf,
-                                                               leaf_start_of, tris, d_err); note_launches();
+    leaf_owner_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.contrib, P.owner_leaf, P.d_err);
+    note_launches();
+    if ((st = exclusive_scan_u32(P.contrib, P.contrib, N, nullptr, P.scan_scratch, stream, P.d_err)) != DIPL_OK)
+        return st;
+    leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.contrib,
+                                                               P.owner_leaf, P.leaf_start_of, P.tris, P.d_err);
+    note_launches();
     if (K > 0) {
-        node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, d_meshes, d_offsets, m, perm, rev_flags,
-                                                                   leaf_start_of, nodes, d_sah, d_err);
+        node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.rev_flags,
+                                                                   P.leaf_start_of, P.nodes, P.d_sah, P.d_err);
         note_launches();
     }
-    roots_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(LP, c_lo0, c_hi0, c_lo1, c_hi1, d_ctrl, m, rev_flags,
-                                                       leaf_start_of, d_roots, d_err); note_launches();
+    roots_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(LP, P.c_lo[0], P.c_hi[0], P.c_lo[1], P.c_hi[1], P.d_ctrl, m,
+                                                       P.rev_flags, P.leaf_start_of, P.d_roots, P.d_err);
+    note_launches();
     DIPL_CUDA(cudaGetLastError());
-
-    // ---- read back the per-mesh summary (the one host synchronisation of a build) -------------------
-    const size_t summary_bytes = sizeof(RootInfo) * m + sizeof(double) * 2 * m + 16;
-    unsigned char* host = pinned_host_buffer(summary_bytes);
-    if (!host) {
-        set_last_error("pinned host allocation failed");
-        return DIPL_ERR_OUT_OF_MEMORY;
+    if (d0.bv_type == DIPL_BV_SOBB) {
+        st = sobb_enqueue(P.child, P.nlo, P.nhi, P.parent, P.leaf_start_of, P.owner_leaf, P.tris, P.nodes, P.rev_flags,
+                          (int)N, (int)K, P.L, d0.kdop_size, P.sobb, P.snodes, stream, P.d_err);
+        if (st != DIPL_OK) return st;
     }
-    RootInfo* h_roots = reinterpret_cast<RootInfo*>(host);
-    double* h_sah = reinterpret_cast<double*>(host + sizeof(RootInfo) * m);
-    uint32_t* h_tail = reinterpret_cast<uint32_t*>(host + sizeof(RootInfo) * m + sizeof(double) * 2 * m);
-    DIPL_CUDA(cudaMemcpyAsync(h_roots, d_roots, sizeof(RootInfo) * m, cudaMemcpyDeviceToHost, stream));
-    DIPL_CUDA(cudaMemcpyAsync(h_sah, d_sah, sizeof(double) * 2 * m, cudaMemcpyDeviceToHost, stream));
-    DIPL_CUDA(cudaMemcpyAsync(h_tail, d_counts, 4, cudaMemcpyDeviceToHost, stream));
-    DIPL_CUDA(cudaMemcpyAsync(h_tail + 1, &d_ctrl->iterations, 4, cudaMemcpyDeviceToHost, stream));
-    DIPL_CUDA(cudaMemcpyAsync(h_tail + 2, d_err, 4, cudaMemcpyDeviceToHost, stream));
-    DIPL_CUDA(cudaStreamSynchronize(stream));
+    // ---- the per-mesh summary to pinned host memory --------------------------------------------------
+    RootInfo* h_roots = reinterpret_cast<RootInfo*>(P.h_summary);
+    double* h_sah = reinterpret_cast<double*>(P.h_summary + sizeof(RootInfo) * m);
+    uint32_t* h_tail = reinterpret_cast<uint32_t*>(P.h_summary + sizeof(RootInfo) * m + sizeof(double) * 2 * m);
+    DIPL_CUDA(cudaMemcpyAsync(h_roots, P.d_roots, sizeof(RootInfo) * m, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_sah, P.d_sah, sizeof(double) * 2 * m, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_tail, P.d_counts, 4, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_tail + 1, &P.d_ctrl->iterations, 4, cudaMemcpyDeviceToHost, stream));
+    DIPL_CUDA(cudaMemcpyAsync(h_tail + 2, P.d_err, 4, cudaMemcpyDeviceToHost, stream));
+    return DIPL_OK;
+}
+
+// After the stream synchronised: check the error word, build the 8-wide layout if asked, make the handles.
+static dipl_status plan_finish(BuildPlan& P, dipl_bvh** out, bool allow_wide) {
+    const int m = P.m;
+    const dipl_build_desc& d0 = P.d0;
+    auto make_handle = [&](int i) {
+        auto* h = new dipl_bvh();
+        h->storage = P.out;
+        h->num_triangles = P.descs[i].num_triangles;
+        h->code_type = P.descs[i].code_type;
+        h->bv_type = P.descs[i].bv_type;
+        h->layout = P.descs[i].layout;
+        h->max_leaf = P.descs[i].max_triangles_per_leaf;
+        h->radius = P.descs[i].nn_search_radius;
+        h->kdop = P.descs[i].kdop_size;
+        h->d_err = P.d_err;
+        h->root = 0;
+        return h;
+    };
+    if (m == 0) {
+        for (int i = 0; i < P.count; ++i) out[i] = make_handle(i);
+        return DIPL_OK;
+    }
+    const RootInfo* h_roots = reinterpret_cast<const RootInfo*>(P.h_summary);
+    const double* h_sah = reinterpret_cast<const double*>(P.h_summary + sizeof(RootInfo) * m);
+    const uint32_t* h_tail =
+        reinterpret_cast<const uint32_t*>(P.h_summary + sizeof(RootInfo) * m + sizeof(double) * 2 * m);
     const uint32_t err = h_tail[2];
     if (err != 0u) {
         set_last_error(err & kErrTimeout ? "build: a bounded device wait timed out"
@@ -1390,57 +1482,46 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
     }
     const int64_t inner_total = (int64_t)h_tail[0];
     const int iterations = (int)h_tail[1];
-
-    // ---- SOBB form: skewed oriented child boxes over the same layout ---------------------------------
-    SNode* snodes = nullptr;
-    if (d0.bv_type == DIPL_BV_SOBB) {
-        st = build_sobb(child, nlo, nhi, parent, leaf_start_of, owner_leaf, tris, nodes, rev_flags, (int)N, (int)K, L,
-                        d0.kdop_size, *storage, stream, d_err, &snodes);
-        if (st != DIPL_OK) return st;
-        if ((st = check_device_error(d_err, stream, "SOBB refit")) != DIPL_OK) return st;
-    }
-
-    // ---- precision form: 8-wide quantised layout over the same clustering ---------------------------
     WNode* wnodes = nullptr;
     float4* wtris = nullptr;
     int64_t wcount = 0;
     std::vector<int> wroots, wlevels;
     if (d0.layout == DIPL_LAYOUT_WIDE8_Q8) {
+        if (!allow_wide) {
+            set_last_error("the 8-wide layout cannot be captured in a build plan (it reads level sizes back)");
+            return DIPL_ERR_UNSUPPORTED;
+        }
         std::vector<int> root_ids(m), root_counts(m);
         for (int k = 0; k < m; ++k) root_ids[k] = h_roots[k].root_id, root_counts[k] = h_roots[k].num_leaves;
-        st = build_wide(child, nlo, nhi, leaf_start_of, tris, (int)N, L, root_ids, root_counts, *storage, stream,
-                        d_err, &wnodes, &wtris, &wcount, wroots, wlevels);
+        dipl_status st = build_wide(P.child, P.nlo, P.nhi, P.leaf_start_of, P.tris, (int)P.N, P.L, root_ids,
+                                    root_counts, *P.out, P.stream, P.d_err, &wnodes, &wtris, &wcount, wroots, wlevels);
         if (st != DIPL_OK) return st;
     }
-
-    std::vector<dipl_bvh*> made;
-    for (int i = 0; i < count; ++i) {
+    for (int i = 0; i < P.count; ++i) {
         dipl_bvh* h = make_handle(i);
-        h->nodes = nodes;
-        h->tris = tris;
-        h->perm = reinterpret_cast<int32_t*>(perm);
-        h->children = child;
-        h->node_lo = nlo;
-        h->node_hi = nhi;
-        h->batch_leaves = N;
+        h->nodes = d0.bv_type == DIPL_BV_SOBB ? static_cast<void*>(P.snodes) : static_cast<void*>(P.nodes);
+        h->tris = P.tris;
+        h->perm = reinterpret_cast<int32_t*>(P.perm);
+        h->children = P.child;
+        h->node_lo = P.nlo;
+        h->node_hi = P.nhi;
+        h->batch_leaves = P.N;
         h->node_capacity = inner_total;
         h->ploc_iterations = iterations;
-        const int k = mesh_of_desc[i];
+        const int k = P.mesh_of_desc[i];
         if (k >= 0) {
             const RootInfo& ri = h_roots[k];
             h->root = ri.root_ref;
             h->depth = ri.depth;
-            h->leaf_base = offsets[k];
+            h->leaf_base = P.offsets[k];
             h->num_nodes = (int64_t)h_sah[2 * k + 1];
             h->sah_area = ri.root_area;
             h->sah_sum = h_sah[2 * k] + ri.leaf_cost;
-            h->num_leaves = 0;
             if (d0.layout == DIPL_LAYOUT_WIDE8_Q8) {
                 h->root = wroots[k];
                 h->depth = wlevels[k];
             }
         }
-        if (d0.bv_type == DIPL_BV_SOBB) h->nodes = snodes;
         if (d0.layout == DIPL_LAYOUT_WIDE8_Q8) {
             h->nodes = wnodes;
             h->tris = wtris;
@@ -1449,10 +1530,92 @@ dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** ou
             h->num_nodes = wcount;
         }
         out[i] = h;
-        made.push_back(h);
     }
     return DIPL_OK;
 }
+
+dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** out, cudaStream_t stream) {
+    DIPL_CHECK_ARG(descs && out && count >= 1, "descs/out must be non-NULL and count >= 1");
+    for (int i = 0; i < count; ++i) out[i] = nullptr;
+    BuildPlan P;
+    dipl_status st = plan_prepare(P, descs, count, stream, false);
+    if (st != DIPL_OK) return st;
+    if ((st = plan_enqueue(P, stream)) != DIPL_OK) return st;
+    if (P.m > 0) DIPL_CUDA(cudaStreamSynchronize(stream));  // the build's one host synchronisation
+    return plan_finish(P, out, true);
+}
+
+}  // namespace dipl
+
+// ---- build plans: a batch captured once into a CUDA graph and replayed ---------------------------------
+struct dipl_build_plan {
+    dipl::BuildPlan plan;
+};
+
+namespace dipl {
+
+dipl_status plan_create(const dipl_build_desc* descs, int count, dipl_build_plan** out, cudaStream_t stream) {
+    DIPL_CHECK_ARG(out != nullptr, "out must be non-NULL");
+    *out = nullptr;
+    auto holder = std::make_unique<dipl_build_plan>();
+    BuildPlan& P = holder->plan;
+    dipl_status st = plan_prepare(P, descs, count, stream, true);
+    if (st != DIPL_OK) return st;
+    if (P.d0.layout == DIPL_LAYOUT_WIDE8_Q8) {
+        set_last_error("the 8-wide layout cannot be captured in a build plan (it reads level sizes back)");
+        return DIPL_ERR_UNSUPPORTED;
+    }
+    // run once eagerly (sets kernel attributes, validates), then capture the same sequence
+    if ((st = plan_enqueue(P, stream)) != DIPL_OK) return st;
+    DIPL_CUDA(cudaStreamSynchronize(stream));
+    cudaStream_t cap;
+    DIPL_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        st = plan_enqueue(P, cap);
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+        if (st == DIPL_OK && e2 != cudaSuccess) st = cuda_status(e2, "cudaStreamEndCapture");
+        if (st == DIPL_OK) {
+            P.graph = g;
+            e2 = cudaGraphInstantiate(&P.graph_exec, g, 0);
+            if (e2 != cudaSuccess) st = cuda_status(e2, "cudaGraphInstantiate");
+            size_t nn = 0;
+            if (st == DIPL_OK && cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+                std::vector<cudaGraphNode_t> nodes_(nn);
+                if (cudaGraphGetNodes(g, nodes_.data(), &nn) == cudaSuccess)
+                    for (auto nd : nodes_) {
+                        cudaGraphNodeType t;
+                        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++P.graph_kernels;
+                    }
+            }
+        } else if (g) {
+            cudaGraphDestroy(g);
+        }
+    } else {
+        st = cuda_status(e, "cudaStreamBeginCapture");
+    }
+    cudaStreamDestroy(cap);
+    if (st != DIPL_OK) return st;
+    *out = holder.release();
+    return DIPL_OK;
+}
+
+dipl_status plan_launch(dipl_build_plan* plan, cudaStream_t stream) {
+    DIPL_CHECK_ARG(plan != nullptr, "plan must be non-NULL");
+    if (plan->plan.m == 0) return DIPL_OK;
+    DIPL_CUDA(cudaGraphLaunch(plan->plan.graph_exec, stream));
+    note_launches(plan->plan.graph_kernels);
+    return DIPL_OK;
+}
+
+dipl_status plan_get_bvhs(dipl_build_plan* plan, dipl_bvh** out, cudaStream_t stream) {
+    DIPL_CHECK_ARG(plan && out, "plan/out must be non-NULL");
+    DIPL_CUDA(cudaStreamSynchronize(stream));
+    return plan_finish(plan->plan, out, false);
+}
+
+void plan_destroy(dipl_build_plan* plan) { delete plan; }
 
 }  // namespace dipl
 

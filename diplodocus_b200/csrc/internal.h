@@ -106,6 +106,10 @@ namespace dipl {
 
 // ---- build / trace entry points used by api.cu ---------------------------------------------------
 dipl_status build_batched(const dipl_build_desc* descs, int count, dipl_bvh** out, cudaStream_t stream);
+dipl_status plan_create(const dipl_build_desc* descs, int count, dipl_build_plan** out, cudaStream_t stream);
+dipl_status plan_launch(dipl_build_plan* plan, cudaStream_t stream);
+dipl_status plan_get_bvhs(dipl_build_plan* plan, dipl_bvh** out, cudaStream_t stream);
+void plan_destroy(dipl_build_plan* plan);
 dipl_status compute_codes(const dipl_build_desc* desc, void* d_codes, cudaStream_t stream);
 dipl_status trace_closest(const dipl_bvh* bvh, const dipl_ray* rays, int64_t n, dipl_hit* hits, int leaf_test,
                           uint32_t flags, unsigned long long* counters, cudaStream_t stream);
@@ -133,10 +137,17 @@ dipl_status trace_wide(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_
                        uint32_t flags, unsigned long long* counters, bool any, cudaStream_t s);
 
 // SOBB form (sobb.cu): skewed oriented child boxes refitted over the binary layout, and their traversal.
-dipl_status build_sobb(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
-                       const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
-                       const uint32_t* rev_index, int N, int K, int L, int kdop_size, Storage& storage,
-                       cudaStream_t s, uint32_t* d_err, SNode** out_nodes);
+struct SobbScratch {
+    void* kdop = nullptr;  // k-DOP per node id
+    float* mag = nullptr;  // coordinate magnitude per node id
+    unsigned* arrivals = nullptr;
+    int triples = 0;
+};
+dipl_status sobb_prepare(long long N, long long K, Storage& work, Storage& out, SobbScratch* sc, SNode** snodes);
+dipl_status sobb_enqueue(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
+                         const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
+                         const uint32_t* rev_index, int N, int K, int L, int kdop_size, const SobbScratch& sc,
+                         SNode* snodes, cudaStream_t s, uint32_t* d_err);
 dipl_status trace_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, int leaf_test,
                        uint32_t flags, unsigned long long* counters, bool any, cudaStream_t s);
 

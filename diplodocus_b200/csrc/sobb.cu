@@ -371,34 +371,39 @@ dipl_status upload_triples() {
 
 }  // namespace
 
-// Refits SOBB child boxes over the binary layout (bnodes, final inner indices rev_index) into snodes.
-dipl_status build_sobb(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
-                       const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
-                       const uint32_t* rev_index, int N, int K, int L, int kdop_size, Storage& storage,
-                       cudaStream_t s, uint32_t* d_err, SNode** out_nodes) {
+// Allocations of the SOBB refit (and the one-time upload of the direction triples).
+dipl_status sobb_prepare(long long N, long long K, Storage& work, Storage& out, SobbScratch* sc, SNode** snodes) {
     dipl_status st = DIPL_OK;
     std::call_once(g_triples_once, [&] { st = upload_triples(); });
     if (st != DIPL_OK) return st;
-    ScratchArena scratch(s);
+    const long long Kalloc = std::max<long long>(K, 1);
     Kdop* kdop;
-    float* mag;
-    unsigned* arrivals;
-    SNode* snodes;
-    const int Kalloc = std::max(K, 1);
-    if ((st = scratch.alloc(&kdop, (size_t)N + Kalloc)) != DIPL_OK || (st = scratch.alloc(&mag, (size_t)N + Kalloc)) != DIPL_OK ||
-        (st = scratch.alloc(&arrivals, Kalloc)) != DIPL_OK || (st = storage.alloc(&snodes, Kalloc)) != DIPL_OK)
+    if ((st = work.alloc(&kdop, (size_t)(N + Kalloc))) != DIPL_OK ||
+        (st = work.alloc(&sc->mag, (size_t)(N + Kalloc))) != DIPL_OK ||
+        (st = work.alloc(&sc->arrivals, (size_t)Kalloc)) != DIPL_OK || (st = out.alloc(snodes, (size_t)Kalloc)) != DIPL_OK)
         return st;
-    DIPL_CUDA(cudaMemsetAsync(arrivals, 0, sizeof(unsigned) * Kalloc, s));
+    sc->kdop = kdop;
+    sc->triples = g_triples;
+    return DIPL_OK;
+}
+
+// Refits SOBB child boxes over the binary layout (bnodes, final inner indices rev_index) into snodes.
+dipl_status sobb_enqueue(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
+                         const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
+                         const uint32_t* rev_index, int N, int K, int L, int kdop_size, const SobbScratch& sc,
+                         SNode* snodes, cudaStream_t s, uint32_t* d_err) {
+    const int Kalloc = std::max(K, 1);
+    Kdop* kdop = static_cast<Kdop*>(sc.kdop);
+    DIPL_CUDA(cudaMemsetAsync(sc.arrivals, 0, sizeof(unsigned) * Kalloc, s));
     SobbIn S{child, node_lo, node_hi, parent, leaf_start_of, btris, N, L, kdop_size / 2};
-    kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, kdop, mag, arrivals, d_err);
+    kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, kdop, sc.mag, sc.arrivals, d_err);
     note_launches();
     if (K > 0) {
-        sobb_node_kernel<<<(unsigned)((K + 255) / 256), 256, 0, s>>>(S, bnodes, rev_index, K, kdop, mag, g_triples,
-                                                                      snodes, d_err);
+        sobb_node_kernel<<<(unsigned)((K + 255) / 256), 256, 0, s>>>(S, bnodes, rev_index, K, kdop, sc.mag,
+                                                                      sc.triples, snodes, d_err);
         note_launches();
     }
     DIPL_CUDA(cudaGetLastError());
-    *out_nodes = snodes;
     return DIPL_OK;
 }
 

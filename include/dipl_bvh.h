@@ -131,6 +131,28 @@ DIPL_API dipl_status dipl_bvh_build(const dipl_build_desc* desc, dipl_bvh** out,
  * share the build options. Returns when complete, like dipl_bvh_build. */
 DIPL_API dipl_status dipl_bvh_build_batched(const dipl_build_desc* descs, int32_t count, dipl_bvh** out, void* stream);
 
+/* Build plans (batching form). A plan fixes a batch of meshes (their vertex pointers and sizes and one set
+ * of options), allocates everything once, runs the build once and captures the whole pipeline (bounds, codes,
+ * sort, the persistent clustering launch, layout) into one CUDA graph. dipl_build_plan_launch replays it,
+ * rebuilding every BVH from the current contents of the vertex arrays (e.g. after a deformation), with no
+ * allocation and no host synchronisation; dipl_build_plan_get_bvhs waits for the stream and returns one
+ * handle per mesh for the latest build (valid until the next launch; destroy them with dipl_bvh_destroy).
+ * The 8-wide layout is not available in plans (its build reads level sizes back). */
+typedef struct dipl_build_plan dipl_build_plan;
+DIPL_API dipl_status dipl_build_plan_create(const dipl_build_desc* descs, int32_t count, dipl_build_plan** out,
+                                            void* stream);
+DIPL_API dipl_status dipl_build_plan_launch(dipl_build_plan* plan, void* stream);
+DIPL_API dipl_status dipl_build_plan_get_bvhs(dipl_build_plan* plan, dipl_bvh** out, void* stream);
+DIPL_API dipl_status dipl_build_plan_destroy(dipl_build_plan* plan);
+
+/* Autotuner of the build knobs (PLOC radius, PLOC block size, sort digit width) for a batch: times real builds
+ * of these meshes and keeps the fastest setting whose SAH cost is within 2% of the radius-16 default; the
+ * winner is cached per (code, bounding volume, layout, leaf size, size bucket floor(log2 total triangles)) in
+ * `cache_path` (one JSON object per line; NULL = no cache). tuned[i] = descs[i] with the chosen knobs;
+ * *from_cache (may be NULL) tells whether the cache answered. Synchronises `stream` (it builds). */
+DIPL_API dipl_status dipl_autotune_build(const dipl_build_desc* descs, int32_t count, const char* cache_path,
+                                         dipl_build_desc* tuned, int32_t* from_cache, void* stream);
+
 /* Closest hit for n rays (device arrays of dipl_ray / dipl_hit). Replaces
  * AccelerationStructure::Intersect (acceleration_structure.h:17; SBvh::Intersect sbvh.cc:60-145) and the
  * device brute force DummyIntersect (gpu_renderer_util.h:29-72). Exact-t ties resolve to the lowest

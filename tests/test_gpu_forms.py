@@ -118,3 +118,42 @@ def test_adjoint_matches_fp64_central_differences():
             rerr.append(abs(grad[ray, a] - fd) / max(abs(fd), 1e-3))
     rerr = np.array(rerr)
     assert np.median(rerr) < 1e-3 and np.quantile(rerr, 0.95) < 2e-2, (np.median(rerr), np.quantile(rerr, 0.95))
+
+
+def test_build_plan_graph_replay_matches_fresh_builds(orc):
+    """The graph-captured batch rebuilds from the current vertices: equal to fresh builds before and after a
+    deformation of the vertex arrays."""
+    meshes = [S.uv_sphere(nu, nu // 2, 1.0, (0, 0, 0), displacement=0.05, seed=30 + i)
+              for i, nu in enumerate((16, 64, 40, 128))] + [S.soup(3000, seed=9)]
+    for kind in (A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmcSobb):
+        cfg = A.AccelerationStructureConfig(kind)
+        plan = A.BuildPlan(cfg, [torch.from_numpy(m) for m in meshes])
+        for step in range(2):
+            if step == 1:  # deform in place: the plan holds the same device arrays
+                for v in plan.verts:
+                    for x in v:
+                        x.mul_(1.1).add_(0.01)
+            plan.launch()
+            bvhs = plan.bvhs()
+            for i, b in enumerate(bvhs):
+                tris_now = torch.stack([x for x in plan.verts[i]], dim=1).cpu().numpy()
+                rays = S.sphere_inward_rays(1024, seed=i) if i < 4 else S.random_rays(1024, seed=i)
+                p1, t1, _, _ = trace(b, rays)
+                h = orc.brute(tris_now, rays)
+                np.testing.assert_array_equal(p1, h.prim)
+                np.testing.assert_array_equal(fbits(t1), fbits(h.t))
+        plan.close()
+
+
+def test_autotuner_picks_valid_knobs_and_caches(tmp_path):
+    meshes = [torch.from_numpy(S.uv_sphere(256, 128, 1.0, (0, 0, 0), displacement=0.05, seed=3))]
+    cfg = A.AccelerationStructureConfig()
+    cache = str(tmp_path / "tune.jsonl")
+    tuned, from_cache, _ = A.autotune(cfg, meshes, cache)
+    assert not from_cache
+    d = tuned[0]
+    assert d.nn_search_radius in (8, 12, 16, 24, 32) and d.ploc_block_size in (128, 256, 512)
+    assert d.sort_digit_bits in (6, 8, 10)
+    tuned2, from_cache2, _ = A.autotune(cfg, meshes, cache)
+    assert from_cache2 and tuned2[0].nn_search_radius == d.nn_search_radius
+    assert '"key": "morton30/aabb/binary/L4/b' in open(cache).read()
