@@ -46,29 +46,60 @@ def peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+    """Samples SM clocks and clock-event (throttle) reasons through NVML while the timed region runs.
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    NVML reads take about a millisecond, so even a timed region of a few tens of milliseconds gets a few
+    dozen samples (nvidia-smi itself takes ~100 ms per query). Falls back to nvidia-smi when NVML is absent.
+    """
 
-    def __init__(self, index):
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, index, period_s=0.01):
         self.index = index
-        self.samples = []
+        self.period = period_s
+        self.samples = []  # (sm_mhz, max_mhz, reason_bits)
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        self._h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            h = None
+            try:
+                pr = torch.cuda.get_device_properties(index)
+                bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self._nvml, self._h = pynvml, h
+        except Exception:
+            self._nvml = None
+
+    def _sample(self):
+        if self._nvml is not None:
+            n = self._nvml
+            sm = n.nvmlDeviceGetClockInfo(self._h, n.NVML_CLOCK_SM)
+            mx = n.nvmlDeviceGetMaxClockInfo(self._h, n.NVML_CLOCK_SM)
+            rs = n.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+            return float(sm), float(mx), int(rs)
+        out = subprocess.run(["nvidia-smi", "-i", str(self.index),
+                              "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                             timeout=5).stdout.strip()
+        a = [x.strip() for x in out.split(",")]
+        return float(a[0]), float(a[1]), int(a[2], 16)
 
     def _run(self):
-        while not self._stop.is_set():
+        while True:
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
+                self.samples.append(self._sample())
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            if self._stop.wait(self.period):
+                break
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -81,14 +112,12 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and "Active" in s[3 + k]
-                          and "Not" not in s[3 + k]})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({name for s in self.samples for name, bit in self.REASONS if s[2] & bit})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": reasons, "samples": len(self.samples),
+                "source": "nvml" if self._nvml is not None else "nvidia-smi"}
 
 
 def workload(name, rays_override=None):
@@ -346,13 +375,214 @@ def run_gpu(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+
+
+# ---------------------------------------------------------------------------------------------------
+# The other configured workloads (one JSON line each; the default line above is the contract's).
+# ---------------------------------------------------------------------------------------------------
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _time(fn, reps, warm=2):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    a, b = _events()
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def _line(workload, value, unit, extra):
+    d = {"metric": METRIC, "workload": workload, "value": round(value, 4), "unit": unit, "n_gpus": 1,
+         "higher_is_better": True, "dtype": "f32", "data": "synthetic"}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def run_small(args):
+    """Small scene: agreement classes of the GPU hits against the reference SBvh and brute force."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from diplodocus_b200 import accel as A
+    from diplodocus_b200 import scenes as S
+    tris, rays = S.small_scene()
+    ref = O.RefOracle()
+    sb = ref.sbvh(tris)
+    prim_rays = rays
+    bvh = A.GpuPlocBvh().Build(A.AccelerationStructureConfig(), A.Stats(), torch.from_numpy(tris))
+    h0 = bvh.Intersect(A.Stats(), torch.from_numpy(prim_rays))
+    p0, t0 = h0.prim.cpu().numpy(), h0.t.cpu().numpy()
+    br, mask = S.bounce_rays(tris, prim_rays, p0, t0, seed=11)
+    rays = np.concatenate([prim_rays, br[mask]])
+    tr = torch.from_numpy(rays).cuda()
+    ms_build = _time(lambda: A.GpuPlocBvh().Build(A.AccelerationStructureConfig(), A.Stats(), torch.from_numpy(tris)), 10)
+    ms_trace = _time(lambda: bvh.Intersect(A.Stats(), tr), 20)
+    h = bvh.Intersect(A.Stats(), tr)
+    gp, gt = h.prim.cpu().numpy(), h.t.cpu().numpy()
+    hs = sb.trace(rays)
+    hb = ref.brute(tris, rays)
+    exact = (gp == hb.prim) & (gt.view(np.uint32) == hb.t.view(np.uint32))
+    vs_sbvh_same = gp == hs.prim
+    diff = ~vs_sbvh_same
+    sb_t = np.where(hs.prim >= 0, hs.t, np.inf)
+    s_class = diff & exact & (sb_t >= gt)  # SBvh missed or took a farther/later-tied hit that brute force beats
+    _line("small", len(tris) / ms_build / 1e3, "Mtri/s", {
+        "config": {"workload": "small", "triangles": len(tris), "rays": len(rays),
+                   "rays_detail": "512x512 pinhole primary + one cosine bounce per primary hit"},
+        "build_ms": round(ms_build, 4), "trace": {"value": round(len(rays) / ms_trace / 1e3, 2), "unit": "Mrays/s"},
+        "sah_cost": round(bvh.sah_cost(), 4), "sbvh_sah_cost": round(sb.sah_cost()[0], 4),
+        "agreement_vs_brute_force": {"E_or_T_bit_exact": int(exact.sum()), "F": int((~exact).sum())},
+        "agreement_vs_sbvh": {"same_id": int(vs_sbvh_same.sum()), "S_sbvh_wrong": int(s_class.sum()),
+                              "F": int((diff & ~s_class).sum())},
+        "sbvh_build_ms": round(sb.build_ms, 3)})
+
+
+def run_soup16m(args):
+    """16M soup: EMC60+SOBB and the 8-wide quantised form against binary FP32 nodes; t/u/v error vs FP64."""
+    import torch
+    from diplodocus_b200 import accel as A
+    from diplodocus_b200 import scenes as S
+    n = args.soup_tris
+    tris = S.soup(n, seed=3)
+    nr = args.rays or (1 << 22)
+    rays = torch.from_numpy(S.random_rays(nr, seed=3)).cuda()
+    tt = torch.from_numpy(tris).cuda()  # resident in HBM: the timed builds exclude host->device copies
+    v = A.soa_vertices(tt)
+    lib = __import__("diplodocus_b200._lib", fromlist=["x"]).load()
+    import ctypes as C
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def build_only(desc):
+        h = C.c_void_p(0)
+        lib.dipl_bvh_build(C.byref(desc), C.byref(h), sp)
+        lib.dipl_bvh_destroy(h)
+
+    out = {}
+    ref_prim = None
+    for name, kind, layout in [("ploc_binary", A.AccelerationStructureType.kPloc, "binary"),
+                               ("ploc_emc", A.AccelerationStructureType.kPlocEmc, "binary"),
+                               ("ploc_emc_sobb", A.AccelerationStructureType.kPlocEmcSobb, "binary"),
+                               ("ploc_wide8_q8", A.AccelerationStructureType.kPloc, "wide8_q8")]:
+        cfg = A.AccelerationStructureConfig(kind, layout=layout)
+        bvh = A.GpuPlocBvh().Build(cfg, A.Stats(), tt)
+        desc = A.make_desc(*v, cfg)
+        ms_build = _time(lambda: build_only(desc), 3, warm=1)
+        ms_trace = _time(lambda: bvh.Intersect(A.Stats(), rays), 2, warm=1)
+        h = bvh.Intersect(A.Stats(), rays)
+        prim = h.prim.cpu().numpy()
+        if ref_prim is None:
+            ref_prim = prim
+        tuv = A.reintersect_f64(bvh._v, rays, h).cpu().numpy()
+        hit = prim >= 0
+        t32 = h.t.cpu().numpy()[hit].astype(np.float64)
+        u32 = h.u.cpu().numpy()[hit].astype(np.float64)
+        rel_t = np.abs(t32 - tuv[hit, 0]) / np.maximum(np.abs(tuv[hit, 0]), 1e-30)
+        info = bvh.info()
+        out[name] = {"build_ms": round(ms_build, 3), "build_mtri_s": round(n / ms_build / 1e3, 1),
+                     "trace_mrays_s": round(nr / ms_trace / 1e3, 2), "sah_cost": round(bvh.sah_cost(), 3),
+                     "node_bytes": int(info.node_bytes), "same_hits_as_binary": float((prim == ref_prim).mean()),
+                     "t_rel_err_vs_fp64": {"median": float(np.median(rel_t)), "p99": float(np.quantile(rel_t, 0.99)),
+                                           "max": float(rel_t.max())},
+                     "u_abs_err_vs_fp64_max": float(np.abs(u32 - tuv[hit, 1]).max())}
+        del bvh
+        torch.cuda.empty_cache()
+    _line("soup16m", out["ploc_emc_sobb"]["build_mtri_s"], "Mtri/s", {
+        "config": {"workload": "soup16m", "triangles": n, "rays": nr,
+                   "description": "log-normal soup (mu=-6, sigma=1.5, 20% 1:50 skinny), random rays in the cube"},
+        "variants": out})
+
+
+def run_batched(args):
+    """256 noise-displaced spheres (1k..2M triangles): one graph-replayed plan vs 256 sequential builds."""
+    import torch
+    from diplodocus_b200 import accel as A
+    from diplodocus_b200 import scenes as S
+    meshes = [torch.from_numpy(m) for m in S.batched_meshes(args.batch_count)]
+    total = sum(m.shape[0] for m in meshes)
+    cfg = A.AccelerationStructureConfig()
+    verts = [A.soa_vertices(m) for m in meshes]
+    descs = [A.make_desc(*v, cfg) for v in verts]
+    lib = __import__("diplodocus_b200._lib", fromlist=["x"]).load()
+    import ctypes as C
+
+    def plain_all():
+        for d in descs:
+            h = C.c_void_p(0)
+            lib.dipl_bvh_build(C.byref(d), C.byref(h), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+            lib.dipl_bvh_destroy(h)
+
+    ms_plain = _time(plain_all, 2, warm=1)
+    cache = os.path.join("/tmp", "dipl_tune_cache.jsonl")
+    t0 = time.perf_counter()
+    tuned, from_cache, tverts = A.autotune(cfg, meshes, cache)
+    tune_s = time.perf_counter() - t0
+    plan = A.BuildPlan(cfg, meshes, tuned_descs=tuned)
+    del tverts
+    ms_plan = _time(plan.launch, 5, warm=2)
+    bvhs = plan.bvhs()
+    nr = 65536
+    rays = torch.from_numpy(S.sphere_inward_rays(nr, seed=4)).cuda()
+    ms_tr = [_time(lambda b=b: b.Intersect(A.Stats(), rays), 2, warm=1) for b in bvhs[:: max(1, len(bvhs) // 16)]]
+    # hit agreement between the plan's BVHs and plain builds on a few meshes
+    agree = []
+    for i in range(0, len(meshes), max(1, len(meshes) // 8)):
+        ref = A.GpuPlocBvh().Build(cfg, A.Stats(), meshes[i])
+        a = ref.Intersect(A.Stats(), rays).prim.cpu().numpy()
+        b = bvhs[i].Intersect(A.Stats(), rays).prim.cpu().numpy()
+        agree.append(float((a == b).mean()))
+    d0 = tuned[0]
+    _line("batched", total / ms_plan / 1e3, "Mtri/s", {
+        "config": {"workload": "batched", "meshes": len(meshes), "triangles": int(total),
+                   "sizes": "log-uniform 1k..2M per mesh", "rays_per_mesh": nr},
+        "plan_graph_ms": round(ms_plan, 3), "sequential_plain_ms": round(ms_plain, 3),
+        "speedup_batched_vs_plain": round(ms_plain / ms_plan, 3),
+        "plain_mtri_s": round(total / ms_plain / 1e3, 1),
+        "autotuned": {"radius": d0.nn_search_radius, "block": d0.ploc_block_size, "digits": d0.sort_digit_bits,
+                      "from_cache": from_cache, "tune_s": round(tune_s, 2)},
+        "trace_mrays_s_per_mesh_median": round(float(np.median([nr / t / 1e3 for t in ms_tr])), 2),
+        "hit_agreement_plan_vs_plain": min(agree)})
+    plan.close()
+
+
+def run_diff(args):
+    """Differentiation: 65k-triangle displaced sphere, 1024x1024 primary rays, forward + adjoint."""
+    import torch
+    from diplodocus_b200 import accel as A
+    from diplodocus_b200 import scenes as S
+    verts, idx, rays_np = S.diff_scene()
+    tris = verts[idx].astype(np.float32)
+    bvh = A.GpuPlocBvh().Build(A.AccelerationStructureConfig(), A.Stats(), torch.from_numpy(tris))
+    rays = torch.from_numpy(rays_np).cuda()
+    h = bvh.Intersect(A.Stats(), rays)
+    g = torch.stack([torch.where(h.prim >= 0, 0.06 * h.t, torch.zeros_like(h.t)), torch.zeros_like(h.t),
+                     torch.zeros_like(h.t)], 1)
+    ms_fwd = _time(lambda: bvh.Intersect(A.Stats(), rays), 10)
+    ms_adj = _time(lambda: A.trace_adjoint(bvh._v, rays, h, g), 10)
+    nr = rays.shape[0]
+    _line("diff", nr / ms_adj / 1e3, "Mrays/s", {
+        "config": {"workload": "diff", "triangles": len(tris), "rays": nr},
+        "forward_mrays_s": round(nr / ms_fwd / 1e3, 2), "adjoint_ms": round(ms_adj, 4),
+        "hit_rate": float((h.prim >= 0).float().mean().item()),
+        "check": "tests/test_gpu_forms.py::test_adjoint_matches_fp64_central_differences"})
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="dipl", choices=["dipl", "reference"])
-    ap.add_argument("--workload", default="displaced_sphere", choices=["displaced_sphere", "small", "soup16m"])
+    ap.add_argument("--workload", default="displaced_sphere",
+                    choices=["displaced_sphere", "small", "soup16m", "batched", "diff"])
+    ap.add_argument("--soup-tris", type=int, default=16 * 1024 * 1024)
+    ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--code", default="morton30", choices=["morton30", "emc60"])
     ap.add_argument("--radius", type=int, default=16)
     ap.add_argument("--leaf-test", default="ref_mt", choices=["ref_mt", "watertight"])
@@ -365,6 +595,11 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload in ("small", "soup16m", "batched", "diff") and world == 1:
+        import torch
+        torch.cuda.set_device(local_rank)
+        {"small": run_small, "soup16m": run_soup16m, "batched": run_batched, "diff": run_diff}[args.workload](args)
         return
     if world > 1:
         import datetime

@@ -354,7 +354,12 @@ class BuildPlan:
         n = len(self.verts)
         self.descs = (L.BuildDesc * n)()
         for i, v in enumerate(self.verts):
-            self.descs[i] = tuned_descs[i] if tuned_descs is not None else make_desc(*v, config)
+            self.descs[i] = make_desc(*v, config)
+            if tuned_descs is not None:  # take the tuned knobs, keep this plan's own vertex arrays
+                t = tuned_descs[i]
+                self.descs[i].nn_search_radius = t.nn_search_radius
+                self.descs[i].ploc_block_size = t.ploc_block_size
+                self.descs[i].sort_digit_bits = t.sort_digit_bits
         self._h = C.c_void_p(0)
         L.check(self._lib.dipl_build_plan_create(self.descs, n, C.byref(self._h), _stream()), "dipl_build_plan_create")
 
