@@ -61,9 +61,22 @@ __device__ __forceinline__ int scount(const SobbIn& S, int id) {
     return id < S.N ? 1 : __float_as_int(S.node_lo[id - S.N].w);
 }
 
-// k-DOP of a final leaf from its triangles, then up the tree: the second arriver at a parent merges.
-__global__ void kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf, Kdop* __restrict__ kdop,
-                                  float* __restrict__ mag, unsigned* __restrict__ arrivals, const uint32_t* err) {
+// Stores / loads a k-DOP as 8 float4 (the whole struct stays in registers: every index is a constant).
+__device__ __forceinline__ void store_kdop(Kdop* dst, const Kdop& k) {
+    float4* d = reinterpret_cast<float4*>(dst);
+#pragma unroll
+    for (int i = 0; i < kDirs / 4; ++i) {
+        d[i] = make_float4(k.lo[4 * i], k.lo[4 * i + 1], k.lo[4 * i + 2], k.lo[4 * i + 3]);
+        d[kDirs / 4 + i] = make_float4(k.hi[4 * i], k.hi[4 * i + 1], k.hi[4 * i + 2], k.hi[4 * i + 3]);
+    }
+}
+
+// k-DOP of a final leaf from its triangles, then up the tree: the second arriver at a parent merges. All 16
+// table directions are always projected (a smaller kdop_size only restricts which triples the node kernel
+// considers), so the k-DOP never leaves registers.
+__global__ void __launch_bounds__(256) kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf,
+                                                         Kdop* __restrict__ kdop, float* __restrict__ mag,
+                                                         unsigned* __restrict__ arrivals, const uint32_t* err) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= S.N || *err != 0u) return;
     int x = owner_leaf[p];
@@ -72,17 +85,19 @@ __global__ void kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf, 
     const float4* t = S.btris + 3 * (long long)S.leaf_start_of[x];
     Kdop k;
     float m = 0.0f;
-    for (int i = 0; i < S.dirs; ++i) k.lo[i] = __int_as_float(0x7F800000), k.hi[i] = __int_as_float(0xFF800000);
+#pragma unroll
+    for (int i = 0; i < kDirs; ++i) k.lo[i] = __int_as_float(0x7F800000), k.hi[i] = __int_as_float(0xFF800000);
     for (int v = 0; v < 3 * cnt; ++v) {
-        const float4 q = t[v];
+        const float4 q = __ldg(t + v);
         m = fmaxf(m, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
-        for (int i = 0; i < S.dirs; ++i) {
+#pragma unroll
+        for (int i = 0; i < kDirs; ++i) {
             const float d = proj(i, q.x, q.y, q.z);
             k.lo[i] = fminf(k.lo[i], d);
             k.hi[i] = fmaxf(k.hi[i], d);
         }
     }
-    kdop[x] = k;
+    store_kdop(kdop + x, k);
     mag[x] = m;
     for (int guard = 0; guard < 4096; ++guard) {
         __threadfence();
@@ -92,63 +107,101 @@ __global__ void kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf, 
         __threadfence();
         const int4 c = S.child[par - S.N];
         // the sibling's k-DOP was written by another SM: read through L2 (no stale L1 lines)
-        const float* a = reinterpret_cast<const float*>(kdop + c.x);
-        const float* b = reinterpret_cast<const float*>(kdop + c.y);
-        for (int i = 0; i < S.dirs; ++i) {
-            k.lo[i] = fminf(__ldcg(a + i), __ldcg(b + i));
-            k.hi[i] = fmaxf(__ldcg(a + kDirs + i), __ldcg(b + kDirs + i));
+        const float4* a = reinterpret_cast<const float4*>(kdop + c.x);
+        const float4* b = reinterpret_cast<const float4*>(kdop + c.y);
+#pragma unroll
+        for (int i = 0; i < kDirs / 4; ++i) {
+            const float4 al = __ldcg(a + i), bl = __ldcg(b + i);
+            const float4 ah = __ldcg(a + kDirs / 4 + i), bh = __ldcg(b + kDirs / 4 + i);
+            k.lo[4 * i] = fminf(al.x, bl.x), k.lo[4 * i + 1] = fminf(al.y, bl.y);
+            k.lo[4 * i + 2] = fminf(al.z, bl.z), k.lo[4 * i + 3] = fminf(al.w, bl.w);
+            k.hi[4 * i] = fmaxf(ah.x, bh.x), k.hi[4 * i + 1] = fmaxf(ah.y, bh.y);
+            k.hi[4 * i + 2] = fmaxf(ah.z, bh.z), k.hi[4 * i + 3] = fmaxf(ah.w, bh.w);
         }
         m = fmaxf(__ldcg(mag + c.x), __ldcg(mag + c.y));
-        kdop[par] = k;
+        store_kdop(kdop + par, k);
         mag[par] = m;
         x = par;
     }
 }
 
-__device__ __forceinline__ void best_sobb(const Kdop& k, float m, int dirs, int triples, int axes[3], float lo[3],
-                                          float hi[3]) {
-    float best = __int_as_float(0x7F800000);
-    int bt = 0;
-    for (int t = 0; t < triples; ++t) {
-        const int a = c_triple[t][0], b = c_triple[t][1], c = c_triple[t][2];
-        if (a >= dirs || b >= dirs || c >= dirs) continue;
-        const float wa = k.hi[a] - k.lo[a], wb = k.hi[b] - k.lo[b], wc = k.hi[c] - k.lo[c];
-        const float sa = (wa * wb + wb * wc + wc * wa) * c_inv_det[t];
-        if (sa < best) {
-            best = sa;
-            bt = t;
+// One warp per inner node of the final layout, one half-warp per child. Lane l of a half holds the child's
+// interval on direction l; the half's lanes share the triples (lane l evaluates triples l, l + 16, ...,
+// reading the three widths by shuffles), and a 16-lane minimum over (area, triple index) keeps the first
+// triple of least area, i.e. the result of a sequential scan in table order with a strict "<".
+constexpr int kSobbNodeThreads = 256;
+
+__global__ void __launch_bounds__(kSobbNodeThreads) sobb_node_kernel(
+    SobbIn S, const BNode* __restrict__ bnodes, const uint32_t* __restrict__ rev_index, int num_inner,
+    const Kdop* __restrict__ kdop, const float* __restrict__ mag, int triples, SNode* __restrict__ snodes,
+    const uint32_t* err) {
+    __shared__ uint32_t s_tri[kMaxTriples];
+    __shared__ float s_inv[kMaxTriples];
+    for (int t = threadIdx.x; t < triples; t += kSobbNodeThreads) {
+        s_tri[t] = (uint32_t)c_triple[t][0] | ((uint32_t)c_triple[t][1] << 8) | ((uint32_t)c_triple[t][2] << 16);
+        s_inv[t] = c_inv_det[t];
+    }
+    __syncthreads();
+    if (*err != 0u) return;
+    const int lane = threadIdx.x & 31, l = lane & 15, half = lane >> 4;
+    const int warps = (int)(gridDim.x * (kSobbNodeThreads / 32));
+    // the node loop and the triple loop are warp-uniform, so every shuffle below has all 32 lanes
+    for (int k = (int)((blockIdx.x * kSobbNodeThreads + threadIdx.x) >> 5); k < num_inner; k += warps) {
+        if (__float_as_int(S.node_lo[k].w) < S.L) continue;  // not an inner node of the layout
+        const int4 c = S.child[k];
+        const int id = half ? c.y : c.x;
+        const float* kd = reinterpret_cast<const float*>(kdop + id);
+        const float lo = kd[l], hi = kd[kDirs + l];
+        const float w = hi - lo;
+        float best = __int_as_float(0x7F800000);
+        int bt = 0x7FFFFFFF;  // none yet
+        for (int t0 = 0; t0 < triples; t0 += 16) {
+            const int t = t0 + l;
+            const uint32_t abc = t < triples ? s_tri[t] : 0u;
+            const int a = abc & 0xFF, b = (abc >> 8) & 0xFF, cc = abc >> 16;
+            const float wa = __shfl_sync(0xffffffffu, w, a, 16), wb = __shfl_sync(0xffffffffu, w, b, 16),
+                        wc = __shfl_sync(0xffffffffu, w, cc, 16);
+            // triples are listed with a < b < c: c < dirs admits the triple
+            if (t < triples && cc < S.dirs) {
+                const float sa = (wa * wb + wb * wc + wc * wa) * s_inv[t];
+                if (sa < best) {
+                    best = sa;
+                    bt = t;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, best, o, 16);
+            const int ot = __shfl_xor_sync(0xffffffffu, bt, o, 16);
+            if (ob < best || (ob == best && ot < bt)) {
+                best = ob;
+                bt = ot;
+            }
+        }
+        if (bt == 0x7FFFFFFF) bt = 0;  // no triple of finite area: the table's first triple (the axes)
+        const uint32_t abc = s_tri[bt];
+        const int ax0 = abc & 0xFF, ax1 = (abc >> 8) & 0xFF, ax2 = abc >> 16;
+        const float pad = mag[id] * 9.5367431640625e-07f + 1e-30f;
+        const float lo0 = __shfl_sync(0xffffffffu, lo, ax0, 16) - pad, hi0 = __shfl_sync(0xffffffffu, hi, ax0, 16) + pad;
+        const float lo1 = __shfl_sync(0xffffffffu, lo, ax1, 16) - pad, hi1 = __shfl_sync(0xffffffffu, hi, ax1, 16) + pad;
+        const float lo2 = __shfl_sync(0xffffffffu, lo, ax2, 16) - pad, hi2 = __shfl_sync(0xffffffffu, hi, ax2, 16) + pad;
+        // child 1's values to lane 0
+        const float r0 = __shfl_down_sync(0xffffffffu, lo0, 16), r1 = __shfl_down_sync(0xffffffffu, hi0, 16);
+        const float r2 = __shfl_down_sync(0xffffffffu, lo1, 16), r3 = __shfl_down_sync(0xffffffffu, hi1, 16);
+        const float r4 = __shfl_down_sync(0xffffffffu, lo2, 16), r5 = __shfl_down_sync(0xffffffffu, hi2, 16);
+        const int rax = __shfl_down_sync(0xffffffffu, (int)abc, 16);
+        if (lane == 0) {
+            const int f = (int)rev_index[num_inner - 1 - k];
+            SNode nd;
+            nd.a = make_float4(lo0, hi0, lo1, hi1);
+            nd.b = make_float4(lo2, hi2, r0, r1);
+            nd.c = make_float4(r2, r3, r4, r5);
+            const int4 refs = bnodes[f].d;  // the same references as the binary layout
+            nd.d = make_int4(refs.x, refs.y, (int)abc, rax);
+            snodes[f] = nd;
         }
     }
-    const float pad = m * 9.5367431640625e-07f + 1e-30f;
-    for (int j = 0; j < 3; ++j) {
-        axes[j] = c_triple[bt][j];
-        lo[j] = k.lo[axes[j]] - pad;
-        hi[j] = k.hi[axes[j]] + pad;
-    }
-}
-
-__global__ void sobb_node_kernel(SobbIn S, const BNode* __restrict__ bnodes, const uint32_t* __restrict__ rev_index,
-                                 int num_inner, const Kdop* __restrict__ kdop, const float* __restrict__ mag,
-                                 int triples, SNode* __restrict__ snodes, const uint32_t* err) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= num_inner || *err != 0u) return;
-    if (__float_as_int(S.node_lo[k].w) < S.L) return;
-    const int f = (int)rev_index[num_inner - 1 - k];
-    const int4 c = S.child[k];
-    int ax[2][3];
-    float lo[2][3], hi[2][3];
-    for (int s = 0; s < 2; ++s) {
-        const int id = s == 0 ? c.x : c.y;
-        best_sobb(kdop[id], mag[id], S.dirs, triples, ax[s], lo[s], hi[s]);
-    }
-    SNode nd;
-    nd.a = make_float4(lo[0][0], hi[0][0], lo[0][1], hi[0][1]);
-    nd.b = make_float4(lo[0][2], hi[0][2], lo[1][0], hi[1][0]);
-    nd.c = make_float4(lo[1][1], hi[1][1], lo[1][2], hi[1][2]);
-    const int4 refs = bnodes[f].d;  // the same references as the binary layout
-    nd.d = make_int4(refs.x, refs.y, ax[0][0] | (ax[0][1] << 8) | (ax[0][2] << 16),
-                     ax[1][0] | (ax[1][1] << 8) | (ax[1][2] << 16));
-    snodes[f] = nd;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -399,8 +452,16 @@ dipl_status sobb_enqueue(const int4* child, const float4* node_lo, const float4*
     kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, kdop, sc.mag, sc.arrivals, d_err);
     note_launches();
     if (K > 0) {
-        sobb_node_kernel<<<(unsigned)((K + 255) / 256), 256, 0, s>>>(S, bnodes, rev_index, K, kdop, sc.mag,
-                                                                      sc.triples, snodes, d_err);
+        // persistent: each CTA stages the triple table once, then its warps stride over the nodes
+        int dev = 0, sms = 0;
+        DIPL_CUDA(cudaGetDevice(&dev));
+        DIPL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const long long warps_needed = K;
+        const long long grid = std::max<long long>(
+            1, std::min<long long>((long long)sms * (2048 / kSobbNodeThreads),
+                                   (warps_needed + kSobbNodeThreads / 32 - 1) / (kSobbNodeThreads / 32)));
+        sobb_node_kernel<<<(unsigned)grid, kSobbNodeThreads, 0, s>>>(S, bnodes, rev_index, K, kdop, sc.mag,
+                                                                     sc.triples, snodes, d_err);
         note_launches();
     }
     DIPL_CUDA(cudaGetLastError());

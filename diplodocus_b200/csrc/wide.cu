@@ -106,7 +106,7 @@ __global__ void wide_collapse_kernel(WideIn W, const int* __restrict__ frontier,
     n_tris[i] = nt;
 }
 
-__device__ __forceinline__ void quantise_axis(float p, float ext, const float* lo, const float* hi, int cnt,
+__device__ __forceinline__ void quantise_axis(float p, float ext, const float* lo, const float* hi, uint32_t valid,
                                               unsigned char* qlo, unsigned char* qhi, unsigned char& ebiased) {
     int e = -126;
     if (ext > 0.0f) {
@@ -118,7 +118,7 @@ __device__ __forceinline__ void quantise_axis(float p, float ext, const float* l
         const float scale = ldexpf(1.0f, e);
         bool ok = true;
         for (int k = 0; k < 8; ++k) {
-            if (k >= cnt) {
+            if (!((valid >> k) & 1u)) {
                 qlo[k] = 0, qhi[k] = 0;
                 continue;
             }
@@ -137,6 +137,11 @@ __device__ __forceinline__ void quantise_axis(float p, float ext, const float* l
     ebiased = (unsigned char)(e + 127);
 }
 
+// Writes one wide node per frontier entry. Children go to slots by octant (after Ylitie et al.): slot s
+// stands for the direction (s&1 ? +x : -x, s&2 ? +y : -y, s&4 ? +z : -z) from the node centre, and the
+// (child, slot) pairs are taken greedily by the largest projection of the child's centre offset on the
+// slot direction. A ray whose direction signs form octant o then visits slots in the order s ^ o, which
+// is roughly front to back. Inner children are ranked, and leaf triangles placed, in slot order.
 __global__ void wide_write_kernel(WideIn W, const int* __restrict__ frontier, int n_front,
                                   const int* __restrict__ kids, const uint32_t* __restrict__ inner_prefix,
                                   const uint32_t* __restrict__ tri_prefix, int base, int next_base, int tri_next,
@@ -146,45 +151,101 @@ __global__ void wide_write_kernel(WideIn W, const int* __restrict__ frontier, in
     if (i >= n_front || *err != 0u) return;
     const int child_base = next_base + (int)inner_prefix[i];
     const int tri_base = tri_next + (int)tri_prefix[i];
-    float lo[3][8], hi[3][8];
     int cnt = 0;
     int ids[8];
+#pragma unroll
     for (int k = 0; k < 8; ++k) {
         ids[k] = kids[8 * i + k];
         if (ids[k] >= 0) cnt = k + 1;
     }
+    float clo[3][8], chi[3][8];
     float3 p = make_float3(__int_as_float(0x7F800000), __int_as_float(0x7F800000), __int_as_float(0x7F800000));
     float3 q = make_float3(-p.x, -p.y, -p.z);
-    for (int k = 0; k < cnt; ++k) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (k >= cnt) continue;
         float3 l, h;
         wbox(W, ids[k], l, h);
-        lo[0][k] = wpad_down(l.x, h.x), hi[0][k] = wpad_up(l.x, h.x);
-        lo[1][k] = wpad_down(l.y, h.y), hi[1][k] = wpad_up(l.y, h.y);
-        lo[2][k] = wpad_down(l.z, h.z), hi[2][k] = wpad_up(l.z, h.z);
-        p = make_float3(fminf(p.x, lo[0][k]), fminf(p.y, lo[1][k]), fminf(p.z, lo[2][k]));
-        q = make_float3(fmaxf(q.x, hi[0][k]), fmaxf(q.y, hi[1][k]), fmaxf(q.z, hi[2][k]));
+        clo[0][k] = wpad_down(l.x, h.x), chi[0][k] = wpad_up(l.x, h.x);
+        clo[1][k] = wpad_down(l.y, h.y), chi[1][k] = wpad_up(l.y, h.y);
+        clo[2][k] = wpad_down(l.z, h.z), chi[2][k] = wpad_up(l.z, h.z);
+        p = make_float3(fminf(p.x, clo[0][k]), fminf(p.y, clo[1][k]), fminf(p.z, clo[2][k]));
+        q = make_float3(fmaxf(q.x, chi[0][k]), fmaxf(q.y, chi[1][k]), fmaxf(q.z, chi[2][k]));
+    }
+    // ---- greedy octant slot assignment -----------------------------------------------------------------
+    const float cx = 0.5f * (p.x + q.x), cy = 0.5f * (p.y + q.y), cz = 0.5f * (p.z + q.z);
+    float ox[8], oy[8], oz[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        ox[k] = k < cnt ? 0.5f * (clo[0][k] + chi[0][k]) - cx : 0.0f;
+        oy[k] = k < cnt ? 0.5f * (clo[1][k] + chi[1][k]) - cy : 0.0f;
+        oz[k] = k < cnt ? 0.5f * (clo[2][k] + chi[2][k]) - cz : 0.0f;
+    }
+    uint32_t free_k = (1u << cnt) - 1u, free_s = 0xFFu;
+    int slot_of[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int round = 0; round < cnt; ++round) {
+        float best = -__int_as_float(0x7F800000);
+        int bk = -1, bs = -1;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (!((free_k >> k) & 1u)) continue;
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                if (!((free_s >> s) & 1u)) continue;
+                const float v = ((s & 1) ? ox[k] : -ox[k]) + ((s & 2) ? oy[k] : -oy[k]) + ((s & 4) ? oz[k] : -oz[k]);
+                if (bk < 0 || v > best) {
+                    best = v;
+                    bk = k;
+                    bs = s;
+                }
+            }
+        }
+        free_k &= ~(1u << bk);
+        free_s &= ~(1u << bs);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k == bk) slot_of[k] = bs;
+    }
+    // children and padded boxes by slot
+    int sid[8];
+    float lo[3][8], hi[3][8];
+    uint32_t valid = 0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        sid[s] = -1;
+        lo[0][s] = lo[1][s] = lo[2][s] = 0.0f;
+        hi[0][s] = hi[1][s] = hi[2][s] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k < cnt && slot_of[k] == s) {
+                sid[s] = ids[k];
+                lo[0][s] = clo[0][k], lo[1][s] = clo[1][k], lo[2][s] = clo[2][k];
+                hi[0][s] = chi[0][k], hi[1][s] = chi[1][k], hi[2][s] = chi[2][k];
+            }
+        }
+        if (sid[s] >= 0) valid |= 1u << s;
     }
     WNode nd;
     nd.px = p.x, nd.py = p.y, nd.pz = p.z;
-    quantise_axis(p.x, q.x - p.x, lo[0], hi[0], cnt, nd.qlox, nd.qhix, nd.ex);
-    quantise_axis(p.y, q.y - p.y, lo[1], hi[1], cnt, nd.qloy, nd.qhiy, nd.ey);
-    quantise_axis(p.z, q.z - p.z, lo[2], hi[2], cnt, nd.qloz, nd.qhiz, nd.ez);
+    quantise_axis(p.x, q.x - p.x, lo[0], hi[0], valid, nd.qlox, nd.qhix, nd.ex);
+    quantise_axis(p.y, q.y - p.y, lo[1], hi[1], valid, nd.qloy, nd.qhiy, nd.ey);
+    quantise_axis(p.z, q.z - p.z, lo[2], hi[2], valid, nd.qloz, nd.qhiz, nd.ez);
     nd.child_base = child_base;
     nd.tri_base = tri_base;
     unsigned char imask = 0;
     int rank = 0, toff = 0;
-    for (int k = 0; k < 8; ++k) {
-        nd.meta[k] = 0;
-        if (k >= cnt) continue;
-        const int id = ids[k];
+    for (int s = 0; s < 8; ++s) {
+        nd.meta[s] = 0;
+        const int id = sid[s];
+        if (id < 0) continue;
         const int n = wcount(W, id);
         if (n >= W.L) {
-            imask |= (unsigned char)(1u << k);
+            imask |= (unsigned char)(1u << s);
             frontier_out[(int)inner_prefix[i] + rank] = id;
-            nd.meta[k] = (unsigned char)rank;
+            nd.meta[s] = (unsigned char)rank;
             ++rank;
         } else {
-            nd.meta[k] = (unsigned char)((n << 5) | toff);
+            nd.meta[s] = (unsigned char)((n << 5) | toff);
             const float4* src = W.btris + 3 * (long long)W.leaf_start_of[id];
             float4* dst = tris + 3 * (long long)(tri_base + toff);
             for (int t = 0; t < 3 * n; ++t) dst[t] = src[t];
@@ -201,7 +262,11 @@ __global__ void copy_tris_kernel(const float4* __restrict__ src, float4* __restr
 }
 
 // ------------------------------------------------------------------------------------------------
-// Traversal.
+// Traversal (after Ylitie et al.): the stack holds node groups, one 8-byte entry per wide node with
+// children still to visit: the node's child base, its inner-slot mask and the not-yet-visited hit
+// children as bits in visiting order (bit b = slot b ^ octant of the ray). Leaf triangles of a node are
+// tested as soon as the node is intersected. A node taken from a group is not re-tested against its own
+// box: its children's boxes are tested against the best t when it is visited.
 // ------------------------------------------------------------------------------------------------
 constexpr int kWTraceThreads = 128;
 constexpr float kWSlabWiden = 1e-6f;
@@ -236,52 +301,52 @@ __global__ void __launch_bounds__(kWTraceThreads) wide_trace_kernel(
         r.tmax = rb.w;
         auto safe = [](float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; };
         r.inv = make_float3(__frcp_rn(safe(r.d.x)), __frcp_rn(safe(r.d.y)), __frcp_rn(safe(r.d.z)));
+        // slot s lies towards (s&1 ? +x : -x, ...): a ray going -x meets the +x children first
+        const uint32_t oct = (r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u);
         const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
         WtRay w{};
         if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(r.d);
         float best_t = r.tmax, best_u = 0.0f, best_v = 0.0f;
         int best_prim = -1;
-        bool found = false, bad = false;
-        int sref[STACK];
-        float st[STACK];
-        int sp = 0;
-        int cur = num_nodes >= 0 ? root : 0x7FFFFFFF;
-        uint32_t steps = 0;
-        const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
-        auto test_range = [&](int first, int count) {
-            for (int k = 0; k < count; ++k) {
-                const float4* tp = tris + 3 * (int64_t)(first + k);
-                const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
-                const int prim = __float_as_int(p0.w);
-                float b1 = 0.0f, b2 = 0.0f;
-                const float t = wleaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
-                                                 make_float3(p2.x, p2.y, p2.z), r, w, backface, b1, b2);
-                if (COUNT) ++tests;
-                if (ANY) {
-                    if (t > r.tmin && t < r.tmax && t < kInfinity) {
-                        found = true;
-                        return;
-                    }
-                } else if (t > r.tmin && t < kInfinity &&
-                           (t < best_t || (t == best_t && found && prim < best_prim))) {
-                    best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
-                }
+        bool found = false, bad = false, done = false;
+        auto test_tri = [&](int idx) {
+            const float4* tp = tris + 3 * (int64_t)idx;
+            const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+            const int prim = __float_as_int(p0.w);
+            float b1 = 0.0f, b2 = 0.0f;
+            const float t = wleaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
+                                             make_float3(p2.x, p2.y, p2.z), r, w, backface, b1, b2);
+            if (COUNT) ++tests;
+            if (ANY) {
+                if (t > r.tmin && t < r.tmax && t < kInfinity) found = true;
+            } else if (t > r.tmin && t < kInfinity && (t < best_t || (t == best_t && found && prim < best_prim))) {
+                best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
             }
         };
-        while (cur != 0x7FFFFFFF) {
+        int2 stack[STACK];
+        int sp = 0;
+        int node = -1;
+        if (num_nodes < 0) {
+            done = true;  // empty BVH
+        } else if (root < 0) {
+            for (int k = 0, c = leaf_count(root); k < c && !(ANY && found); ++k) test_tri(leaf_first(root) + k);
+            done = true;
+        } else {
+            node = root;
+        }
+        uint32_t steps = 0;
+        const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+        while (!done) {
             if (++steps > step_limit) {
                 bad = true;
                 break;
             }
-            if (cur < 0) {
-                test_range(leaf_first(cur), leaf_count(cur));
-                if (ANY && found) break;
-            } else {
-                if (cur >= num_nodes) {
+            if (node >= 0) {
+                if (node >= num_nodes) {
                     bad = true;
                     break;
                 }
-                const float4* np = reinterpret_cast<const float4*>(nodes + cur);
+                const float4* np = reinterpret_cast<const float4*>(nodes + node);
                 const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2), f3 = __ldg(np + 3),
                              f4 = __ldg(np + 4);
                 if (COUNT) ++visits;
@@ -296,10 +361,7 @@ __global__ void __launch_bounds__(kWTraceThreads) wide_trace_kernel(
                                          __float_as_uint(f3.z), __float_as_uint(f3.w), __float_as_uint(f4.x),
                                          __float_as_uint(f4.y), __float_as_uint(f4.z), __float_as_uint(f4.w)};
                 const float lim = best_t + fabsf(best_t) * kWPruneSlack;
-                // children hit, nearest last on the stack
-                int hit_ref[8];
-                float hit_t[8];
-                int nh = 0;
+                uint32_t inner_hits = 0, tri_mask = 0;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const uint32_t meta = ((k < 4 ? meta_lo : meta_hi) >> (8 * (k & 3))) & 0xFFu;
@@ -318,36 +380,41 @@ __global__ void __launch_bounds__(kWTraceThreads) wide_trace_kernel(
                     tn = tn - fabsf(tn) * kWSlabWiden;
                     tf = tf + fabsf(tf) * kWSlabWiden;
                     if (!(tn <= tf && tf >= r.tmin && tn <= lim)) continue;
-                    const int ref = inner ? child_base + (int)meta
-                                          : make_leaf_ref(tri_base + (int)(meta & 31u), (int)(meta >> 5));
-                    // insertion by descending t: the nearest ends last
-                    int pos = nh++;
-                    while (pos > 0 && hit_t[pos - 1] < tn) {
-                        hit_t[pos] = hit_t[pos - 1];
-                        hit_ref[pos] = hit_ref[pos - 1];
-                        --pos;
+                    if (inner) inner_hits |= 1u << (k ^ oct);
+                    else tri_mask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+                }
+                while (tri_mask) {
+                    const int b = __ffs(tri_mask) - 1;
+                    tri_mask &= tri_mask - 1u;
+                    test_tri(tri_base + b);
+                    if (ANY && found) break;
+                }
+                if (ANY && found) break;
+                node = -1;
+                if (inner_hits) {
+                    const int b = __ffs(inner_hits) - 1;
+                    inner_hits &= inner_hits - 1u;
+                    const uint32_t slot = (uint32_t)b ^ oct;
+                    node = child_base + __popc(imask & ((1u << slot) - 1u));
+                    if (inner_hits) {
+                        if (sp >= STACK) {
+                            bad = true;
+                            break;
+                        }
+                        stack[sp++] = make_int2(child_base, (int)((inner_hits << 8) | imask));
                     }
-                    hit_t[pos] = tn;
-                    hit_ref[pos] = ref;
                 }
-                if (sp + nh > STACK) {
-                    bad = true;
-                    break;
-                }
-                for (int k = 0; k < nh; ++k) {
-                    sref[sp] = hit_ref[k];
-                    st[sp] = hit_t[k];
-                    ++sp;
-                }
-            }
-            cur = 0x7FFFFFFF;
-            const float lim = best_t + fabsf(best_t) * kWPruneSlack;
-            while (sp > 0) {
-                --sp;
-                if (st[sp] <= lim) {
-                    cur = sref[sp];
-                    break;
-                }
+            } else {
+                if (sp == 0) break;
+                const int2 e = stack[sp - 1];
+                uint32_t gh = (uint32_t)e.y >> 8;
+                const uint32_t gi = (uint32_t)e.y & 0xFFu;
+                const int b = __ffs(gh) - 1;
+                gh &= gh - 1u;
+                const uint32_t slot = (uint32_t)b ^ oct;
+                node = e.x + __popc(gi & ((1u << slot) - 1u));
+                if (gh) stack[sp - 1].y = (int)((gh << 8) | gi);
+                else --sp;
             }
         }
         if (bad) atomicOr(err, kErrStack);
@@ -384,12 +451,13 @@ dipl_status launch_wide(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl
     return DIPL_OK;
 }
 
+// At most one group per wide level is on the stack (depth = wide levels of the layout).
 template <int LEAF, bool ANY, bool COUNT>
 dipl_status launch_wide_stack(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
                               uint32_t flags, unsigned long long* counters, cudaStream_t s) {
-    const int need = 7 * b->depth + 8;
-    if (need <= 64) return launch_wide<LEAF, ANY, COUNT, 64>(b, rays, n, hits, occ, flags, counters, s);
-    if (need <= 192) return launch_wide<LEAF, ANY, COUNT, 192>(b, rays, n, hits, occ, flags, counters, s);
+    const int need = b->depth + 1;
+    if (need <= 32) return launch_wide<LEAF, ANY, COUNT, 32>(b, rays, n, hits, occ, flags, counters, s);
+    if (need <= 96) return launch_wide<LEAF, ANY, COUNT, 96>(b, rays, n, hits, occ, flags, counters, s);
     return launch_wide<LEAF, ANY, COUNT, 512>(b, rays, n, hits, occ, flags, counters, s);
 }
 

@@ -173,6 +173,17 @@ def test_wide_quantised_bounds_are_conservative(name):
                 out += list(range(first, first + (r["meta"][k] >> 5)))
         return out
 
+    # the traversal finds an inner child from its slot alone: rank = inner slots below it; leaf triangles
+    # of a node are packed in slot order
+    for r in rec:
+        toff = 0
+        for k in range(8):
+            if (r["imask"] >> k) & 1:
+                assert r["meta"][k] == bin(int(r["imask"]) & ((1 << k) - 1)).count("1")
+            elif r["meta"][k]:
+                assert r["meta"][k] & 31 == toff
+                toff += r["meta"][k] >> 5
+
     checked = 0
     for node in range(len(rec)):
         r = rec[node]
