@@ -452,7 +452,7 @@ def run_soup16m(args):
     from diplodocus_b200 import scenes as S
     n = args.soup_tris
     tris = S.soup(n, seed=3)
-    nr = args.rays or (1 << 22)
+    nr = args.rays or (1 << 24)
     rays = torch.from_numpy(S.random_rays(nr, seed=3)).cuda()
     tt = torch.from_numpy(tris).cuda()  # resident in HBM: the timed builds exclude host->device copies
     v = A.soa_vertices(tt)
@@ -465,6 +465,7 @@ def run_soup16m(args):
         lib.dipl_bvh_build(C.byref(desc), C.byref(h), sp)
         lib.dipl_bvh_destroy(h)
 
+    peak, _ = peaks()
     out = {}
     ref_prim = None
     for name, kind, layout in [("ploc_binary", A.AccelerationStructureType.kPloc, "binary"),
@@ -476,7 +477,9 @@ def run_soup16m(args):
         desc = A.make_desc(*v, cfg)
         ms_build = _time(lambda: build_only(desc), 3, warm=1)
         ms_trace = _time(lambda: bvh.Intersect(A.Stats(), rays), 2, warm=1)
-        h = bvh.Intersect(A.Stats(), rays)
+        st = A.Stats()
+        h = bvh.Intersect(st, rays, count=True)  # same kernel with visit counters, same rays
+        visits, tests = st.accel_stats.traversal_count / nr, st.accel_stats.intersection_count / nr
         prim = h.prim.cpu().numpy()
         if ref_prim is None:
             ref_prim = prim
@@ -486,8 +489,15 @@ def run_soup16m(args):
         u32 = h.u.cpu().numpy()[hit].astype(np.float64)
         rel_t = np.abs(t32 - tuv[hit, 0]) / np.maximum(np.abs(tuv[hit, 0]), 1e-30)
         info = bvh.info()
+        node_size = info.node_bytes / max(info.num_inner_nodes, 1)
+        ray_bytes = 32 + 16 + visits * node_size + tests * 36
+        achieved = ray_bytes * nr / (ms_trace / 1e3) / 1e9
         out[name] = {"build_ms": round(ms_build, 3), "build_mtri_s": round(n / ms_build / 1e3, 1),
                      "trace_mrays_s": round(nr / ms_trace / 1e3, 2), "sah_cost": round(bvh.sah_cost(), 3),
+                     "node_visits_per_ray": round(visits, 2), "tri_tests_per_ray": round(tests, 2),
+                     "roofline_trace": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                                        "unit": "GB/s", "frac": round(achieved / peak, 4),
+                                        "bytes_per_ray": round(ray_bytes, 1), "node_bytes": round(node_size, 1)},
                      "node_bytes": int(info.node_bytes), "same_hits_as_binary": float((prim == ref_prim).mean()),
                      "t_rel_err_vs_fp64": {"median": float(np.median(rel_t)), "p99": float(np.quantile(rel_t, 0.99)),
                                            "max": float(rel_t.max())},

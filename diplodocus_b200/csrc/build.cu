@@ -33,6 +33,9 @@ struct CodeParams {
     unsigned long long top[4];
     unsigned long long mask[4];
     int bits[4];
+    // EMC60: dep[a][c][v] = the bits of nibble v of dimension a's cell index, chunk c (bits 4c..4c+3),
+    // deposited at their code positions, so a code is an OR of table entries instead of a bit loop.
+    unsigned long long dep[4][16][16];
 };
 
 struct PlocCtrl {
@@ -216,7 +219,7 @@ __global__ void code_params_kernel(const Bounds* __restrict__ bounds, int m, int
         bmin[a] = ordered_to_float(bounds[k].v[6 + a]);
         bmax[a] = ordered_to_float(bounds[k].v[9 + a]);
     }
-    CodeParams p;
+    CodeParams p;  // scalar fields only; the deposit tables are written to out[k] directly
     if (code_type == DIPL_CODE_MORTON30) {
         for (int a = 0; a < 3; ++a) {
             float ext = __fsub_rn(cmax[a], cmin[a]);
@@ -251,8 +254,18 @@ __global__ void code_params_kernel(const Bounds* __restrict__ bounds, int m, int
             p.s[a] = (ext[a] > 0.0f && p.bits[a] > 0) ? __fdiv_rn(cells, ext[a]) : 0.0f;
             p.top[a] = p.bits[a] >= 64 ? ~0ull : ((1ull << p.bits[a]) - 1ull);
         }
+        for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 16; ++c)
+                for (int v = 0; v < 16; ++v)
+                    out[k].dep[a][c][v] = deposit_bits((unsigned long long)v << (4 * c), p.mask[a]);
     }
-    out[k] = p;
+    for (int a = 0; a < 4; ++a) {
+        out[k].lo[a] = p.lo[a];
+        out[k].s[a] = p.s[a];
+        out[k].top[a] = p.top[a];
+        out[k].mask[a] = p.mask[a];
+        out[k].bits[a] = p.bits[a];
+    }
 }
 
 __device__ __forceinline__ unsigned long long tri_code(const Tri& t, const CodeParams& p, int code_type) {
@@ -280,7 +293,8 @@ __device__ __forceinline__ unsigned long long tri_code(const Tri& t, const CodeP
         float q = fmaxf(__fmul_rn(__fsub_rn(xs[a], p.lo[a]), p.s[a]), 0.0f);
         unsigned long long qi = q < 1.8e19f ? (unsigned long long)q : p.top[a];
         if (qi > p.top[a]) qi = p.top[a];
-        code |= deposit_bits(qi, p.mask[a]);
+        const int chunks = (p.bits[a] + 3) >> 2;
+        for (int c = 0; c < chunks; ++c) code |= p.dep[a][c][(qi >> (4 * c)) & 15ull];
     }
     return code;
 }
@@ -289,7 +303,8 @@ template <typename K>
 __global__ void __launch_bounds__(256) codes_kernel(const MeshDesc* __restrict__ meshes,
                                                     const long long* __restrict__ offsets, int m, long long n,
                                                     const CodeParams* __restrict__ params, int code_type,
-                                                    int code_shift, int mesh_shift, K* __restrict__ keys) {
+                                                    int code_shift, int mesh_shift, K* __restrict__ keys,
+                                                    float4* __restrict__ tbox) {
     long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (g >= n) return;
     int k = find_mesh(offsets, m, g);
@@ -298,6 +313,12 @@ __global__ void __launch_bounds__(256) codes_kernel(const MeshDesc* __restrict__
     unsigned long long code = tri_code(t, params[k], code_type) >> code_shift;
     if (mesh_shift > 0) code |= (unsigned long long)k << mesh_shift;
     keys[g] = static_cast<K>(code);
+    if (tbox) {  // one 32-byte record per triangle: later gathers by sorted position read one sector
+        float3 lo, hi;
+        tri_box(t, lo, hi);
+        tbox[2 * g] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+        tbox[2 * g + 1] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -333,6 +354,8 @@ struct PlocParams {
 // Clusters at most this many are finished by the single-CTA tail kernel, resident in shared memory.
 constexpr int kTailMax = 2048;
 constexpr int kTailThreads = 1024;
+// At most this many clusters: CTA 0 finishes alone (no cluster exchange per iteration).
+constexpr int kTailSolo = 512;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -504,6 +527,8 @@ struct PlocSmem {
     int nn[T + 2 * kRadiusMax];
     unsigned long long key[T + 2 * kRadiusMax];
     uint32_t warp_sum[B / 32];
+    unsigned long long lb_sum[B / 32];  // block look-back scratch
+    int lb_flag[B / 32];
     unsigned long long prefix;
     int ok;
     int n, mbase;
@@ -560,17 +585,17 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     }
     const uint32_t excl = woff + x - mine;
 
-    // ---- decoupled look-back over tiles: (kept, merged) prefixes (warp 0) ---------------------------
-    if (threadIdx.x < 32) {
+    // ---- decoupled look-back over tiles: (kept, merged) prefixes (whole block) ----------------------
+    {
         const unsigned long long agg = ((unsigned long long)(total & 0xFFFFu) << 31) | (total >> 16);
         unsigned long long* st = P.status[parity];
         unsigned long long prefix = 0;
         bool ok = true;
-        if (tile == 0) {
+        if (tile == 0) {  // block-uniform
             if (threadIdx.x == 0) st_release_u64(&st[0], (2ull << 62) | agg);
         } else {
             if (threadIdx.x == 0) st_release_u64(&st[tile], (1ull << 62) | agg);
-            prefix = warp_lookback(st, tile, P.err, &ok);
+            prefix = block_lookback<B>(st, tile, P.err, &ok, s.lb_sum, s.lb_flag);
             if (threadIdx.x == 0 && ok) st_release_u64(&st[tile], (2ull << 62) | (prefix + agg));
         }
         if (threadIdx.x == 0) {
@@ -675,10 +700,12 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
 
 // The last iterations (at most kTailMax clusters) in one thread-block cluster of kTailCtas CTAs of 1024 threads.
 // Every CTA keeps all clusters in its shared memory (double-buffered); per iteration each CTA finds the nearest
-// neighbours of its slice of positions and stores them into every CTA's neighbour array through distributed
-// shared memory; after one cluster barrier every CTA runs the same merge and compaction over all positions, so
-// all copies stay identical without exchanging them (only CTA 0 writes the new nodes). Same rules as
-// ploc_kernel, so the result still equals the oracle's loop.
+// neighbours of its slice of positions, and after one cluster barrier reads the other slices from their
+// owners' shared memory (distributed shared memory loads, all in flight at once); then every CTA runs the
+// same merge and compaction over all positions, so all copies stay identical without exchanging them (only
+// CTA 0 writes the new nodes). Once at most kTailSolo clusters remain, the other CTAs leave and CTA 0 finishes
+// alone without a cluster barrier per iteration. Same rules as ploc_kernel, so the result still equals the
+// oracle's loop.
 constexpr int kTailCtasMax = 8;
 
 struct TailSmem {
@@ -722,26 +749,48 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     int cur = 0;
     uint32_t tail_iters = 0;
     bool failed = false;
+    bool solo = ctas == 1;  // CTA 0 alone: the peers have left the cluster
     while (n > P.num_meshes) {
         if (iter + tail_iters >= kMaxPlocIterations) {
             if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
             failed = true;
             break;
         }
+        if (!solo && n <= kTailSolo) {
+            // few clusters: one CTA searches them all faster than the cluster exchanges slices
+            cluster.sync();  // no peer reads this CTA's shared memory after this point
+            if (rank != 0) return;
+            solo = true;
+        }
         const int par = (int)(tail_iters & 1);
         const float4* __restrict__ lo = s.lo[cur];
         const float4* __restrict__ hi = s.hi[cur];
         const int4* __restrict__ info = s.info[cur];
-        // ---- neighbours of this CTA's slice, then broadcast to the peers ------------------------------
-        const int slice = (n + ctas - 1) / ctas;
-        const int q0 = min(n, rank * slice), q1 = min(n, q0 + slice);
-        nn_search_split<kTailThreads>(lo, hi, n, q0, q1, r, s.nn[par]);
-        __syncthreads();
-        for (int peer = 1; peer < ctas; ++peer) {
-            int* remote = cluster.map_shared_rank(s.nn[par], (rank + peer) % ctas);
-            for (int q = q0 + (int)threadIdx.x; q < q1; q += kTailThreads) remote[q] = s.nn[par][q];
+        // ---- neighbours of this CTA's slice; then every slice from its owner ---------------------------
+        if (solo) {
+            nn_search_split<kTailThreads>(lo, hi, n, 0, n, r, s.nn[par]);
+            __syncthreads();
+        } else {
+            const int slice = (n + ctas - 1) / ctas;
+            const int q0 = min(n, rank * slice), q1 = min(n, q0 + slice);
+            nn_search_split<kTailThreads>(lo, hi, n, q0, q1, r, s.nn[par]);
+            cluster.sync();  // release our slice, acquire the peers'
+            // pull the other slices (all loads in flight at once; the owners do not write s.nn[par] again
+            // before the next iteration's cluster barrier)
+            int v[IPT];
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) {
+                const int q = (int)threadIdx.x + k * kTailThreads;
+                const int owner = q < n ? q / slice : rank;
+                v[k] = owner != rank ? cluster.map_shared_rank(s.nn[par], owner)[q] : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) {
+                const int q = (int)threadIdx.x + k * kTailThreads;
+                if (q < n && q / slice != rank) s.nn[par][q] = v[k];
+            }
+            __syncthreads();
         }
-        cluster.sync();  // release our stores, acquire the peers'
         const int* __restrict__ nn = s.nn[par];
         // ---- merge decisions and compaction over all positions (identical in every CTA) --------------
         const int ib = threadIdx.x * IPT;
@@ -819,7 +868,7 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
         cur = nxt;
         ++tail_iters;
     }
-    cluster.sync();  // no CTA leaves while a peer may still store into its shared memory
+    if (!solo) cluster.sync();  // no CTA leaves while a peer may still read its shared memory
     if (failed || rank != 0) return;
     // final clusters (one per mesh) to the buffer of the final parity, for the root pass
     const uint32_t final_iter = iter + tail_iters;
@@ -832,15 +881,15 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
 }
 
 __global__ void ploc_init_kernel(const MeshDesc* __restrict__ meshes, const long long* __restrict__ offsets, int m,
-                                 long long n, const uint32_t* __restrict__ perm, float4* __restrict__ lo,
-                                 float4* __restrict__ hi, int4* __restrict__ info, int* __restrict__ parent) {
+                                 long long n, const uint32_t* __restrict__ perm, const float4* __restrict__ tbox,
+                                 float4* __restrict__ lo, float4* __restrict__ hi, int4* __restrict__ info,
+                                 int* __restrict__ parent) {
     long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (p >= n) return;
     long long g = perm[p];
     int k = find_mesh(offsets, m, g);
-    Tri t = load_tri(meshes[k], g - meshes[k].first);
-    float3 a, b;
-    tri_box(t, a, b);
+    (void)meshes;
+    const float4 a = __ldg(tbox + 2 * g), b = __ldg(tbox + 2 * g + 1);
     lo[p] = make_float4(a.x, a.y, a.z, __int_as_float((int)p));
     hi[p] = make_float4(b.x, b.y, b.z, __int_as_float(k));
     info[p] = make_int4(1, (int)p, 0, 0);
@@ -956,13 +1005,13 @@ __device__ __forceinline__ double box_area(float3 lo, float3 hi) {
     return 2.0 * (dx * dy + dy * dz + dz * dx);
 }
 
-__device__ __forceinline__ void child_box(const LayoutParams& P, const MeshDesc* meshes, const long long* offsets,
-                                          int m, const uint32_t* perm, int id, float3& lo, float3& hi) {
+__device__ __forceinline__ void child_box(const LayoutParams& P, const float4* tbox, const uint32_t* perm, int id,
+                                          float3& lo, float3& hi) {
     if (id < P.num_leaves) {
         long long g = perm[id];
-        int k = find_mesh(offsets, m, g);
-        Tri t = load_tri(meshes[k], g - meshes[k].first);
-        tri_box(t, lo, hi);
+        const float4 a = __ldg(tbox + 2 * g), b = __ldg(tbox + 2 * g + 1);
+        lo = make_float3(a.x, a.y, a.z);
+        hi = make_float3(b.x, b.y, b.z);
     } else {
         float4 a = P.node_lo[id - P.num_leaves], b = P.node_hi[id - P.num_leaves];
         lo = make_float3(a.x, a.y, a.z);
@@ -970,7 +1019,7 @@ __device__ __forceinline__ void child_box(const LayoutParams& P, const MeshDesc*
     }
 }
 
-__device__ __forceinline__ void node_write_one(const LayoutParams& P, const MeshDesc* __restrict__ meshes,
+__device__ __forceinline__ void node_write_one(const LayoutParams& P, const float4* __restrict__ tbox,
                                                const long long* __restrict__ offsets, int m,
                                                const uint32_t* __restrict__ perm,
                                                const uint32_t* __restrict__ rev_index,
@@ -988,7 +1037,7 @@ __device__ __forceinline__ void node_write_one(const LayoutParams& P, const Mesh
                           make_float3(P.node_hi[k].x, P.node_hi[k].y, P.node_hi[k].z));
     for (int s = 0; s < 2; ++s) {
         int id = s == 0 ? c.x : c.y;
-        child_box(P, meshes, offsets, m, perm, id, lo[s], hi[s]);
+        child_box(P, tbox, perm, id, lo[s], hi[s]);
         int cnt = node_count(P, id);
         if (cnt >= P.L) {
             ref[s] = (int)rev_index[P.num_inner - 1 - (id - P.num_leaves)];
@@ -1017,12 +1066,12 @@ __device__ __forceinline__ void node_write_one(const LayoutParams& P, const Mesh
 }
 
 // Single-mesh builds: one FP64 atomic pair per block instead of one per node.
-__global__ void node_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
+__global__ void node_write_kernel(LayoutParams P, const float4* __restrict__ tbox,
                                   const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
                                   const uint32_t* __restrict__ rev_index, const int* __restrict__ leaf_start_of,
                                   BNode* __restrict__ nodes, double* __restrict__ sah, const uint32_t* err) {
     double local_sum = 0.0, local_count = 0.0;
-    node_write_one(P, meshes, offsets, m, perm, rev_index, leaf_start_of, nodes, sah, err, local_sum, local_count);
+    node_write_one(P, tbox, offsets, m, perm, rev_index, leaf_start_of, nodes, sah, err, local_sum, local_count);
     if (m != 1) return;
     __shared__ double s_sum[32], s_cnt[32];
     for (int o = 16; o > 0; o >>= 1) {
@@ -1201,6 +1250,7 @@ struct BuildPlan {
     CodeParams* d_params = nullptr;
     void *keys = nullptr, *keys_sorted = nullptr, *keys_alt = nullptr;
     uint32_t *perm = nullptr, *perm_alt = nullptr;
+    float4* tbox = nullptr;  // per triangle (input order): box lo, box hi (32 bytes)
     unsigned char* sort_scratch = nullptr;
     PlocCtrl* d_ctrl = nullptr;
     int4* child = nullptr;
@@ -1298,6 +1348,7 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
         (st = W.alloc((unsigned char**)&P.keys_sorted, N * P.key_bytes)) != DIPL_OK ||
         (st = W.alloc((unsigned char**)&P.keys_alt, N * P.key_bytes)) != DIPL_OK ||
         (st = O.alloc(&P.perm, N)) != DIPL_OK || (st = W.alloc(&P.perm_alt, N)) != DIPL_OK ||
+        (st = W.alloc(&P.tbox, 2 * N)) != DIPL_OK ||
         (st = W.alloc(&P.sort_scratch, radix_sort_scratch_bytes(N, 0, P.key_bits, P.digit_bits))) != DIPL_OK)
         return st;
     P.B = ploc_block_for(d0.ploc_block_size);
@@ -1365,11 +1416,11 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     if (P.key_bytes == 4)
         codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.d_params,
                                                                        d0.code_type, P.code_shift, P.mesh_shift,
-                                                                       (uint32_t*)P.keys);
+                                                                       (uint32_t*)P.keys, P.tbox);
     else
         codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
             P.d_meshes, P.d_offsets, m, N, P.d_params, d0.code_type, P.code_shift, P.mesh_shift,
-            (unsigned long long*)P.keys);
+            (unsigned long long*)P.keys, P.tbox);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
     st = radix_sort_pairs(P.keys, nullptr, P.keys_sorted, P.perm, P.keys_alt, P.perm_alt, N, P.key_bytes, 0,
@@ -1384,8 +1435,8 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     DIPL_CUDA(cudaMemsetAsync(P.status, 0, sizeof(unsigned long long) * (2 * P.tiles_max + 2), stream));
     fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(P.parent, N + K, -1);
     note_launches();
-    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.perm, P.c_lo[0],
-                                                             P.c_hi[0], P.c_in[0], P.parent);
+    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.perm, P.tbox,
+                                                             P.c_lo[0], P.c_hi[0], P.c_in[0], P.parent);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
     pp.lo[0] = P.c_lo[0], pp.hi[0] = P.c_hi[0], pp.lo[1] = P.c_lo[1], pp.hi[1] = P.c_hi[1];
@@ -1423,7 +1474,7 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
                                                                P.owner_leaf, P.leaf_start_of, P.tris, P.d_err);
     note_launches();
     if (K > 0) {
-        node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.rev_flags,
+        node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.tbox, P.d_offsets, m, P.perm, P.rev_flags,
                                                                    P.leaf_start_of, P.nodes, P.d_sah, P.d_err);
         note_launches();
     }
@@ -1648,10 +1699,12 @@ dipl_status compute_codes(const dipl_build_desc* desc, void* d_codes, cudaStream
     code_params_kernel<<<1, 32, 0, stream>>>(d_bounds, 1, desc->code_type, d_params); note_launches();
     if (desc->code_type == DIPL_CODE_MORTON30)
         codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, 1, N, d_params,
-                                                                       desc->code_type, 0, 0, (uint32_t*)d_codes);
+                                                                       desc->code_type, 0, 0, (uint32_t*)d_codes,
+                                                                       nullptr);
     else
         codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
-            d_meshes, d_offsets, 1, N, d_params, desc->code_type, 0, 0, (unsigned long long*)d_codes); note_launches();
+            d_meshes, d_offsets, 1, N, d_params, desc->code_type, 0, 0, (unsigned long long*)d_codes, nullptr);
+    note_launches();
     DIPL_CUDA(cudaGetLastError());
     // keep the scratch alive until the kernels ran (frees are stream-ordered)
     return DIPL_OK;

@@ -177,6 +177,70 @@ __device__ __forceinline__ unsigned long long warp_lookback(const unsigned long 
     return prefix;
 }
 
+// Block-wide decoupled look-back (call with every thread of the block; same status layout as warp_lookback).
+// Thread t polls predecessor `tile - 1 - t`, so one round trip covers B predecessors: when all tiles of a
+// round run at once, the inclusive-prefix frontier then advances B tiles per round trip instead of 32.
+// `wsum` / `wflag` are shared scratch of B/32 entries. Returns the same value in every thread.
+template <int B>
+__device__ __forceinline__ unsigned long long block_lookback(const unsigned long long* status, long long tile,
+                                                             uint32_t* err, bool* ok, unsigned long long* wsum,
+                                                             int* wflag) {
+    constexpr unsigned long long kVal = (1ull << 62) - 1ull;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long prefix = 0;
+    long long j = tile - 1;
+    uint32_t spins = 0;
+    *ok = true;
+    for (;;) {
+        const long long idx = j - (long long)threadIdx.x;
+        // positions before tile 0 read as an inclusive prefix of zero
+        const unsigned long long w = idx >= 0 ? ld_acquire_u64(status + idx) : (2ull << 62);
+        const unsigned long long state = w >> 62;
+        const uint32_t inc = __ballot_sync(0xffffffffu, state == 2ull);
+        const uint32_t zero = __ballot_sync(0xffffffffu, state == 0ull);
+        const int lim = inc ? __ffs(inc) - 1 : 31;
+        const uint32_t upto = lim == 31 ? 0xffffffffu : ((2u << lim) - 1u);
+        unsigned long long v = lane <= lim ? (w & kVal) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) {
+            wsum[warp] = v;
+            wflag[warp] = (zero & upto) ? 2 : (inc ? 1 : 0);  // 2: not ready, 1: reached an inclusive prefix
+        }
+        __syncthreads();
+        // every thread combines the warps nearest first (same result everywhere, no second pass)
+        unsigned long long s = 0;
+        int code = 0;
+#pragma unroll
+        for (int wi = 0; wi < B / 32; ++wi) {
+            const int f = wflag[wi];
+            if (f == 2) {
+                code = 2;
+                break;
+            }
+            s += wsum[wi];
+            if (f == 1) {
+                code = 1;
+                break;
+            }
+        }
+        __syncthreads();  // scratch is rewritten by the next round
+        if (code == 2) {
+            if (++spins > kSpinLimit) {
+                if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+                *ok = false;
+                return 0ull;
+            }
+            __nanosleep(20);
+            continue;
+        }
+        prefix += s;
+        if (code == 1) break;
+        j -= B;
+    }
+    return prefix;
+}
+
 // Surface-area-like distance of PLOC: half the area of the union box, evaluated with fixed FMAs so
 // the host restatement (oracle/dipl_oracle.c ploc_key) rounds identically. NaN counts as +inf.
 __device__ __forceinline__ float ploc_distance(float lx0, float ly0, float lz0, float hx0, float hy0, float hz0,

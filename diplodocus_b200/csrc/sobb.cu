@@ -32,10 +32,8 @@ __constant__ float c_dir[kDirs][3] = {
     {0.f, 0.52573111f, 0.85065081f}, {0.52573111f, 0.85065081f, 0.f}, {0.85065081f, 0.f, 0.52573111f},
 };
 
-// Triples of directions with |det| > 0.2 and 1/|det|, filled by the host once.
-constexpr int kMaxTriples = 560;
-__constant__ unsigned char c_triple[kMaxTriples][3];
-__constant__ float c_inv_det[kMaxTriples];
+// 1/|det(n_a, n_b, n_c)| at a*256 + b*16 + c for a < b < c with |det| > 0.2, else 0; filled by the host once.
+__constant__ float c_inv3[kDirs * kDirs * kDirs];
 
 struct Kdop {
     float lo[kDirs], hi[kDirs];
@@ -59,6 +57,12 @@ struct SobbIn {
 
 __device__ __forceinline__ int scount(const SobbIn& S, int id) {
     return id < S.N ? 1 : __float_as_int(S.node_lo[id - S.N].w);
+}
+
+__device__ __forceinline__ unsigned atomic_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
 }
 
 // Stores / loads a k-DOP as 8 float4 (the whole struct stays in registers: every index is a constant).
@@ -100,88 +104,121 @@ __global__ void __launch_bounds__(256) kdop_refit_kernel(SobbIn S, const int* __
     store_kdop(kdop + x, k);
     mag[x] = m;
     for (int guard = 0; guard < 4096; ++guard) {
-        __threadfence();
         const int par = S.parent[x];
         if (par < 0) return;
-        if (atomicAdd(&arrivals[par - S.N], 1u) == 0u) return;  // the sibling is not done yet
-        __threadfence();
+        // release: our k-DOP is visible before the count moves; acquire: so is the sibling's when we are second
+        if (atomic_add_acq_rel(&arrivals[par - S.N], 1u) == 0u) return;  // the sibling is not done yet
         const int4 c = S.child[par - S.N];
+        const int sib = c.x == x ? c.y : c.x;
         // the sibling's k-DOP was written by another SM: read through L2 (no stale L1 lines)
-        const float4* a = reinterpret_cast<const float4*>(kdop + c.x);
-        const float4* b = reinterpret_cast<const float4*>(kdop + c.y);
+        const float4* b = reinterpret_cast<const float4*>(kdop + sib);
 #pragma unroll
         for (int i = 0; i < kDirs / 4; ++i) {
-            const float4 al = __ldcg(a + i), bl = __ldcg(b + i);
-            const float4 ah = __ldcg(a + kDirs / 4 + i), bh = __ldcg(b + kDirs / 4 + i);
-            k.lo[4 * i] = fminf(al.x, bl.x), k.lo[4 * i + 1] = fminf(al.y, bl.y);
-            k.lo[4 * i + 2] = fminf(al.z, bl.z), k.lo[4 * i + 3] = fminf(al.w, bl.w);
-            k.hi[4 * i] = fmaxf(ah.x, bh.x), k.hi[4 * i + 1] = fmaxf(ah.y, bh.y);
-            k.hi[4 * i + 2] = fmaxf(ah.z, bh.z), k.hi[4 * i + 3] = fmaxf(ah.w, bh.w);
+            const float4 bl = __ldcg(b + i), bh = __ldcg(b + kDirs / 4 + i);
+            k.lo[4 * i] = fminf(k.lo[4 * i], bl.x), k.lo[4 * i + 1] = fminf(k.lo[4 * i + 1], bl.y);
+            k.lo[4 * i + 2] = fminf(k.lo[4 * i + 2], bl.z), k.lo[4 * i + 3] = fminf(k.lo[4 * i + 3], bl.w);
+            k.hi[4 * i] = fmaxf(k.hi[4 * i], bh.x), k.hi[4 * i + 1] = fmaxf(k.hi[4 * i + 1], bh.y);
+            k.hi[4 * i + 2] = fmaxf(k.hi[4 * i + 2], bh.z), k.hi[4 * i + 3] = fmaxf(k.hi[4 * i + 3], bh.w);
         }
-        m = fmaxf(__ldcg(mag + c.x), __ldcg(mag + c.y));
+        m = fmaxf(m, __ldcg(mag + sib));
         store_kdop(kdop + par, k);
         mag[par] = m;
         x = par;
     }
 }
 
-// One warp per inner node of the final layout, one half-warp per child. Lane l of a half holds the child's
-// interval on direction l; the half's lanes share the triples (lane l evaluates triples l, l + 16, ...,
-// reading the three widths by shuffles), and a 16-lane minimum over (area, triple index) keeps the first
-// triple of least area, i.e. the result of a sequential scan in table order with a strict "<".
+// One warp per inner node of the final layout, one half-warp per child; lane l of a half holds the child's
+// interval on direction l. Only the 8 directions of least width take part (ranked in the half by width,
+// ties to the lower index): their C(8,3) = 56 triples are spread over the 16 lanes, each looks up 1/|det|
+// in a dense 16^3 table (0 = not admissible: |det| <= 0.2, or a direction beyond kdop_size / 2), and a
+// 16-lane minimum over (area, a*256 + b*16 + c) keeps the least area, ties to the lexicographically first
+// triple. Any triple bounds the child (every slab holds all its geometry), so the choice only steers
+// traversal cost; the axes are the fallback when no candidate triple is admissible.
 constexpr int kSobbNodeThreads = 256;
+
+// The 56 index triples i < j < k of 0..7, packed i | j << 3 | k << 6.
+__constant__ unsigned short c_combo8[56] = {
+#define DIPL_C8(i, j, k) (unsigned short)((i) | ((j) << 3) | ((k) << 6))
+    DIPL_C8(0, 1, 2), DIPL_C8(0, 1, 3), DIPL_C8(0, 1, 4), DIPL_C8(0, 1, 5), DIPL_C8(0, 1, 6), DIPL_C8(0, 1, 7),
+    DIPL_C8(0, 2, 3), DIPL_C8(0, 2, 4), DIPL_C8(0, 2, 5), DIPL_C8(0, 2, 6), DIPL_C8(0, 2, 7), DIPL_C8(0, 3, 4),
+    DIPL_C8(0, 3, 5), DIPL_C8(0, 3, 6), DIPL_C8(0, 3, 7), DIPL_C8(0, 4, 5), DIPL_C8(0, 4, 6), DIPL_C8(0, 4, 7),
+    DIPL_C8(0, 5, 6), DIPL_C8(0, 5, 7), DIPL_C8(0, 6, 7), DIPL_C8(1, 2, 3), DIPL_C8(1, 2, 4), DIPL_C8(1, 2, 5),
+    DIPL_C8(1, 2, 6), DIPL_C8(1, 2, 7), DIPL_C8(1, 3, 4), DIPL_C8(1, 3, 5), DIPL_C8(1, 3, 6), DIPL_C8(1, 3, 7),
+    DIPL_C8(1, 4, 5), DIPL_C8(1, 4, 6), DIPL_C8(1, 4, 7), DIPL_C8(1, 5, 6), DIPL_C8(1, 5, 7), DIPL_C8(1, 6, 7),
+    DIPL_C8(2, 3, 4), DIPL_C8(2, 3, 5), DIPL_C8(2, 3, 6), DIPL_C8(2, 3, 7), DIPL_C8(2, 4, 5), DIPL_C8(2, 4, 6),
+    DIPL_C8(2, 4, 7), DIPL_C8(2, 5, 6), DIPL_C8(2, 5, 7), DIPL_C8(2, 6, 7), DIPL_C8(3, 4, 5), DIPL_C8(3, 4, 6),
+    DIPL_C8(3, 4, 7), DIPL_C8(3, 5, 6), DIPL_C8(3, 5, 7), DIPL_C8(3, 6, 7), DIPL_C8(4, 5, 6), DIPL_C8(4, 5, 7),
+    DIPL_C8(4, 6, 7), DIPL_C8(5, 6, 7),
+#undef DIPL_C8
+};
 
 __global__ void __launch_bounds__(kSobbNodeThreads) sobb_node_kernel(
     SobbIn S, const BNode* __restrict__ bnodes, const uint32_t* __restrict__ rev_index, int num_inner,
-    const Kdop* __restrict__ kdop, const float* __restrict__ mag, int triples, SNode* __restrict__ snodes,
-    const uint32_t* err) {
-    __shared__ uint32_t s_tri[kMaxTriples];
-    __shared__ float s_inv[kMaxTriples];
-    for (int t = threadIdx.x; t < triples; t += kSobbNodeThreads) {
-        s_tri[t] = (uint32_t)c_triple[t][0] | ((uint32_t)c_triple[t][1] << 8) | ((uint32_t)c_triple[t][2] << 16);
-        s_inv[t] = c_inv_det[t];
-    }
+    const Kdop* __restrict__ kdop, const float* __restrict__ mag, SNode* __restrict__ snodes, const uint32_t* err) {
+    __shared__ float s_inv[kDirs * kDirs * kDirs];
+    __shared__ unsigned short s_combo[56];
+    for (int t = threadIdx.x; t < kDirs * kDirs * kDirs; t += kSobbNodeThreads)
+        s_inv[t] = ((t & 15) < S.dirs) ? c_inv3[t] : 0.0f;  // a < b < c: c < dirs admits the triple
+    for (int t = threadIdx.x; t < 56; t += kSobbNodeThreads) s_combo[t] = c_combo8[t];
     __syncthreads();
     if (*err != 0u) return;
     const int lane = threadIdx.x & 31, l = lane & 15, half = lane >> 4;
     const int warps = (int)(gridDim.x * (kSobbNodeThreads / 32));
-    // the node loop and the triple loop are warp-uniform, so every shuffle below has all 32 lanes
+    // the node loop is warp-uniform and every loop below has a fixed trip count: all shuffles see 32 lanes
     for (int k = (int)((blockIdx.x * kSobbNodeThreads + threadIdx.x) >> 5); k < num_inner; k += warps) {
         if (__float_as_int(S.node_lo[k].w) < S.L) continue;  // not an inner node of the layout
         const int4 c = S.child[k];
         const int id = half ? c.y : c.x;
         const float* kd = reinterpret_cast<const float*>(kdop + id);
         const float lo = kd[l], hi = kd[kDirs + l];
-        const float w = hi - lo;
+        float w = hi - lo;
+        if (!(w == w) || l >= S.dirs) w = __int_as_float(0x7F800000);  // NaN or unused direction: widest
+        // rank of this direction by width within the half (ties to the lower index)
+        int rank = 0;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const float wm = __shfl_sync(0xffffffffu, w, m, 16);
+            rank += (wm < w || (wm == w && m < l)) ? 1 : 0;
+        }
+        const uint32_t sel = (__ballot_sync(0xffffffffu, rank < 8) >> (16 * half)) & 0xFFFFu;
+        // lane p < 8 of the half: the p-th selected direction in index order
+        uint32_t mm = sel;
+        for (int q = 0; q < (l & 7); ++q) mm &= mm - 1u;
+        const int dir_p = __ffs(mm) - 1;
+        const float w_p = __shfl_sync(0xffffffffu, w, dir_p & 15, 16);
         float best = __int_as_float(0x7F800000);
-        int bt = 0x7FFFFFFF;  // none yet
-        for (int t0 = 0; t0 < triples; t0 += 16) {
-            const int t = t0 + l;
-            const uint32_t abc = t < triples ? s_tri[t] : 0u;
-            const int a = abc & 0xFF, b = (abc >> 8) & 0xFF, cc = abc >> 16;
-            const float wa = __shfl_sync(0xffffffffu, w, a, 16), wb = __shfl_sync(0xffffffffu, w, b, 16),
-                        wc = __shfl_sync(0xffffffffu, w, cc, 16);
-            // triples are listed with a < b < c: c < dirs admits the triple
-            if (t < triples && cc < S.dirs) {
-                const float sa = (wa * wb + wb * wc + wc * wa) * s_inv[t];
-                if (sa < best) {
+        uint32_t bkey = 0xFFFFFFFFu;
+#pragma unroll
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            const int t = c0 + l;
+            const uint32_t cb = t < 56 ? s_combo[t] : 0u;
+            const int i = cb & 7, j = (cb >> 3) & 7, q = (cb >> 6) & 7;
+            const float wa = __shfl_sync(0xffffffffu, w_p, i, 16), wb = __shfl_sync(0xffffffffu, w_p, j, 16),
+                        wc = __shfl_sync(0xffffffffu, w_p, q, 16);
+            const int a = __shfl_sync(0xffffffffu, dir_p, i, 16), b = __shfl_sync(0xffffffffu, dir_p, j, 16),
+                      cc = __shfl_sync(0xffffffffu, dir_p, q, 16);
+            const uint32_t key = (uint32_t)(a * 256 + b * 16 + cc);
+            const float inv = t < 56 ? s_inv[key & 4095u] : 0.0f;
+            if (inv > 0.0f) {
+                const float sa = (wa * wb + wb * wc + wc * wa) * inv;
+                if (sa < best || (sa == best && key < bkey)) {
                     best = sa;
-                    bt = t;
+                    bkey = key;
                 }
             }
         }
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) {
             const float ob = __shfl_xor_sync(0xffffffffu, best, o, 16);
-            const int ot = __shfl_xor_sync(0xffffffffu, bt, o, 16);
-            if (ob < best || (ob == best && ot < bt)) {
+            const uint32_t ok = __shfl_xor_sync(0xffffffffu, bkey, o, 16);
+            if (ob < best || (ob == best && ok < bkey)) {
                 best = ob;
-                bt = ot;
+                bkey = ok;
             }
         }
-        if (bt == 0x7FFFFFFF) bt = 0;  // no triple of finite area: the table's first triple (the axes)
-        const uint32_t abc = s_tri[bt];
-        const int ax0 = abc & 0xFF, ax1 = (abc >> 8) & 0xFF, ax2 = abc >> 16;
+        if (bkey == 0xFFFFFFFFu) bkey = (0u << 8) | (1u << 4) | 2u;  // the axes
+        const int ax0 = (int)(bkey >> 8), ax1 = (int)((bkey >> 4) & 15u), ax2 = (int)(bkey & 15u);
+        const uint32_t abc = (uint32_t)ax0 | ((uint32_t)ax1 << 8) | ((uint32_t)ax2 << 16);
         const float pad = mag[id] * 9.5367431640625e-07f + 1e-30f;
         const float lo0 = __shfl_sync(0xffffffffu, lo, ax0, 16) - pad, hi0 = __shfl_sync(0xffffffffu, hi, ax0, 16) + pad;
         const float lo1 = __shfl_sync(0xffffffffu, lo, ax1, 16) - pad, hi1 = __shfl_sync(0xffffffffu, hi, ax1, 16) + pad;
@@ -399,12 +436,14 @@ dipl_status upload_triples() {
         {0.70710677f, 0.f, -0.70710677f}, {0.f, 0.70710677f, 0.70710677f}, {0.f, 0.70710677f, -0.70710677f},
         {0.f, 0.52573111f, 0.85065081f}, {0.52573111f, 0.85065081f, 0.f}, {0.85065081f, 0.f, 0.52573111f},
     };
-    unsigned char tri[kMaxTriples][3];
-    float inv[kMaxTriples];
+    static float inv[kDirs * kDirs * kDirs];
     int nt = 0;
     for (int a = 0; a < kDirs; ++a)
-        for (int b = a + 1; b < kDirs; ++b)
-            for (int c = b + 1; c < kDirs; ++c) {
+        for (int b = 0; b < kDirs; ++b)
+            for (int c = 0; c < kDirs; ++c) {
+                float& slot = inv[a * kDirs * kDirs + b * kDirs + c];
+                slot = 0.0f;
+                if (!(a < b && b < c)) continue;
                 const float* A = dirs[a];
                 const float* B = dirs[b];
                 const float* Cc = dirs[c];
@@ -412,12 +451,10 @@ dipl_status upload_triples() {
                                    (double)A[1] * (B[0] * Cc[2] - B[2] * Cc[0]) +
                                    (double)A[2] * (B[0] * Cc[1] - B[1] * Cc[0]);
                 if (std::fabs(det) < 0.2) continue;
-                tri[nt][0] = (unsigned char)a, tri[nt][1] = (unsigned char)b, tri[nt][2] = (unsigned char)c;
-                inv[nt] = (float)(1.0 / std::fabs(det));
+                slot = (float)(1.0 / std::fabs(det));
                 ++nt;
             }
-    DIPL_CUDA(cudaMemcpyToSymbol(c_triple, tri, sizeof(tri)));
-    DIPL_CUDA(cudaMemcpyToSymbol(c_inv_det, inv, sizeof(inv)));
+    DIPL_CUDA(cudaMemcpyToSymbol(c_inv3, inv, sizeof(inv)));
     g_triples = nt;
     return DIPL_OK;
 }
@@ -460,8 +497,8 @@ dipl_status sobb_enqueue(const int4* child, const float4* node_lo, const float4*
         const long long grid = std::max<long long>(
             1, std::min<long long>((long long)sms * (2048 / kSobbNodeThreads),
                                    (warps_needed + kSobbNodeThreads / 32 - 1) / (kSobbNodeThreads / 32)));
-        sobb_node_kernel<<<(unsigned)grid, kSobbNodeThreads, 0, s>>>(S, bnodes, rev_index, K, kdop, sc.mag,
-                                                                     sc.triples, snodes, d_err);
+        sobb_node_kernel<<<(unsigned)grid, kSobbNodeThreads, 0, s>>>(S, bnodes, rev_index, K, kdop, sc.mag, snodes,
+                                                                     d_err);
         note_launches();
     }
     DIPL_CUDA(cudaGetLastError());
