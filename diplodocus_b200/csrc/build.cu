@@ -254,10 +254,6 @@ __global__ void code_params_kernel(const Bounds* __restrict__ bounds, int m, int
             p.s[a] = (ext[a] > 0.0f && p.bits[a] > 0) ? __fdiv_rn(cells, ext[a]) : 0.0f;
             p.top[a] = p.bits[a] >= 64 ? ~0ull : ((1ull << p.bits[a]) - 1ull);
         }
-        for (int a = 0; a < 4; ++a)
-            for (int c = 0; c < 16; ++c)
-                for (int v = 0; v < 16; ++v)
-                    out[k].dep[a][c][v] = deposit_bits((unsigned long long)v << (4 * c), p.mask[a]);
     }
     for (int a = 0; a < 4; ++a) {
         out[k].lo[a] = p.lo[a];
@@ -265,6 +261,15 @@ __global__ void code_params_kernel(const Bounds* __restrict__ bounds, int m, int
         out[k].top[a] = p.top[a];
         out[k].mask[a] = p.mask[a];
         out[k].bits[a] = p.bits[a];
+    }
+}
+
+// EMC60 deposit tables of every mesh: one block per mesh, one thread per (dimension, chunk, nibble) entry.
+__global__ void __launch_bounds__(256) emc_tables_kernel(CodeParams* params) {
+    CodeParams& p = params[blockIdx.x];
+    for (int e = threadIdx.x; e < 4 * 16 * 16; e += blockDim.x) {
+        const int a = e >> 8, c = (e >> 4) & 15, v = e & 15;
+        p.dep[a][c][v] = deposit_bits((unsigned long long)v << (4 * c), p.mask[a]);
     }
 }
 
@@ -350,6 +355,13 @@ struct PlocParams {
     int num_meshes;
     int radius;
 };
+
+// Parity-selected pointers of PlocParams (a select, so the parameter block is never copied to the stack for
+// a run-time array index).
+template <typename T>
+__device__ __forceinline__ T by_parity(T const (&a)[2], int parity) {
+    return parity ? a[1] : a[0];
+}
 
 // Clusters at most this many are finished by the single-CTA tail kernel, resident in shared memory.
 constexpr int kTailMax = 2048;
@@ -442,65 +454,6 @@ __device__ __forceinline__ void nn_search_sym(const float4* __restrict__ slo, co
     }
 }
 
-// Tail variant: every position's candidates are split over P consecutive threads (P a power of two, up to
-// 16) when there are few clusters, then the per-thread minima are combined with a 64-bit min over the
-// oracle's key (distance bits << 32 | gap << 2 | parity << 1 | side). Each thread visits its own gaps in
-// increasing order, so its local strict-"<" minimum is its subset's key minimum.
-template <int NT>
-__device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, const float4* __restrict__ shi, int n,
-                                                int q0, int q1, int r, int* __restrict__ nn) {
-    const int m = q1 - q0;
-    int P = 1;
-    while (P < 16 && 2 * P * m <= NT) P *= 2;
-    const int sub = (int)threadIdx.x & (P - 1);
-    const int lanes = NT / P;
-    const int rounds = (m + lanes - 1) / lanes;
-    for (int rd = 0; rd < rounds; ++rd) {
-        const int q = q0 + (int)threadIdx.x / P + rd * lanes;
-        unsigned long long key = ~0ull;
-        if (q < q1) {
-            const float4 a = slo[q], b = shi[q];
-            const int sg = __float_as_int(b.w);
-            float bestd = __int_as_float(0x7F800000);
-            int bestj = -1;
-            auto consider = [&](int j) {
-                if (j < 0 || j >= n) return;
-                const float4 c = slo[j], e = shi[j];
-                if (__float_as_int(e.w) != sg) return;
-                const float d = ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, e.x, e.y, e.z);
-                if (d < bestd || bestj < 0) {
-                    bestd = d;
-                    bestj = j;
-                }
-            };
-            for (int k = 1 + sub; k <= r; k += P) {
-                const bool fwd_first = (k & 1) && !(q & 1);
-                consider(fwd_first ? q + k : q - k);
-                consider(fwd_first ? q - k : q + k);
-            }
-            if (bestj >= 0) {
-                const unsigned gap = (unsigned)abs(bestj - q);
-                const unsigned mn = (unsigned)min(bestj, q);
-                key = ((unsigned long long)__float_as_uint(bestd) << 32) |
-                      (unsigned long long)((gap << 2) | ((mn & 1u) << 1) | (bestj > q ? 1u : 0u));
-            }
-        }
-        for (int o = P / 2; o > 0; o >>= 1) {
-            const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
-            key = other < key ? other : key;
-        }
-        if (q < q1 && sub == 0) {
-            int j = -1;
-            if (key != ~0ull) {
-                const unsigned tie = (unsigned)key;
-                const int gap = (int)(tie >> 2);
-                j = (tie & 1u) ? q + gap : q - gap;
-            }
-            nn[q] = j;
-        }
-    }
-}
-
 // Writes internal node `knew` = merge of clusters (la, lb, li) and (ra, rb, ri); returns the merged cluster.
 __device__ __forceinline__ void emit_node(const PlocParams& P, int knew, const float4& la, const float4& lb,
                                           const int4& li, const float4& ra, const float4& rb, const int4& ri,
@@ -543,9 +496,9 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     const int w0 = max(s0 - 2 * r, 0), w1 = min(s0 + T + 2 * r, n);
     // window: asynchronous 16-byte copies, all in flight at once (one memory round trip)
     for (int i = threadIdx.x; i < w1 - w0; i += B) {
-        cp_async16(&s.lo[i], P.lo[parity] + w0 + i);
-        cp_async16(&s.hi[i], P.hi[parity] + w0 + i);
-        cp_async16(&s.info[i], P.info[parity] + w0 + i);
+        cp_async16(&s.lo[i], by_parity(P.lo, parity) + w0 + i);
+        cp_async16(&s.hi[i], by_parity(P.hi, parity) + w0 + i);
+        cp_async16(&s.info[i], by_parity(P.info, parity) + w0 + i);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -588,7 +541,7 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     // ---- decoupled look-back over tiles: (kept, merged) prefixes (whole block) ----------------------
     {
         const unsigned long long agg = ((unsigned long long)(total & 0xFFFFu) << 31) | (total >> 16);
-        unsigned long long* st = P.status[parity];
+        unsigned long long* st = by_parity(P.status, parity);
         unsigned long long prefix = 0;
         bool ok = true;
         if (tile == 0) {  // block-uniform
@@ -614,9 +567,9 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     const uint32_t merged_before = (uint32_t)(s.prefix & 0x7FFFFFFFull);
 
     // ---- write surviving clusters and new nodes ----------------------------------------------------
-    float4* __restrict__ out_lo = P.lo[parity ^ 1];
-    float4* __restrict__ out_hi = P.hi[parity ^ 1];
-    int4* __restrict__ out_info = P.info[parity ^ 1];
+    float4* __restrict__ out_lo = by_parity(P.lo, parity ^ 1);
+    float4* __restrict__ out_hi = by_parity(P.hi, parity ^ 1);
+    int4* __restrict__ out_info = by_parity(P.info, parity ^ 1);
     uint32_t kpos = kept_before + (excl & 0xFFFFu);
     uint32_t mpos = (uint32_t)mbase + merged_before + (excl >> 16);
     const int max_internal = P.num_leaves - P.num_meshes;
@@ -682,7 +635,7 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
         // Clear the other parity's look-back words for the next iteration: it has at most n / B tiles.
         // Nobody reads that array during this iteration.
         const int next_words = (n + B - 1) / B;
-        for (int t = blockIdx.x * B + threadIdx.x; t < next_words; t += active * B) P.status[parity ^ 1][t] = 0ull;
+        for (int t = blockIdx.x * B + threadIdx.x; t < next_words; t += active * B) by_parity(P.status, parity ^ 1)[t] = 0ull;
         for (int t = blockIdx.x; t < tiles; t += active) {
             ploc_tile<B>(P, s, t, tiles, n, mbase, parity, ipt);
             __syncthreads();
@@ -710,11 +663,12 @@ constexpr int kTailCtasMax = 8;
 
 struct TailSmem {
     float4 lo[2][kTailMax];
-    float4 hi[2][kTailMax];
+    float4 hi[2][kTailMax];  // the idle half also serves as the neighbour search's key scratch
     int4 info[2][kTailMax];
-    int nn[2][kTailMax];  // by iteration parity: peers write slice k+1 while slice k may still be read
+    int nn[2][kTailMax];  // by iteration parity: peers read slice k while slice k+1 is being written
     uint32_t warp_sum[kTailThreads / 32];
 };
+static_assert(sizeof(float4) * kTailMax >= sizeof(unsigned long long) * kTailMax, "key scratch must fit");
 
 __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     extern __shared__ __align__(16) unsigned char s_raw[];
@@ -736,9 +690,9 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     }
     const uint32_t first_parity = iter & 1;
     for (int i = threadIdx.x; i < n; i += kTailThreads) {
-        cp_async16(&s.lo[0][i], P.lo[first_parity] + i);
-        cp_async16(&s.hi[0][i], P.hi[first_parity] + i);
-        cp_async16(&s.info[0][i], P.info[first_parity] + i);
+        cp_async16(&s.lo[0][i], by_parity(P.lo, first_parity) + i);
+        cp_async16(&s.hi[0][i], by_parity(P.hi, first_parity) + i);
+        cp_async16(&s.info[0][i], by_parity(P.info, first_parity) + i);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -767,13 +721,16 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
         const float4* __restrict__ hi = s.hi[cur];
         const int4* __restrict__ info = s.info[cur];
         // ---- neighbours of this CTA's slice; then every slice from its owner ---------------------------
+        // (symmetric pair search; its 64-bit key scratch is the idle half of the double-buffered boxes,
+        // which the compaction below rewrites only after the neighbours are known)
+        unsigned long long* key_scratch = reinterpret_cast<unsigned long long*>(s.hi[cur ^ 1]);
         if (solo) {
-            nn_search_split<kTailThreads>(lo, hi, n, 0, n, r, s.nn[par]);
+            nn_search_sym<kTailThreads>(lo, hi, 0, n, 0, n, r, s.nn[par], key_scratch);
             __syncthreads();
         } else {
             const int slice = (n + ctas - 1) / ctas;
             const int q0 = min(n, rank * slice), q1 = min(n, q0 + slice);
-            nn_search_split<kTailThreads>(lo, hi, n, q0, q1, r, s.nn[par]);
+            nn_search_sym<kTailThreads>(lo, hi, 0, n, q0, q1, r, s.nn[par] + q0, key_scratch);
             cluster.sync();  // release our slice, acquire the peers'
             // pull the other slices (all loads in flight at once; the owners do not write s.nn[par] again
             // before the next iteration's cluster barrier)
@@ -873,9 +830,9 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     // final clusters (one per mesh) to the buffer of the final parity, for the root pass
     const uint32_t final_iter = iter + tail_iters;
     for (int i = threadIdx.x; i < n; i += kTailThreads) {
-        P.lo[final_iter & 1][i] = s.lo[cur][i];
-        P.hi[final_iter & 1][i] = s.hi[cur][i];
-        P.info[final_iter & 1][i] = s.info[cur][i];
+        by_parity(P.lo, final_iter & 1)[i] = s.lo[cur][i];
+        by_parity(P.hi, final_iter & 1)[i] = s.hi[cur][i];
+        by_parity(P.info, final_iter & 1)[i] = s.info[cur][i];
     }
     if (threadIdx.x == 0) P.ctrl->iterations = final_iter;
 }
@@ -1413,6 +1370,10 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     }
     code_params_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(P.d_bounds, m, d0.code_type, P.d_params);
     note_launches();
+    if (d0.code_type == DIPL_CODE_EMC60) {
+        emc_tables_kernel<<<(unsigned)m, 256, 0, stream>>>(P.d_params);
+        note_launches();
+    }
     if (P.key_bytes == 4)
         codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.d_params,
                                                                        d0.code_type, P.code_shift, P.mesh_shift,
@@ -1697,6 +1658,10 @@ dipl_status compute_codes(const dipl_build_desc* desc, void* d_codes, cudaStream
     long long chunk = (N + grid - 1) / grid;
     bounds_kernel<<<(unsigned)grid, 256, 0, stream>>>(d_meshes, d_offsets, 1, N, chunk, d_bounds); note_launches();
     code_params_kernel<<<1, 32, 0, stream>>>(d_bounds, 1, desc->code_type, d_params); note_launches();
+    if (desc->code_type == DIPL_CODE_EMC60) {
+        emc_tables_kernel<<<1, 256, 0, stream>>>(d_params);
+        note_launches();
+    }
     if (desc->code_type == DIPL_CODE_MORTON30)
         codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(d_meshes, d_offsets, 1, N, d_params,
                                                                        desc->code_type, 0, 0, (uint32_t*)d_codes,

@@ -1,6 +1,6 @@
 // Stable LSD radix sort of (key, uint32 value) pairs, one kernel per digit (onesweep scheme of
 // Adinets & Merrill 2022): an up-front histogram kernel counts every digit of every pass in one read
-// of the keys; each pass kernel then ranks a 3840-key tile with warp-level match_any multisplit,
+// of the keys; each pass kernel then ranks a 4096-key tile with warp-level match_any multisplit,
 // resolves its global digit offsets by decoupled look-back over earlier tiles (bounded spin), and
 // scatters through shared memory so the global writes come out in digit runs.
 #include "internal.h"
@@ -8,10 +8,12 @@
 namespace dipl {
 namespace {
 
-constexpr int kSortThreads = 256;
+// 512 threads x 8 keys: few registers per thread (at most 64, so 3 tiles of 16 warps share an SM) keep
+// enough loads in flight to hide memory latency.
+constexpr int kSortThreads = 512;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 15;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 3840 keys
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys
 constexpr int kMaxPasses = 11;
 
 // Look-back word: 2-bit state in the top bits, 30-bit count below.
@@ -97,7 +99,7 @@ struct SortSmem {
 };
 
 template <typename K, int BITS>
-__global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
+__global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(
     const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int64_t n, int shift, int width, const uint32_t* __restrict__ pass_hist,
     uint32_t* __restrict__ lookback, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ err) {

@@ -26,8 +26,9 @@ constexpr int64_t kNoAllocMaxKeys = int64_t(1) << 18;
 constexpr size_t kErrBytes = 256;
 constexpr size_t kAltKeyBytes = size_t(kNoAllocMaxKeys) * 8;  // room for 64-bit keys
 constexpr size_t kAltValBytes = size_t(kNoAllocMaxKeys) * 4;
-// Histograms + look-back words of the widest choice: 10-bit digits over 64-bit keys (7 passes), 3840-key
-// tiles (the largest radix_sort_scratch_bytes over the accepted digit widths and key widths).
+// Histograms + look-back words of the widest choice: 10-bit digits over 64-bit keys (7 passes), counted
+// for 3840-key tiles, which bounds the tile count of the sort's larger tiles (radix_sort_scratch_bytes is
+// checked against this size on every call).
 constexpr size_t kSortTilesMax = (size_t(kNoAllocMaxKeys) + 3839) / 3840;
 constexpr size_t kSortScratchBytes = (11 * 1024 + 64) * 4 + 7 * kSortTilesMax * 1024 * 4 + 256;
 constexpr size_t kNoAllocScratchBytes = kErrBytes + kAltKeyBytes + kAltValBytes + kSortScratchBytes;
