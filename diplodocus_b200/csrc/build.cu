@@ -366,8 +366,9 @@ __device__ __forceinline__ T by_parity(T const (&a)[2], int parity) {
 // Clusters at most this many are finished by the single-CTA tail kernel, resident in shared memory.
 constexpr int kTailMax = 2048;
 constexpr int kTailThreads = 1024;
-// At most this many clusters: CTA 0 finishes alone (no cluster exchange per iteration).
-constexpr int kTailSolo = 512;
+// At most this many clusters: CTA 0 finishes alone (no cluster exchange per iteration). Below this size a
+// search over all positions costs less than one cluster barrier plus the exchange of the slices.
+constexpr int kTailSolo = 128;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -451,6 +452,67 @@ __device__ __forceinline__ void nn_search_sym(const float4* __restrict__ slo, co
             j = (tie & 1u) ? q + gap : q - gap;
         }
         nn[q - q0] = j;
+    }
+}
+
+// Tail variant: every position's candidates are split over P consecutive threads (P a power of two, up to
+// 16) when there are few clusters, then the per-thread minima are combined with a 64-bit min over the
+// oracle's key (distance bits << 32 | gap << 2 | parity << 1 | side). Each thread visits its own gaps in
+// increasing order, so its local strict-"<" minimum is its subset's key minimum.
+template <int NT>
+__device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, const float4* __restrict__ shi, int n,
+                                                int q0, int q1, int r, int* __restrict__ nn) {
+    const int m = q1 - q0;
+    int P = 1;
+    while (P < 16 && 2 * P * m <= NT) P *= 2;
+    const int sub = (int)threadIdx.x & (P - 1);
+    const int lanes = NT / P;
+    const int rounds = (m + lanes - 1) / lanes;
+    for (int rd = 0; rd < rounds; ++rd) {
+        const int q = q0 + (int)threadIdx.x / P + rd * lanes;
+        // a warp covers 32 / P consecutive positions: warps past the last one have nothing to do
+        if (q0 + (int)(threadIdx.x & ~31u) / P + rd * lanes >= q1) break;
+        unsigned long long key = ~0ull;
+        if (q < q1) {
+            const float4 a = slo[q], b = shi[q];
+            const int sg = __float_as_int(b.w);
+            float bestd = __int_as_float(0x7F800000);
+            int bestj = -1;
+            auto consider = [&](int j) {
+                if (j < 0 || j >= n) return;
+                const float4 c = slo[j], e = shi[j];
+                if (__float_as_int(e.w) != sg) return;
+                const float d = ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, e.x, e.y, e.z);
+                if (d < bestd || bestj < 0) {
+                    bestd = d;
+                    bestj = j;
+                }
+            };
+            for (int k = 1 + sub; k <= r; k += P) {
+                const bool fwd_first = (k & 1) && !(q & 1);
+                consider(fwd_first ? q + k : q - k);
+                consider(fwd_first ? q - k : q + k);
+            }
+            if (bestj >= 0) {
+                const unsigned gap = (unsigned)abs(bestj - q);
+                const unsigned mn = (unsigned)min(bestj, q);
+                key = ((unsigned long long)__float_as_uint(bestd) << 32) |
+                      (unsigned long long)((gap << 2) | ((mn & 1u) << 1) | (bestj > q ? 1u : 0u));
+            }
+        }
+        for (int o = P / 2; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+            key = other < key ? other : key;
+        }
+        if (q < q1 && sub == 0) {
+            int j = -1;
+            if (key != ~0ull) {
+                const unsigned tie = (unsigned)key;
+                const int gap = (int)(tie >> 2);
+                j = (tie & 1u) ? q + gap : q - gap;
+            }
+            nn[q] = j;
+        }
     }
 }
 
@@ -663,12 +725,11 @@ constexpr int kTailCtasMax = 8;
 
 struct TailSmem {
     float4 lo[2][kTailMax];
-    float4 hi[2][kTailMax];  // the idle half also serves as the neighbour search's key scratch
+    float4 hi[2][kTailMax];
     int4 info[2][kTailMax];
     int nn[2][kTailMax];  // by iteration parity: peers read slice k while slice k+1 is being written
     uint32_t warp_sum[kTailThreads / 32];
 };
-static_assert(sizeof(float4) * kTailMax >= sizeof(unsigned long long) * kTailMax, "key scratch must fit");
 
 __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     extern __shared__ __align__(16) unsigned char s_raw[];
@@ -721,16 +782,14 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
         const float4* __restrict__ hi = s.hi[cur];
         const int4* __restrict__ info = s.info[cur];
         // ---- neighbours of this CTA's slice; then every slice from its owner ---------------------------
-        // (symmetric pair search; its 64-bit key scratch is the idle half of the double-buffered boxes,
-        // which the compaction below rewrites only after the neighbours are known)
-        unsigned long long* key_scratch = reinterpret_cast<unsigned long long*>(s.hi[cur ^ 1]);
+        // (each position's candidates split over up to 16 threads: few positions, short searches)
         if (solo) {
-            nn_search_sym<kTailThreads>(lo, hi, 0, n, 0, n, r, s.nn[par], key_scratch);
+            nn_search_split<kTailThreads>(lo, hi, n, 0, n, r, s.nn[par]);
             __syncthreads();
         } else {
             const int slice = (n + ctas - 1) / ctas;
             const int q0 = min(n, rank * slice), q1 = min(n, q0 + slice);
-            nn_search_sym<kTailThreads>(lo, hi, 0, n, q0, q1, r, s.nn[par] + q0, key_scratch);
+            nn_search_split<kTailThreads>(lo, hi, n, q0, q1, r, s.nn[par]);
             cluster.sync();  // release our slice, acquire the peers'
             // pull the other slices (all loads in flight at once; the owners do not write s.nn[par] again
             // before the next iteration's cluster barrier)
