@@ -193,6 +193,20 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------------------------------
+# DRAM bytes (read + write) of one build and of one 4M-ray closest-hit trace of the default workload, from one
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, summed over the build's kernels):
+# profiles/dram_traffic_displaced_sphere_1m.md. Other workloads report null.
+MEASURED_TRAFFIC = {"displaced_sphere": {"build": 489.09e6, "trace": 360.96e6, "rays": 4194304,
+                                         "triangles": 1046528}}
+
+
+def measured_traffic(workload, kind, n_tri, n_rays):
+    m = MEASURED_TRAFFIC.get(workload)
+    if not m or m["triangles"] != n_tri or m["rays"] != n_rays:
+        return None
+    return m[kind]
+
+
 def build_bytes_per_tri(code_type, digit_bits=8, node_bytes_per_tri=None):
     """Algorithmic bytes of one build per triangle (byte model, Morton30: 176 B, EMC60: 308 B)."""
     k = 4 if code_type == 0 else 8
@@ -346,11 +360,16 @@ def run_gpu(args, rank, world, local_rank):
         "build_ms": round(build_s * 1e3, 4), "trace_ms": round(trace_s * 1e3, 4),
         "sah_cost": round(sah.value, 4), "ploc_iterations": int(info.ploc_iterations), "bvh_depth": int(info.depth),
         "roofline": {"bound": "hbm", "achieved": round(achieved_build, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved_build / peak, 4), "traffic": None,
+                     "frac": round(achieved_build / peak, 4),
+                     "traffic": measured_traffic(args.workload, "build", n, nr) if args.code == "morton30" else None,
                      "kernel": "build pipeline (bounds, codes, sort, PLOC, layout)",
+                     "traffic_note": "bytes per build from one ncu capture (cold caches per kernel), "
+                                     "profiles/dram_traffic_displaced_sphere_1m.md",
                      "bytes_per_unit": round(bpt, 1), "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
         "roofline_trace": {"bound": "hbm", "achieved": round(achieved_trace, 1), "peak": peak, "unit": "GB/s",
-                           "frac": round(achieved_trace / peak, 4), "bytes_per_ray": round(ray_bytes, 1)},
+                           "frac": round(achieved_trace / peak, 4), "bytes_per_ray": round(ray_bytes, 1),
+                           "traffic": measured_traffic(args.workload, "trace", n, nr)
+                           if args.leaf_test == "ref_mt" and args.code == "morton30" else None},
         "e2e": {"value": round(world * n * steps / (t_e2e / 1e3) / 1e6, 3), "unit": "Mtri/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "note": "whole step (H2D vertices + build + H2D rays + trace + D2H hits) per triangle"},
