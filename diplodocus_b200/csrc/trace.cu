@@ -7,7 +7,8 @@
 // Closest-hit rule: among triangles with tmin < t < tmax, the smallest t, ties to the lowest primitive id.
 // That is exactly what the reference brute force returns (ascending ids, strict <,
 // dummy_acceleration_structure.cc:21-64). To keep it under any traversal order the box tests are
-// conservative: slab distances widen by 1e-6 relative (their own rounding is below 2e-7), boxes are padded
+// conservative: slab distances widen by 1e-6 relative (their own rounding, with the approximate reciprocal
+// of the direction, stays below 5e-7), boxes are padded
 // by 2^-20 of their coordinate magnitude at build time, and a node is pruned only when it starts beyond
 // the best t by more than 1e-5 relative, so a node can never be skipped for rounding of its own box.
 #include "internal.h"
@@ -25,6 +26,12 @@ struct RayState {
     float tmin, tmax;
 };
 
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ RayState load_ray(const dipl_ray* rays, int64_t i) {
     const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * i;
     const float4 a = __ldg(r4), b = __ldg(r4 + 1);
@@ -34,9 +41,11 @@ __device__ __forceinline__ RayState load_ray(const dipl_ray* rays, int64_t i) {
     r.tmin = a.w;
     r.tmax = b.w;
     // Directions below 1e-20 in magnitude are treated as +-1e-20 so that 1/d stays finite and a ray lying
-    // on a slab plane is still inside it (0 * inf would be NaN).
+    // on a slab plane is still inside it (0 * inf would be NaN). 1/d only feeds the slab tests, which widen
+    // their interval by 1e-6 relative: the hardware reciprocal (relative error below 2^-22) is well inside
+    // that margin.
     auto safe = [](float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; };
-    r.inv = make_float3(__frcp_rn(safe(r.d.x)), __frcp_rn(safe(r.d.y)), __frcp_rn(safe(r.d.z)));
+    r.inv = make_float3(rcp_approx(safe(r.d.x)), rcp_approx(safe(r.d.y)), rcp_approx(safe(r.d.z)));
     return r;
 }
 
