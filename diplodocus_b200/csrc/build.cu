@@ -982,29 +982,27 @@ __device__ __forceinline__ void write_tri(const MeshDesc* meshes, const long lon
     tris[3 * (long long)slot + 2] = make_float4(t.c.x, t.c.y, t.c.z, 0.0f);
 }
 
+// One thread per sorted position: the position's leaf (the highest ancestor with fewer than L triangles) and
+// its rank in the leaf's left-to-right order (the triangle counts of the left siblings met on the way up) give
+// its slot directly, so every thread gathers and writes one triangle (no per-leaf loop).
 __global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
                                   const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
-                                  const uint32_t* __restrict__ starts, const int* __restrict__ owner_leaf,
-                                  int* __restrict__ leaf_start_of, float4* __restrict__ tris, const uint32_t* err) {
+                                  const uint32_t* __restrict__ starts, int* __restrict__ leaf_start_of,
+                                  float4* __restrict__ tris, const uint32_t* err) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.num_leaves || *err != 0u) return;
-    int x = owner_leaf[p];
-    if (x < 0) return;
-    int start = (int)starts[p];
-    leaf_start_of[x] = start;
-    int stack[16];
-    int sp = 0, slot = start;
-    stack[sp++] = x;
-    while (sp > 0) {
-        int y = stack[--sp];
-        if (y < P.num_leaves) {
-            write_tri(meshes, offsets, m, perm, y, tris, slot++);
-        } else if (sp + 2 <= 16) {
-            int4 c = P.child[y - P.num_leaves];
-            stack[sp++] = c.y;  // right after left
-            stack[sp++] = c.x;
-        }
+    int x = p, rank = 0;
+    for (int guard = 0; guard < 64; ++guard) {
+        const int par = P.parent[x];
+        if (par < 0 || node_count(P, par) >= P.L) break;
+        const int4 c = P.child[par - P.num_leaves];
+        if (c.y == x) rank += node_count(P, c.x);
+        x = par;
     }
+    const int first = node_pmin(P, x);
+    const int start = (int)starts[first];
+    if (p == first) leaf_start_of[x] = start;
+    write_tri(meshes, offsets, m, perm, p, tris, start + rank);
 }
 
 __device__ __forceinline__ float pad_down(float lo, float hi) {
@@ -1491,7 +1489,7 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     if ((st = exclusive_scan_u32(P.contrib, P.contrib, N, nullptr, P.scan_scratch, stream, P.d_err)) != DIPL_OK)
         return st;
     leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.contrib,
-                                                               P.owner_leaf, P.leaf_start_of, P.tris, P.d_err);
+                                                               P.leaf_start_of, P.tris, P.d_err);
     note_launches();
     if (K > 0) {
         node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.tbox, P.d_offsets, m, P.perm, P.rev_flags,
