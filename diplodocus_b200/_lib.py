@@ -28,7 +28,8 @@ EXPORTS = [
     "dipl_bvh_trace_closest",
     "dipl_bvh_trace_closest_counted", "dipl_bvh_trace_any", "dipl_bvh_sah_cost", "dipl_bvh_get_info",
     "dipl_bvh_download_topology", "dipl_bvh_download_layout", "dipl_bvh_check_errors", "dipl_bvh_destroy", "dipl_compute_codes",
-    "dipl_radix_sort_pairs", "dipl_radix_sort_pairs_noalloc", "dipl_reintersect_f64", "dipl_trace_adjoint", "dipl_status_string",
+    "dipl_radix_sort_pairs", "dipl_radix_sort_pairs_noalloc", "dipl_reintersect_f64", "dipl_trace_adjoint",
+    "dipl_generate_pinhole_rays", "dipl_generate_bounce_rays", "dipl_status_string",
     "dipl_last_error", "dipl_abi_version", "dipl_kernel_launch_count",
 ]
 
@@ -46,6 +47,12 @@ class BvhInfo(C.Structure):
                 ("ploc_iterations", C.c_int32), ("code_type", C.c_int32), ("bv_type", C.c_int32),
                 ("layout", C.c_int32), ("max_triangles_per_leaf", C.c_int32), ("nn_search_radius", C.c_int32),
                 ("kdop_size", C.c_int32)]
+
+
+class Camera(C.Structure):
+    """dipl_camera: pinhole camera (pos, dir, up, fov in radians, far = primary rays' tmax)."""
+    _fields_ = [("pos", C.c_float * 3), ("dir", C.c_float * 3), ("up", C.c_float * 3), ("fov", C.c_float),
+                ("far_t", C.c_float)]
 
 
 class DiplError(RuntimeError):
@@ -89,6 +96,8 @@ def load(path: str = LIB_PATH):
         "dipl_radix_sort_pairs_noalloc": (i32, [vp, vp, vp, vp, i64, i32, i32, i32, i32, vp]),
         "dipl_reintersect_f64": (i32, [vp, vp, vp, vp, vp, i64, vp, vp]),
         "dipl_trace_adjoint": (i32, [vp, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]),
+        "dipl_generate_pinhole_rays": (i32, [C.POINTER(Camera), i32, i32, vp, vp]),
+        "dipl_generate_bounce_rays": (i32, [vp, vp, vp, vp, vp, i64, u32, vp, vp]),
         "dipl_status_string": (C.c_char_p, [i32]),
         "dipl_last_error": (C.c_char_p, []),
         "dipl_abi_version": (i32, []),

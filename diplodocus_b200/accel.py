@@ -343,6 +343,40 @@ def trace_adjoint(v, rays: torch.Tensor, hits: Hits, dtuv: torch.Tensor):
     return dv[0], dv[1], dv[2], dorig, ddir
 
 
+# -- GPU frontend: wavefront ray generation (generate -> trace -> bounce -> trace) ---------------------------
+def generate_pinhole_rays(cam_pos, cam_dir, cam_up, fov, far, width, height, device="cuda") -> torch.Tensor:
+    """One primary ray per pixel (row-major from the top-left), generated on the device (dipl_generate_pinhole_rays)."""
+    lib = L.load()
+    cam = L.Camera((C.c_float * 3)(*cam_pos), (C.c_float * 3)(*cam_dir), (C.c_float * 3)(*cam_up), float(fov),
+                   float(far))
+    rays = torch.empty((width * height, 8), dtype=torch.float32, device=device)
+    L.check(lib.dipl_generate_pinhole_rays(C.byref(cam), int(width), int(height), _ptr(rays), _stream()),
+            "dipl_generate_pinhole_rays")
+    return rays
+
+
+def generate_bounce_rays(v, rays: torch.Tensor, hits: Hits, seed: int) -> torch.Tensor:
+    """One cosine-weighted bounce ray per hit, on the device (dipl_generate_bounce_rays); misses get a ray that
+    hits nothing. ``v`` are the SoA vertex arrays the BVH was built from."""
+    lib = L.load()
+    n = rays.shape[0]
+    out = torch.empty_like(rays)
+    L.check(lib.dipl_generate_bounce_rays(_ptr(v[0]), _ptr(v[1]), _ptr(v[2]), _ptr(rays), _ptr(hits.raw), n,
+                                          int(seed) & 0xFFFFFFFF, _ptr(out), _stream()), "dipl_generate_bounce_rays")
+    return out
+
+
+def trace_frame(bvh: "GpuPlocBvh", camera: dict, width: int, height: int, seed: int):
+    """One wavefront frame of the renderer path: primary rays, their closest hits, one bounce ray per hit and
+    the bounce hits, all on the device. Returns (primary rays, primary hits, bounce rays, bounce hits)."""
+    rays = generate_pinhole_rays(camera["cam_pos"], camera["cam_dir"], camera["cam_up"], camera["fov"],
+                                 camera["far"], width, height)
+    hits = bvh.Intersect(Stats(), rays)
+    bounce = generate_bounce_rays(bvh._v, rays, hits, seed)
+    bhits = bvh.Intersect(Stats(), bounce)
+    return rays, hits, bounce, bhits
+
+
 class BuildPlan:
     """A batch of meshes captured once into a CUDA graph (dipl_build_plan_*); ``launch`` rebuilds every BVH from
     the current vertex contents; ``bvhs`` waits and returns one GpuPlocBvh per mesh for the latest build."""

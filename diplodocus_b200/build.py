@@ -18,8 +18,10 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libdipl_bvh.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Host code is compiled without floating-point contraction: host-side FP32 set-up (the camera basis) must round
+# like the host restatement that checks it.
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-         "-I" + os.path.join(ROOT, "include")]
+         "-Xcompiler", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
 
 def _headers():

@@ -1,0 +1,191 @@
+// GPU frontend: wavefront ray generation for the renderer path that traces through the engine
+// (generate -> dipl_bvh_trace_closest -> bounce -> dipl_bvh_trace_closest), replacing the per-pixel set-up
+// of RaytracingBounceKernel (src/gpu/renderer/gpu_renderer_api.cu:43-53) and the next-segment sampling of
+// TracePath (src/gpu/renderer/gpu_pathtracer.cu:12), which the reference runs around DummyIntersect.
+//
+// Both kernels use only IEEE add, mul, div and sqrt in FP32, in a fixed order and without FMA contraction
+// (explicit _rn intrinsics), so the host restatement reproduces every record bit for bit.
+#include <cmath>
+
+#include "internal.h"
+
+namespace dipl {
+namespace {
+
+constexpr int kGenThreads = 256;
+constexpr uint32_t kBounceStream = 6;  // hash stream of bounce sampling (distinct from the other uses of a seed)
+constexpr int kDiskTries = 16;         // rejection draws for a point of the unit disk (fails with p < 1e-10)
+
+struct V3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ V3 v_add(V3 a, V3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ V3 v_sub(V3 a, V3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ V3 v_scale(V3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
+__device__ __forceinline__ float v_dot(V3 a, V3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+// Cross (src/util/vec3.h:119-121): (a.y b.z - a.z b.y, a.z b.x - a.x b.z, a.x b.y - a.y b.x).
+__device__ __forceinline__ V3 v_cross(V3 a, V3 b) {
+    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+// v / |v|, |v| = sqrt((x x + y y) + z z), each component divided (Normalize, src/util/vec3.h:111-117).
+__device__ __forceinline__ V3 v_normalize(V3 v) {
+    const float len = __fsqrt_rn(v_dot(v, v));
+    return {__fdiv_rn(v.x, len), __fdiv_rn(v.y, len), __fdiv_rn(v.z, len)};
+}
+
+// HashU32 (src/util/util.h:24-32) and the (seed, stream, index, dimension) key of the workload generators.
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7FEB352Du;
+    x ^= x >> 15;
+    x *= 0x846CA68Bu;
+    x ^= x >> 16;
+    return x;
+}
+__device__ __forceinline__ float u01_key(uint32_t seed, uint32_t stream, uint64_t idx, uint32_t dim) {
+    const uint32_t k = seed * 0x9E3779B1u + stream * 0x85EBCA6Bu + dim * 0xC2B2AE35u;
+    const uint32_t lo = (uint32_t)idx, hi = (uint32_t)(idx >> 32);
+    const uint32_t h = hash_u32(k ^ hash_u32(lo ^ hash_u32(hi + dim)));
+    return (float)(h >> 8) * (1.0f / 16777216.0f);  // U01FromU32 (util.h:34-37): exact in FP32
+}
+
+struct CameraBasis {
+    V3 pos, p00, qw, qh;
+    float far_t;
+};
+
+__global__ void __launch_bounds__(kGenThreads) pinhole_kernel(CameraBasis cb, int width, int64_t n,
+                                                              dipl_ray* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)kGenThreads + threadIdx.x;
+    if (i >= n) return;
+    const float x = (float)(int)(i % width), y = (float)(int)(i / width);
+    const V3 d = v_normalize(v_add(v_add(cb.p00, v_scale(cb.qw, x)), v_scale(cb.qh, y)));
+    float4* o4 = reinterpret_cast<float4*>(out + i);
+    o4[0] = make_float4(cb.pos.x, cb.pos.y, cb.pos.z, kEpsilon);
+    o4[1] = make_float4(d.x, d.y, d.z, cb.far_t);
+}
+
+// RayEpsilon (src/scene/ray.h:15-24).
+__device__ __forceinline__ float ray_epsilon(V3 p, float t) {
+    const float p_scale = fmaxf(fmaxf(fmaxf(fabsf(p.x), fabsf(p.y)), fabsf(p.z)), 1.0f);
+    const float t_scale = fmaxf(t, 1.0f);
+    const float bias = fmaxf(__fmul_rn(1e-6f, p_scale), __fmul_rn(1e-7f, t_scale));
+    return fminf(fmaxf(bias, 1e-7f), 1e-3f);
+}
+
+__global__ void __launch_bounds__(kGenThreads) bounce_kernel(const float* __restrict__ v0, const float* __restrict__ v1,
+                                                             const float* __restrict__ v2,
+                                                             const dipl_ray* __restrict__ rays,
+                                                             const dipl_hit* __restrict__ hits, int64_t n,
+                                                             uint32_t seed, dipl_ray* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)kGenThreads + threadIdx.x;
+    if (i >= n) return;
+    const int4 h = __ldg(reinterpret_cast<const int4*>(hits) + i);
+    float4* o4 = reinterpret_cast<float4*>(out + i);
+    if (h.x < 0) {  // a miss: a ray that can hit nothing (tmin > tmax)
+        o4[0] = make_float4(0.0f, 0.0f, 0.0f, kEpsilon);
+        o4[1] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+        return;
+    }
+    const float4 ra = __ldg(reinterpret_cast<const float4*>(rays + i)), rb = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
+    const V3 o = {ra.x, ra.y, ra.z}, din = {rb.x, rb.y, rb.z};
+    const float t = __int_as_float(h.y);
+    const int64_t p = h.x;
+    const V3 a = {__ldg(v0 + 3 * p), __ldg(v0 + 3 * p + 1), __ldg(v0 + 3 * p + 2)};
+    const V3 b = {__ldg(v1 + 3 * p), __ldg(v1 + 3 * p + 1), __ldg(v1 + 3 * p + 2)};
+    const V3 c = {__ldg(v2 + 3 * p), __ldg(v2 + 3 * p + 1), __ldg(v2 + 3 * p + 2)};
+    V3 ng = v_cross(v_sub(b, a), v_sub(c, a));
+    const float len2 = v_dot(ng, ng);
+    if (!(len2 > 0.0f)) {
+        ng = {-din.x, -din.y, -din.z};  // degenerate triangle: the normal faces the ray
+    } else {
+        ng = v_normalize(ng);
+        if (v_dot(ng, din) > 0.0f) ng = {-ng.x, -ng.y, -ng.z};  // facing the incoming ray
+    }
+    // a point of the unit disk by rejection, lifted to the hemisphere: cosine-weighted (Malley's method)
+    float dx = 0.0f, dy = 0.0f, r2 = 0.0f;
+    for (int k = 0; k < kDiskTries; ++k) {
+        const float x = __fsub_rn(__fmul_rn(2.0f, u01_key(seed, kBounceStream, (uint64_t)i, 2u * k)), 1.0f);
+        const float y = __fsub_rn(__fmul_rn(2.0f, u01_key(seed, kBounceStream, (uint64_t)i, 2u * k + 1u)), 1.0f);
+        const float q = __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
+        if (q < 1.0f) {
+            dx = x, dy = y, r2 = q;
+            break;
+        }
+    }
+    const float dz = __fsqrt_rn(__fsub_rn(1.0f, r2));
+    const V3 helper = fabsf(ng.x) > 0.9f ? V3{0.0f, 1.0f, 0.0f} : V3{1.0f, 0.0f, 0.0f};
+    const V3 tx = v_normalize(v_cross(helper, ng));
+    const V3 ty = v_cross(ng, tx);
+    const V3 d = v_normalize(v_add(v_add(v_scale(tx, dx), v_scale(ty, dy)), v_scale(ng, dz)));
+    const V3 pos = v_add(o, v_scale(din, t));  // Ray::At (src/scene/ray.h:13)
+    const float eps = ray_epsilon(pos, t);
+    const V3 org = v_add(pos, v_scale(ng, eps));  // d lies on ng's side: OffsetRayOrigin's offset is +ng
+    o4[0] = make_float4(org.x, org.y, org.z, kEpsilon);
+    o4[1] = make_float4(d.x, d.y, d.z, kInfinity);
+}
+
+// Camera basis on the host, the reference renderers' formula (cpu_raytracer.cc:64-70) in FP32; 2 tan(fov/2) is
+// evaluated once in double precision (tan of the FP32 half angle, rounded to FP32).
+CameraBasis camera_basis(const dipl_camera& c, int w, int h) {
+    auto add = [](V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; };
+    auto sub = [](V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; };
+    auto scale = [](V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; };
+    auto cross = [](V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; };
+    auto normalize = [](V3 v) {
+        volatile float s = (v.x * v.x + v.y * v.y) + v.z * v.z;  // no contraction: separate products and sums
+        const float len = std::sqrt((float)s);
+        return V3{v.x / len, v.y / len, v.z / len};
+    };
+    const V3 dir = {c.dir[0], c.dir[1], c.dir[2]}, up = {c.up[0], c.up[1], c.up[2]};
+    const V3 right = normalize(cross(dir, up));
+    const float half = c.fov / 2.0f;
+    const float gw = (float)(2.0 * std::tan((double)half));
+    const float gh = gw * ((float)h / (float)w);
+    const V3 qw = scale(right, gw / (float)(w - 1));
+    const V3 qh = scale(V3{-up.x, -up.y, -up.z}, gh / (float)(h - 1));
+    const V3 p00 = add(sub(dir, scale(right, gw / 2.0f)), scale(up, gh / 2.0f));
+    CameraBasis cb;
+    cb.pos = {c.pos[0], c.pos[1], c.pos[2]};
+    cb.p00 = p00, cb.qw = qw, cb.qh = qh, cb.far_t = c.far_t;
+    return cb;
+}
+
+}  // namespace
+}  // namespace dipl
+
+using namespace dipl;
+
+extern "C" dipl_status dipl_generate_pinhole_rays(const dipl_camera* camera, int32_t width, int32_t height,
+                                                  dipl_ray* d_rays, void* stream) {
+    DIPL_CHECK_ARG(camera && width >= 2 && height >= 2, "camera must be non-NULL and width, height >= 2");
+    DIPL_CHECK_ARG(d_rays && (reinterpret_cast<uintptr_t>(d_rays) & 15) == 0, "d_rays must be 16-byte aligned");
+    const int64_t n = (int64_t)width * height;
+    const CameraBasis cb = camera_basis(*camera, width, height);
+    pinhole_kernel<<<(unsigned)((n + kGenThreads - 1) / kGenThreads), kGenThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        cb, width, n, d_rays);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return DIPL_OK;
+}
+
+extern "C" dipl_status dipl_generate_bounce_rays(const float* d_v0, const float* d_v1, const float* d_v2,
+                                                 const dipl_ray* d_rays, const dipl_hit* d_hits, int64_t n,
+                                                 uint32_t seed, dipl_ray* d_out, void* stream) {
+    DIPL_CHECK_ARG(n >= 0, "n must be >= 0");
+    if (n == 0) return DIPL_OK;
+    DIPL_CHECK_ARG(d_v0 && d_v1 && d_v2 && d_rays && d_hits && d_out, "arrays must be non-NULL");
+    DIPL_CHECK_ARG((reinterpret_cast<uintptr_t>(d_rays) & 15) == 0 && (reinterpret_cast<uintptr_t>(d_hits) & 15) == 0 &&
+                       (reinterpret_cast<uintptr_t>(d_out) & 15) == 0,
+                   "rays, hits and output must be 16-byte aligned");
+    DIPL_CHECK_ARG(d_out != d_rays, "d_out may not alias d_rays");
+    bounce_kernel<<<(unsigned)((n + kGenThreads - 1) / kGenThreads), kGenThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        d_v0, d_v1, d_v2, d_rays, d_hits, n, seed, d_out);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return DIPL_OK;
+}

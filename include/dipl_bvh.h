@@ -239,6 +239,38 @@ DIPL_API dipl_status dipl_trace_adjoint(const float* d_v0, const float* d_v1, co
                                const dipl_hit* d_hits, const float* d_dtuv, int64_t n, float* d_dv0, float* d_dv1,
                                float* d_dv2, float* d_dorig, float* d_ddir, void* stream);
 
+/* ---- GPU frontend: wavefront ray generation (generate -> trace -> bounce -> trace) ------------------------ */
+
+/* Pinhole camera of the reference scene (Camera: pos, dir, up, fov in radians; far = the primary rays' t_max). */
+typedef struct dipl_camera {
+    float pos[3];
+    float dir[3];
+    float up[3];
+    float fov;
+    float far_t;
+} dipl_camera;
+
+/* One primary ray per pixel, row-major from the top-left pixel, into d_rays (width * height records).
+ * Replaces the per-pixel ray set-up of the reference renderers: the camera basis of
+ * CpuRaytracer::StartRender / GpuRenderer::StartRender (src/renderer/cpu_raytracer.cc:64-70,
+ * src/renderer/gpu_renderer.cc:25-35) and the direction of RaytracingBounceKernel
+ * (src/gpu/renderer/gpu_renderer_api.cu:43-53): dir = normalize(p00 + qw*x + qh*y), with the CPU build's
+ * Normalize (src/util/vec3.h:111-117) in FP32 without FMA; origin = pos, tmin = 1e-6, tmax = far_t. */
+DIPL_API dipl_status dipl_generate_pinhole_rays(const dipl_camera* camera, int32_t width, int32_t height,
+                                                dipl_ray* d_rays, void* stream);
+
+/* One cosine-weighted bounce ray per hit (the renderer's next path segment, TracePath in
+ * src/gpu/renderer/gpu_pathtracer.cu:12). For hit i: the hit point o + d*t, the triangle's geometric normal
+ * (from the vertex arrays, facing the incoming ray), a direction drawn from the cosine-weighted hemisphere
+ * about it with the reference's counter-based hash (HashU32 / U01FromU32, src/util/util.h:24-37; seed, ray
+ * index), and the origin offset along the normal by RayEpsilon (src/scene/ray.h:15-24) like OffsetRayOrigin
+ * (src/renderer/cpu_raytracer.cc:41-46); tmax = FLT_MAX. Misses give a ray that hits nothing (tmax = 0).
+ * All arithmetic is IEEE add/mul/div/sqrt in FP32 in a fixed order, so the records are reproducible bit for
+ * bit on the host. d_out may not alias d_rays. */
+DIPL_API dipl_status dipl_generate_bounce_rays(const float* d_v0, const float* d_v1, const float* d_v2,
+                                               const dipl_ray* d_rays, const dipl_hit* d_hits, int64_t n,
+                                               uint32_t seed, dipl_ray* d_out, void* stream);
+
 DIPL_API const char* dipl_status_string(dipl_status status);
 /* Message of the calling thread's most recent failure ("" if none). */
 DIPL_API const char* dipl_last_error(void);

@@ -549,3 +549,115 @@ void orc_test_pairs(const float* tris, const float* rays, int64_t nr, const int3
         v_out[r] = b2;
     }
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* GPU frontend restated: pinhole primary rays and cosine-weighted bounce rays, FP32 in the     */
+/* device kernels' operation order (IEEE add/mul/div/sqrt only; this file is compiled with      */
+/* -ffp-contract=off), so every record must match bit for bit.                                  */
+/* Camera basis: the reference renderers' formula (src/renderer/cpu_raytracer.cc:64-70);        */
+/* Normalize divides each component by sqrt((x x + y y) + z z) (src/util/vec3.h:111-117).        */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct { float x, y, z; } orc_v3;
+static orc_v3 v3_add(orc_v3 a, orc_v3 b) { orc_v3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+static orc_v3 v3_sub(orc_v3 a, orc_v3 b) { orc_v3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static orc_v3 v3_scale(orc_v3 a, float s) { orc_v3 r = {a.x * s, a.y * s, a.z * s}; return r; }
+static float v3_dot(orc_v3 a, orc_v3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static orc_v3 v3_cross(orc_v3 a, orc_v3 b) {
+    orc_v3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+static orc_v3 v3_normalize(orc_v3 v) {
+    float len = sqrtf(v3_dot(v, v));
+    orc_v3 r = {v.x / len, v.y / len, v.z / len};
+    return r;
+}
+
+/* cam: pos[3], dir[3], up[3], fov, far; rays: width*height records of 8 floats. */
+void orc_pinhole_rays(const float* cam, int w, int h, float* rays) {
+    orc_v3 pos = {cam[0], cam[1], cam[2]}, dir = {cam[3], cam[4], cam[5]}, up = {cam[6], cam[7], cam[8]};
+    float fov = cam[9], far_t = cam[10];
+    orc_v3 right = v3_normalize(v3_cross(dir, up));
+    float half = fov / 2.0f;
+    float gw = (float)(2.0 * tan((double)half));
+    float gh = gw * ((float)h / (float)w);
+    orc_v3 qw = v3_scale(right, gw / (float)(w - 1));
+    orc_v3 nup = {-up.x, -up.y, -up.z};
+    orc_v3 qh = v3_scale(nup, gh / (float)(h - 1));
+    orc_v3 p00 = v3_add(v3_sub(dir, v3_scale(right, gw / 2.0f)), v3_scale(up, gh / 2.0f));
+    for (int64_t i = 0; i < (int64_t)w * h; ++i) {
+        float x = (float)(int)(i % w), y = (float)(int)(i / w);
+        orc_v3 d = v3_normalize(v3_add(v3_add(p00, v3_scale(qw, x)), v3_scale(qh, y)));
+        float* r = rays + 8 * i;
+        r[0] = pos.x, r[1] = pos.y, r[2] = pos.z, r[3] = ORC_EPS;
+        r[4] = d.x, r[5] = d.y, r[6] = d.z, r[7] = far_t;
+    }
+}
+
+static uint32_t orc_hash_u32(uint32_t x) { /* HashU32, src/util/util.h:24-32 */
+    x ^= x >> 16;
+    x *= 0x7FEB352Du;
+    x ^= x >> 15;
+    x *= 0x846CA68Bu;
+    x ^= x >> 16;
+    return x;
+}
+static float orc_u01_key(uint32_t seed, uint32_t stream, uint64_t idx, uint32_t dim) {
+    uint32_t k = seed * 0x9E3779B1u + stream * 0x85EBCA6Bu + dim * 0xC2B2AE35u;
+    uint32_t lo = (uint32_t)idx, hi = (uint32_t)(idx >> 32);
+    uint32_t hh = orc_hash_u32(k ^ orc_hash_u32(lo ^ orc_hash_u32(hi + dim)));
+    return (float)(hh >> 8) * (1.0f / 16777216.0f); /* U01FromU32, util.h:34-37 */
+}
+static float orc_ray_epsilon(orc_v3 p, float t) { /* RayEpsilon, src/scene/ray.h:15-24 */
+    float ps = fmaxf(fmaxf(fmaxf(fabsf(p.x), fabsf(p.y)), fabsf(p.z)), 1.0f);
+    float ts = fmaxf(t, 1.0f);
+    float bias = fmaxf(1e-6f * ps, 1e-7f * ts);
+    return fminf(fmaxf(bias, 1e-7f), 1e-3f);
+}
+
+/* tris: (N, 3, 3) AoS; rays: n records of 8 floats; prim/t: the hits; out: n bounce rays. */
+void orc_bounce_rays(const float* tris, const float* rays, const int32_t* prim, const float* t, int64_t n,
+                     uint32_t seed, float* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        float* q = out + 8 * i;
+        if (prim[i] < 0) {
+            q[0] = 0.0f, q[1] = 0.0f, q[2] = 0.0f, q[3] = ORC_EPS, q[4] = 0.0f, q[5] = 0.0f, q[6] = 1.0f, q[7] = 0.0f;
+            continue;
+        }
+        const float* r = rays + 8 * i;
+        orc_v3 o = {r[0], r[1], r[2]}, din = {r[4], r[5], r[6]};
+        const float* tri = tris + 9 * (int64_t)prim[i];
+        orc_v3 a = {tri[0], tri[1], tri[2]}, b = {tri[3], tri[4], tri[5]}, c = {tri[6], tri[7], tri[8]};
+        orc_v3 ng = v3_cross(v3_sub(b, a), v3_sub(c, a));
+        if (!(v3_dot(ng, ng) > 0.0f)) {
+            orc_v3 m = {-din.x, -din.y, -din.z};
+            ng = m;
+        } else {
+            ng = v3_normalize(ng);
+            if (v3_dot(ng, din) > 0.0f) {
+                orc_v3 m = {-ng.x, -ng.y, -ng.z};
+                ng = m;
+            }
+        }
+        float dx = 0.0f, dy = 0.0f, r2 = 0.0f;
+        for (int k = 0; k < 16; ++k) {
+            float x = 2.0f * orc_u01_key(seed, 6u, (uint64_t)i, 2u * (uint32_t)k) - 1.0f;
+            float y = 2.0f * orc_u01_key(seed, 6u, (uint64_t)i, 2u * (uint32_t)k + 1u) - 1.0f;
+            float qq = x * x + y * y;
+            if (qq < 1.0f) {
+                dx = x, dy = y, r2 = qq;
+                break;
+            }
+        }
+        float dz = sqrtf(1.0f - r2);
+        orc_v3 helper = {1.0f, 0.0f, 0.0f};
+        if (fabsf(ng.x) > 0.9f) helper.x = 0.0f, helper.y = 1.0f;
+        orc_v3 tx = v3_normalize(v3_cross(helper, ng));
+        orc_v3 ty = v3_cross(ng, tx);
+        orc_v3 d = v3_normalize(v3_add(v3_add(v3_scale(tx, dx), v3_scale(ty, dy)), v3_scale(ng, dz)));
+        orc_v3 pos = v3_add(o, v3_scale(din, t[i]));
+        float eps = orc_ray_epsilon(pos, t[i]);
+        orc_v3 org = v3_add(pos, v3_scale(ng, eps));
+        q[0] = org.x, q[1] = org.y, q[2] = org.z, q[3] = ORC_EPS;
+        q[4] = d.x, q[5] = d.y, q[6] = d.z, q[7] = ORC_INF;
+    }
+}

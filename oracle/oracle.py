@@ -156,6 +156,24 @@ class Oracle:
         L.orc_test_pairs.argtypes = [_f32p, _f32p, C.c_int64, _i32p, C.c_int, C.c_int, _f32p, _f32p, _f32p]
         L.orc_ploc.restype = C.c_int64
         L.orc_ploc.argtypes = [_f32p, C.c_int64, _i32p, C.c_void_p, C.c_int64, C.c_int, _i32p, _f32p, _i32p]
+        L.orc_pinhole_rays.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
+        L.orc_bounce_rays.argtypes = [_f32p, _f32p, _i32p, _f32p, C.c_int64, C.c_uint32, _f32p]
+
+    def pinhole_rays(self, cam_pos, cam_dir, cam_up, fov, far, width, height):
+        """Primary rays of the GPU frontend's pinhole generator, restated (records of 8 floats)."""
+        cam = np.array([*cam_pos, *cam_dir, *cam_up, fov, far], dtype=np.float32)
+        out = np.empty((width * height, 8), np.float32)
+        self.lib.orc_pinhole_rays(cam, int(width), int(height), out)
+        return out
+
+    def bounce_rays(self, tris, rays, prim, t, seed):
+        """Bounce rays of the GPU frontend's generator, restated (one per ray; misses get a null ray)."""
+        tris, rays = _tris(tris), _rays(rays)
+        prim = np.ascontiguousarray(prim, np.int32)
+        t = np.ascontiguousarray(t, np.float32)
+        out = np.empty((len(rays), 8), np.float32)
+        self.lib.orc_bounce_rays(tris, rays, prim, t, len(rays), int(seed) & 0xFFFFFFFF, out)
+        return out
 
     def set_threads(self, n):
         self.lib.orc_set_threads(int(n))
