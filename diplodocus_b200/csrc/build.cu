@@ -84,7 +84,20 @@ __device__ __forceinline__ float3 centroid(const Tri& t) {
                        __fdiv_rn(__fadd_rn(__fadd_rn(t.a.z, t.b.z), t.c.z), 3.0f));
 }
 
+// A triangle with a NaN or infinite coordinate can never be hit: both leaf tests then compute t as NaN
+// (an infinite edge meets a zero reciprocal or a NaN product). Such a triangle gets an empty box (lo = +inf,
+// hi = -inf) and stays out of the scene bounds, so no box above it becomes infinite or NaN.
+__device__ __forceinline__ bool tri_finite(const Tri& t) {
+    return isfinite(t.a.x) && isfinite(t.a.y) && isfinite(t.a.z) && isfinite(t.b.x) && isfinite(t.b.y) &&
+           isfinite(t.b.z) && isfinite(t.c.x) && isfinite(t.c.y) && isfinite(t.c.z);
+}
+
 __device__ __forceinline__ void tri_box(const Tri& t, float3& lo, float3& hi) {
+    if (!tri_finite(t)) {
+        lo = make_float3(__int_as_float(0x7F800000), __int_as_float(0x7F800000), __int_as_float(0x7F800000));
+        hi = make_float3(__int_as_float(0xFF800000), __int_as_float(0xFF800000), __int_as_float(0xFF800000));
+        return;
+    }
     lo = make_float3(fminf(fminf(t.a.x, t.b.x), t.c.x), fminf(fminf(t.a.y, t.b.y), t.c.y),
                      fminf(fminf(t.a.z, t.b.z), t.c.z));
     hi = make_float3(fmaxf(fmaxf(t.a.x, t.b.x), t.c.x), fmaxf(fmaxf(t.a.y, t.b.y), t.c.y),
@@ -147,6 +160,7 @@ __global__ void __launch_bounds__(256) bounds_kernel(const MeshDesc* __restrict_
         }
         any = true;
         Tri t = load_tri(meshes[k], g - meshes[k].first);
+        if (!tri_finite(t)) continue;  // never hit: left out of the bounds
         float3 c = centroid(t), lo, hi;
         tri_box(t, lo, hi);
         acc[0] = fminf(acc[0], c.x), acc[1] = fminf(acc[1], c.y), acc[2] = fminf(acc[2], c.z);

@@ -91,14 +91,21 @@ __global__ void __launch_bounds__(256) kdop_refit_kernel(SobbIn S, const int* __
     float m = 0.0f;
 #pragma unroll
     for (int i = 0; i < kDirs; ++i) k.lo[i] = __int_as_float(0x7F800000), k.hi[i] = __int_as_float(0xFF800000);
-    for (int v = 0; v < 3 * cnt; ++v) {
-        const float4 q = __ldg(t + v);
-        m = fmaxf(m, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
+    for (int tr = 0; tr < cnt; ++tr) {
+        const float4 q0 = __ldg(t + 3 * tr), q1 = __ldg(t + 3 * tr + 1), q2 = __ldg(t + 3 * tr + 2);
+        // a triangle with a non-finite coordinate is never hit: it adds nothing to the k-DOP
+        if (!(isfinite(q0.x) && isfinite(q0.y) && isfinite(q0.z) && isfinite(q1.x) && isfinite(q1.y) &&
+              isfinite(q1.z) && isfinite(q2.x) && isfinite(q2.y) && isfinite(q2.z)))
+            continue;
+        for (int v = 0; v < 3; ++v) {
+            const float4 q = v == 0 ? q0 : (v == 1 ? q1 : q2);
+            m = fmaxf(m, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
 #pragma unroll
-        for (int i = 0; i < kDirs; ++i) {
-            const float d = proj(i, q.x, q.y, q.z);
-            k.lo[i] = fminf(k.lo[i], d);
-            k.hi[i] = fmaxf(k.hi[i], d);
+            for (int i = 0; i < kDirs; ++i) {
+                const float d = proj(i, q.x, q.y, q.z);
+                k.lo[i] = fminf(k.lo[i], d);
+                k.hi[i] = fmaxf(k.hi[i], d);
+            }
         }
     }
     store_kdop(kdop + x, k);

@@ -38,6 +38,13 @@ __device__ __forceinline__ void wbox(const WideIn& W, int id, float3& lo, float3
     if (id < W.N) {
         const float4* t = W.btris + 3 * (long long)W.leaf_start_of[id];
         const float4 a = t[0], b = t[1], c = t[2];
+        if (!(isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(b.x) && isfinite(b.y) && isfinite(b.z) &&
+              isfinite(c.x) && isfinite(c.y) && isfinite(c.z))) {
+            // never hit (NaN t under both leaf tests): an empty box, like the build's cluster boxes
+            lo = make_float3(__int_as_float(0x7F800000), __int_as_float(0x7F800000), __int_as_float(0x7F800000));
+            hi = make_float3(__int_as_float(0xFF800000), __int_as_float(0xFF800000), __int_as_float(0xFF800000));
+            return;
+        }
         lo = make_float3(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z));
         hi = make_float3(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z));
     } else {

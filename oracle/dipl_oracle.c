@@ -304,6 +304,14 @@ static inline void centroid(const float* p, float* c) {
     for (int a = 0; a < 3; ++a) c[a] = ((p[a] + p[3 + a]) + p[6 + a]) / 3.0f;
 }
 
+/* A triangle with a NaN or infinite coordinate can never be hit (both leaf tests give t = NaN): it stays
+ * out of the scene bounds and its cluster box is empty (lo = +inf, hi = -inf), as on the device. */
+static int tri_finite(const float* p) {
+    for (int k = 0; k < 9; ++k)
+        if (!isfinite(p[k])) return 0;
+    return 1;
+}
+
 void orc_scene_bounds(const float* tris, int64_t n, float* cmin, float* cmax, float* bmin, float* bmax) {
     for (int a = 0; a < 3; ++a) {
         cmin[a] = bmin[a] = INFINITY;
@@ -311,6 +319,7 @@ void orc_scene_bounds(const float* tris, int64_t n, float* cmin, float* cmax, fl
     }
     for (int64_t i = 0; i < n; ++i) {
         const float* p = tris + 9 * i;
+        if (!tri_finite(p)) continue;
         float c[3];
         centroid(p, c);
         for (int a = 0; a < 3; ++a) {
@@ -466,9 +475,10 @@ int64_t orc_ploc(const float* tris, int64_t n, const int32_t* perm, const int32_
     int64_t* nn = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
     for (int64_t i = 0; i < n; ++i) {
         const float* p = tris + 9 * (int64_t)perm[i];
+        const int fin = tri_finite(p);
         for (int a = 0; a < 3; ++a) {
-            cur[i].lo[a] = fminf(fminf(p[a], p[3 + a]), p[6 + a]);
-            cur[i].hi[a] = fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]);
+            cur[i].lo[a] = fin ? fminf(fminf(p[a], p[3 + a]), p[6 + a]) : INFINITY;
+            cur[i].hi[a] = fin ? fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]) : -INFINITY;
         }
         cur[i].node = (int32_t)i;
         cur[i].seg = seg ? seg[i] : 0;

@@ -96,6 +96,27 @@ def test_ploc_topology_duplicates_and_emc(orc, kind):
     np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
 
 
+@pytest.mark.parametrize("kind", [A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmc])
+def test_ploc_topology_with_non_finite_triangles(orc, kind):
+    """Triangles with NaN or infinite coordinates (never hittable) get empty boxes and stay out of the scene
+    bounds on the device exactly as in the restatement: same codes, same topology, same boxes."""
+    tris = S.soup(5000, seed=21).copy()
+    rng = np.random.default_rng(3)
+    bad = rng.choice(len(tris), 300, replace=False)
+    for k, i in enumerate(bad):
+        tris[i, rng.integers(3), rng.integers(3)] = [np.nan, np.inf, -np.inf][k % 3]
+    tris[bad[:20]] = np.nan
+    bvh = build(tris, kind)
+    perm, ch, bx = bvh.download_topology()
+    codes = orc.morton30(tris) if kind is A.AccelerationStructureType.kPloc else orc.emc60(tris)
+    exp_perm = O.sort_perm(codes)
+    np.testing.assert_array_equal(perm, exp_perm)
+    ech, ebx, it = orc.ploc(tris, exp_perm, radius=16)
+    np.testing.assert_array_equal(ch, ech)
+    np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
+    assert np.isfinite(ebx[~np.isinf(ebx).all(axis=1)]).all()
+
+
 def test_ploc_topology_1m_displaced_sphere(orc):
     tris = S.uv_sphere(1024, 512, 1.0, (0, 0, 0), displacement=0.05, seed=2)
     bvh = build(tris)
