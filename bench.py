@@ -207,6 +207,18 @@ def measured_traffic(workload, kind, n_tri, n_rays):
     return m[kind]
 
 
+def max_over_ranks(values, world, device=None):
+    """Per-rank device times -> their maximum over all ranks (every rank gets it; identity when world == 1).
+    The job's time is its slowest replica's."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def build_bytes_per_tri(code_type, digit_bits=8, node_bytes_per_tri=None):
     """Algorithmic bytes of one build per triangle (byte model, Morton30: 176 B, EMC60: 308 B)."""
     k = 4 if code_type == 0 else 8
@@ -279,10 +291,7 @@ def run_gpu(args, rank, world, local_rank):
     t_step = float(np.sum(step_ms))
     t_build = float(np.sum(build_ms))
     t_trace = float(np.sum(trace_ms))
-    if world > 1:
-        tt = torch.tensor([t_step, t_build, t_trace], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step, t_build, t_trace = tt.tolist()
+    t_step, t_build, t_trace = max_over_ranks([t_step, t_build, t_trace], world, dev)
 
     # SAH cost and info of one build (outside the timed region)
     h = step()
@@ -357,10 +366,7 @@ def run_gpu(args, rank, world, local_rank):
     e1.record(d2h_s)
     torch.cuda.synchronize()
     t_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = tt.item()
+    (t_e2e,) = max_over_ranks([t_e2e], world, dev)
     h2d = sum(x.numel() * 4 for x in v) + rays.numel() * 4
     d2h = hits.numel() * 4
 
