@@ -160,15 +160,34 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(
     }
     __syncthreads();
 
-    // ---- decoupled look-back per digit ------------------------------------------------------------
+    // ---- publish this tile's digit counts first, so later tiles can sum past it while it scatters ----------
+    constexpr int kDigitsPerThread = (BINS + kSortThreads - 1) / kSortThreads;
     uint32_t* my = lookback + (size_t)tile * BINS;
-    for (int d = threadIdx.x; d < BINS; d += kSortThreads) {
-        uint32_t total = s.dtotal[d];
+    uint32_t tot[kDigitsPerThread];
+#pragma unroll
+    for (int q = 0; q < kDigitsPerThread; ++q) {
+        const int d = (int)threadIdx.x + q * kSortThreads;
+        tot[q] = d < BINS ? s.dtotal[d] : 0u;
+        if (d < BINS) st_release_u32(&my[d], (tile == 0 ? kLbInclusive : kLbAggregate) | tot[q]);
+    }
+    __syncthreads();
+    block_exclusive_scan_smem(s.dtotal, BINS + 1);  // dtotal[d] := local start of digit d in the tile
+
+    // ---- scatter into shared memory in digit order --------------------------------------------------------
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        uint32_t pos = s.dtotal[dig[k]] + s.whist[warp][dig[k]] + rank[k];
+        s.keys[pos] = key[k];
+        s.vals[pos] = val[k];
+    }
+
+    // ---- decoupled look-back per digit (bounded spin), overlapping the other threads' scatter ---------------
+#pragma unroll
+    for (int q = 0; q < kDigitsPerThread; ++q) {
+        const int d = (int)threadIdx.x + q * kSortThreads;
+        if (d >= BINS) break;
         uint32_t prefix = 0;
-        if (tile == 0) {
-            st_release_u32(&my[d], kLbInclusive | total);
-        } else {
-            st_release_u32(&my[d], kLbAggregate | total);
+        if (tile != 0) {
             int64_t j = (int64_t)tile - 1;
             uint32_t spins = 0;
             while (j >= 0) {
@@ -186,23 +205,13 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(
                 if (state == kLbInclusive) break;
                 --j;
             }
-            st_release_u32(&my[d], kLbInclusive | ((prefix + total) & kLbCountMask));
+            st_release_u32(&my[d], kLbInclusive | ((prefix + tot[q]) & kLbCountMask));
         }
-        s.gofs[d] = static_cast<int32_t>(s.gexcl[d] + prefix);
+        s.gofs[d] = static_cast<int32_t>(s.gexcl[d] + prefix) - static_cast<int32_t>(s.dtotal[d]);
     }
-    __syncthreads();
-    block_exclusive_scan_smem(s.dtotal, BINS + 1);  // dtotal[d] := local start of digit d in the tile
-    for (int d = threadIdx.x; d < BINS; d += kSortThreads) s.gofs[d] -= static_cast<int32_t>(s.dtotal[d]);
     __syncthreads();
 
-    // ---- scatter into shared memory in digit order, then out to global ----------------------------
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        uint32_t pos = s.dtotal[dig[k]] + s.whist[warp][dig[k]] + rank[k];
-        s.keys[pos] = key[k];
-        s.vals[pos] = val[k];
-    }
-    __syncthreads();
+    // ---- out to global in digit runs --------------------------------------------------------------------------
     const int valid_count = static_cast<int>(s.dtotal[BINS]);
     for (int i = threadIdx.x; i < valid_count; i += kSortThreads) {
         K k = s.keys[i];
