@@ -43,6 +43,7 @@ struct PlocCtrl {
     uint32_t merges[2];  // internal nodes created before an iteration (by parity)
     uint32_t iterations;
     uint32_t pad;
+    uint32_t tiles_taken[2];  // tiles claimed in an iteration (by parity)
     GridBarrier barrier;
 };
 
@@ -376,6 +377,10 @@ template <typename T>
 __device__ __forceinline__ T by_parity(T const (&a)[2], int parity) {
     return parity ? a[1] : a[0];
 }
+template <typename T>
+__device__ __forceinline__ T& parity_slot(T (&a)[2], int parity) {
+    return parity ? a[1] : a[0];
+}
 
 // Clusters at most this many are finished by the single-CTA tail kernel, resident in shared memory.
 constexpr int kTailMax = 2048;
@@ -561,6 +566,7 @@ struct PlocSmem {
     unsigned long long prefix;
     int ok;
     int n, mbase;
+    uint32_t claim;
 };
 
 template <int B>
@@ -712,7 +718,14 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
         // Nobody reads that array during this iteration.
         const int next_words = (n + B - 1) / B;
         for (int t = blockIdx.x * B + threadIdx.x; t < next_words; t += active * B) by_parity(P.status, parity ^ 1)[t] = 0ull;
-        for (int t = blockIdx.x; t < tiles; t += active) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) parity_slot(P.ctrl->tiles_taken, parity ^ 1) = 0u;
+        // Tiles are claimed in order from a counter: a block that finishes early takes the next tile, and a
+        // tile's look-back predecessors were claimed (and mostly finished) before it.
+        for (;;) {
+            if (threadIdx.x == 0) s.claim = atomicAdd(&parity_slot(P.ctrl->tiles_taken, parity), 1u);
+            __syncthreads();
+            const int t = (int)s.claim;
+            if (t >= tiles) break;
             ploc_tile<B>(P, s, t, tiles, n, mbase, parity, ipt);
             __syncthreads();
         }
