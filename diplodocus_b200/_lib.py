@@ -29,7 +29,8 @@ EXPORTS = [
     "dipl_bvh_trace_closest_counted", "dipl_bvh_trace_any", "dipl_bvh_sah_cost", "dipl_bvh_get_info",
     "dipl_bvh_download_topology", "dipl_bvh_download_layout", "dipl_bvh_check_errors", "dipl_bvh_destroy", "dipl_compute_codes",
     "dipl_radix_sort_pairs", "dipl_radix_sort_pairs_noalloc", "dipl_reintersect_f64", "dipl_trace_adjoint",
-    "dipl_generate_pinhole_rays", "dipl_generate_bounce_rays", "dipl_status_string",
+    "dipl_generate_pinhole_rays", "dipl_generate_bounce_rays", "dipl_selftest_bounded_waits",
+    "dipl_status_string",
     "dipl_last_error", "dipl_abi_version", "dipl_kernel_launch_count",
 ]
 
@@ -98,6 +99,7 @@ def load(path: str = LIB_PATH):
         "dipl_trace_adjoint": (i32, [vp, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]),
         "dipl_generate_pinhole_rays": (i32, [C.POINTER(Camera), i32, i32, vp, vp]),
         "dipl_generate_bounce_rays": (i32, [vp, vp, vp, vp, vp, i64, u32, vp, vp]),
+        "dipl_selftest_bounded_waits": (i32, [u32, vp, vp]),
         "dipl_status_string": (C.c_char_p, [i32]),
         "dipl_last_error": (C.c_char_p, []),
         "dipl_abi_version": (i32, []),

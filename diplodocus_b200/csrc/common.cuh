@@ -109,7 +109,8 @@ struct GridBarrier {
 };
 
 // `expected` = number of blocks taking part (the same value in every participating block).
-__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t expected, uint32_t* err) {
+__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t expected, uint32_t* err,
+                                             uint32_t spin_limit = kSpinLimit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -124,7 +125,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t expected
         } else {
             uint32_t spins = 0;
             while (ld_acquire_u32(&bar->generation) == gen) {
-                if (++spins > kSpinLimit || ld_acquire_u32(err) != 0u) {
+                if (++spins > spin_limit || ld_acquire_u32(err) != 0u) {
                     atomicOr(err, kErrTimeout);
                     ok = 0;
                     break;
@@ -143,7 +144,8 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, uint32_t expected
 // and a value in the low 62 bits; values add without carries between packed fields. Returns the exclusive
 // prefix of `tile`, reading 32 predecessors per round trip. Bounded: on timeout sets *err and *ok = false.
 __device__ __forceinline__ unsigned long long warp_lookback(const unsigned long long* status, long long tile,
-                                                            uint32_t* err, bool* ok) {
+                                                            uint32_t* err, bool* ok,
+                                                            uint32_t spin_limit = kSpinLimit) {
     constexpr unsigned long long kVal = (1ull << 62) - 1ull;
     const int lane = threadIdx.x & 31;
     unsigned long long prefix = 0;
@@ -159,7 +161,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(const unsigned long 
         const int lim = inc ? __ffs(inc) - 1 : 31;
         const uint32_t upto = lim == 31 ? 0xffffffffu : ((2u << lim) - 1u);
         if (zero & upto) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 if (lane == 0) atomicOr(err, kErrTimeout);
                 *ok = false;
                 return 0ull;
@@ -184,7 +186,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(const unsigned long 
 template <int B>
 __device__ __forceinline__ unsigned long long block_lookback(const unsigned long long* status, long long tile,
                                                              uint32_t* err, bool* ok, unsigned long long* wsum,
-                                                             int* wflag) {
+                                                             int* wflag, uint32_t spin_limit = kSpinLimit) {
     constexpr unsigned long long kVal = (1ull << 62) - 1ull;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long prefix = 0;
@@ -226,7 +228,7 @@ __device__ __forceinline__ unsigned long long block_lookback(const unsigned long
         }
         __syncthreads();  // scratch is rewritten by the next round
         if (code == 2) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
                 *ok = false;
                 return 0ull;

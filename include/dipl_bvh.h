@@ -271,6 +271,15 @@ DIPL_API dipl_status dipl_generate_bounce_rays(const float* d_v0, const float* d
                                                const dipl_ray* d_rays, const dipl_hit* d_hits, int64_t n,
                                                uint32_t seed, dipl_ray* d_out, void* stream);
 
+/* No counterpart in the reference. Failure-detection self-test: runs the library's bounded device waits (the
+ * warp and block decoupled look-backs of the sort and the clustering, and the grid barrier between clustering
+ * iterations) on a status word that no tile publishes and on a barrier with one participant that never
+ * arrives, each giving up after spin_limit polls (1..2^20), then launches one more kernel on the same context.
+ * *out_flags gets bit 0/1/2 when the warp look-back / block look-back / grid barrier gave up and bit 3 when
+ * the follow-up kernel ran. Returns DIPL_ERR_TIMEOUT when all four bits are set (the expected outcome),
+ * DIPL_ERR_INTERNAL otherwise. Synchronises `stream`. */
+DIPL_API dipl_status dipl_selftest_bounded_waits(uint32_t spin_limit, uint32_t* out_flags, void* stream);
+
 DIPL_API const char* dipl_status_string(dipl_status status);
 /* Message of the calling thread's most recent failure ("" if none). */
 DIPL_API const char* dipl_last_error(void);
