@@ -83,7 +83,20 @@ class AccelerationStats:
 
 
 @dataclass
+class RaytracingStats:
+    """The reference's RaytracingStats (src/stats/raytracing_stats.h:5-10): seconds and ray counts of a frame.
+    ``trace_frame`` fills it the way CpuRaytracer does (cpu_raytracer.cc:88-147): one primary ray per pixel, one
+    secondary ray per traced bounce."""
+    raytracing_time: float = 0.0
+    primary_ray_count: int = 0
+    secondary_ray_count: int = 0
+    shadow_ray_count: int = 0
+
+
+@dataclass
 class Stats:
+    """The reference's Stats (src/stats/stats.h:8-11)."""
+    rt_stats: RaytracingStats = field(default_factory=RaytracingStats)
     accel_stats: AccelerationStats = field(default_factory=AccelerationStats)
 
 
@@ -366,14 +379,24 @@ def generate_bounce_rays(v, rays: torch.Tensor, hits: Hits, seed: int) -> torch.
     return out
 
 
-def trace_frame(bvh: "GpuPlocBvh", camera: dict, width: int, height: int, seed: int):
+def trace_frame(bvh: "GpuPlocBvh", camera: dict, width: int, height: int, seed: int, stats: "Stats | None" = None):
     """One wavefront frame of the renderer path: primary rays, their closest hits, one bounce ray per hit and
-    the bounce hits, all on the device. Returns (primary rays, primary hits, bounce rays, bounce hits)."""
+    the bounce hits, all on the device. Returns (primary rays, primary hits, bounce rays, bounce hits).
+
+    With ``stats``, adds the frame to its RaytracingStats (time in seconds, synchronised; width * height primary
+    rays; one secondary ray per primary hit, the bounces that carry a ray) and its AccelerationStats queries."""
+    st = stats if stats is not None else Stats()
+    t0 = time.perf_counter()
     rays = generate_pinhole_rays(camera["cam_pos"], camera["cam_dir"], camera["cam_up"], camera["fov"],
                                  camera["far"], width, height)
-    hits = bvh.Intersect(Stats(), rays)
+    hits = bvh.Intersect(st, rays)
     bounce = generate_bounce_rays(bvh._v, rays, hits, seed)
-    bhits = bvh.Intersect(Stats(), bounce)
+    bhits = bvh.Intersect(st, bounce)
+    if stats is not None:
+        secondary = int((hits.prim >= 0).sum().item())  # synchronises the stream
+        stats.rt_stats.raytracing_time += time.perf_counter() - t0
+        stats.rt_stats.primary_ray_count += int(width) * int(height)
+        stats.rt_stats.secondary_ray_count += secondary
     return rays, hits, bounce, bhits
 
 

@@ -2,7 +2,8 @@
 
 ctypes bindings for the two oracles:
 
-* ``RefOracle``  — the reference's own SBvh / brute force / Moller-Trumbore compiled from its
+* ``RefOracle``  — the reference's own SBvh / brute force / Moller-Trumbore / OBJ scene loader / console
+  statistics exporter compiled from its
   sources (oracle/_ref/libref_oracle.so, built by oracle/Makefile in a tree where the reference
   is present; the built file then travels with the repository snapshot).
 * ``Oracle``     — the plain-C restatement in oracle/dipl_oracle.c (oracle/libdipl_oracle.so).
@@ -82,9 +83,70 @@ class RefOracle:
                                       C.c_int]
         L.ref_intersect_one.restype = C.c_float
         L.ref_intersect_one.argtypes = [_f32p, _f32p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.ref_obj_scene_load.restype = C.c_void_p
+        L.ref_obj_scene_load.argtypes = [C.c_char_p, C.c_char_p]
+        L.ref_obj_scene_free.argtypes = [C.c_void_p]
+        L.ref_obj_scene_counts.argtypes = [C.c_void_p, _i64p]
+        L.ref_obj_scene_triangles.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, _i32p, C.c_void_p]
+        L.ref_obj_scene_materials.argtypes = [C.c_void_p, _f32p, C.c_void_p]
+        L.ref_obj_scene_area_lights.argtypes = [C.c_void_p, _i32p, _f32p, _f32p]
+        L.ref_obj_scene_camera_lights.argtypes = [C.c_void_p, _f32p, _f32p]
+        L.ref_console_stats.argtypes = [_f64p, _f64p]
 
     def sbvh(self, tris, max_depth=32, max_triangles_per_leaf=4, bin_count=16):
         return SBvh(self, _tris(tris), max_depth, max_triangles_per_leaf, bin_count)
+
+    def obj_scene(self, dirpath, name):
+        """The reference ObjSceneLoader::Load (obj_scene_loader.cc:189-205) on <dirpath>/<name>.{meta,obj}: a dict
+        of numpy arrays, or None where the reference loader fails."""
+        L = self.lib
+        h = L.ref_obj_scene_load(str(dirpath).encode(), str(name).encode())
+        if not h:
+            return None
+        try:
+            cnt = np.zeros(4, np.int64)
+            L.ref_obj_scene_counts(h, cnt)
+            nt, nm, na, npl = (int(x) for x in cnt)
+            pos = np.zeros((nt, 9), np.float32)
+            nrm = np.zeros((nt, 9), np.float32)
+            geom = np.zeros((nt, 3), np.float32)
+            mat = np.zeros(nt, np.int32)
+            has_n = np.zeros(nt, np.uint8)
+            L.ref_obj_scene_triangles(h, pos, nrm, geom, mat, has_n.ctypes.data_as(C.c_void_p))
+            mvals = np.zeros((nm, 19), np.float32)
+            names = np.zeros((nm, 64), np.uint8)
+            L.ref_obj_scene_materials(h, mvals, names.ctypes.data_as(C.c_void_p))
+            al_id = np.zeros(na, np.int32)
+            al_color = np.zeros((na, 3), np.float32)
+            al_area = np.zeros(na, np.float32)
+            L.ref_obj_scene_area_lights(h, al_id, al_color, al_area)
+            cam = np.zeros(11, np.float32)
+            lights = np.zeros((npl, 7), np.float32)
+            L.ref_obj_scene_camera_lights(h, cam, lights)
+        finally:
+            L.ref_obj_scene_free(h)
+        return {"positions": pos, "normals": nrm, "geom_normals": geom, "material_ids": mat,
+                "has_vertex_normals": has_n.astype(bool), "material_values": mvals,
+                "material_names": [bytes(r).split(b"\0", 1)[0].decode() for r in names],
+                "area_light_triangles": al_id, "area_light_colors": al_color, "area_light_areas": al_area,
+                "camera": cam, "point_lights": lights}
+
+    def console_stats(self, rt, accel):
+        """The reference ConsoleStatsExporter's text for the given values (rt: 4, accel: 8 numbers, the order of
+        RaytracingStats / AccelerationStats), captured from the process's stdout."""
+        import sys
+        import tempfile
+        sys.stdout.flush()
+        with tempfile.TemporaryFile() as tmp:
+            saved = os.dup(1)
+            try:
+                os.dup2(tmp.fileno(), 1)
+                self.lib.ref_console_stats(np.asarray(rt, np.float64), np.asarray(accel, np.float64))
+            finally:
+                os.dup2(saved, 1)
+                os.close(saved)
+            tmp.seek(0)
+            return tmp.read().decode()
 
     def brute(self, tris, rays, backface=False, threads=None):
         tris, rays = _tris(tris), _rays(rays)

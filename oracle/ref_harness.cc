@@ -8,6 +8,9 @@
 //   DummyAccelerationStucture::Intersect src/acceleration/dummy_acceleration_structure.cc:21-64
 //                                      (brute force, ascending id, strict <: lowest-id ties)
 //   Triangle::IntersectRay            src/scene/triangle.cc:10-43       (Moller-Trumbore, eps 1e-6)
+//   ObjSceneLoader::Load              src/io/scene/obj_scene_loader.cc:20-205 (OBJ + MTL through the vendored
+//                                      tinyobjloader, .meta camera and point lights) -> flat arrays
+//   ConsoleStatsExporter::ExportOne   src/io/stats/console_stats_exporter.cc:10-58 (its text on stdout)
 //
 // Input layout: triangles as float[N][3][3] (v0, v1, v2; xyz), rays as float[R][8]
 // (origin xyz, tmin, dir xyz, tmax). The reference Ray has no tmin (it always uses kEpsilon),
@@ -30,6 +33,10 @@
 #undef private
 #include "acceleration/dummy_acceleration_structure.h"
 #include "config/acceleration_structure_config.h"
+#include "config/scene_load_config.h"
+#include "io/scene/obj_scene_loader.h"
+#include "io/stats/console_stats_exporter.h"
+#include "scene/scene.h"
 #include "scene/ray.h"
 #include "scene/ray_hit.h"
 #include "scene/triangle.h"
@@ -206,6 +213,129 @@ float ref_intersect_one(const float* tri9, const float* ray8, int backface, floa
     std::vector<Triangle> tv = MakeTriangles(tri9, 1);
     Ray r = MakeRay(ray8);
     return tv[0].IntersectRay(r, *b1, *b2, backface != 0);
+}
+
+// ---- scene loading: the reference ObjSceneLoader, its Scene exported as flat arrays -----------------------
+struct RefScene {
+    Scene scene;
+};
+
+// NULL when the reference loader fails (missing or malformed .meta / .obj), like its std::nullopt.
+void* ref_obj_scene_load(const char* dirpath, const char* name) {
+    Logger::init(Logger::LogLevel::Error);
+    SceneLoadConfig cfg;
+    cfg.dirpath = dirpath;
+    cfg.name = name;
+    std::optional<Scene> sc = ObjSceneLoader().Load(cfg);
+    if (!sc) return nullptr;
+    auto* h = new RefScene{std::move(*sc)};
+    return h;
+}
+
+void ref_obj_scene_free(void* h) { delete static_cast<RefScene*>(h); }
+
+// counts: triangles, materials, area lights, point lights
+void ref_obj_scene_counts(void* h, int64_t* counts) {
+    const Scene& s = static_cast<RefScene*>(h)->scene;
+    counts[0] = (int64_t)s.Triangles().size();
+    counts[1] = (int64_t)s.Materials().size();
+    counts[2] = (int64_t)s.AreaLights().size();
+    counts[3] = (int64_t)s.PointLights().size();
+}
+
+// pos / normals: 9 floats per triangle (v0, v1, v2); geom: 3 floats
+void ref_obj_scene_triangles(void* h, float* pos, float* normals, float* geom, int32_t* material_ids,
+                             uint8_t* has_normals) {
+    const Scene& s = static_cast<RefScene*>(h)->scene;
+    size_t i = 0;
+    for (const Triangle& t : s.Triangles()) {
+        const Vertex* vs[3] = {&t.v0, &t.v1, &t.v2};
+        for (int k = 0; k < 3; ++k) {
+            pos[9 * i + 3 * k + 0] = vs[k]->pos.x;
+            pos[9 * i + 3 * k + 1] = vs[k]->pos.y;
+            pos[9 * i + 3 * k + 2] = vs[k]->pos.z;
+            normals[9 * i + 3 * k + 0] = t.has_vertex_normals ? vs[k]->normal.x : 0.0f;
+            normals[9 * i + 3 * k + 1] = t.has_vertex_normals ? vs[k]->normal.y : 0.0f;
+            normals[9 * i + 3 * k + 2] = t.has_vertex_normals ? vs[k]->normal.z : 0.0f;
+        }
+        geom[3 * i + 0] = t.geom_normal.x;
+        geom[3 * i + 1] = t.geom_normal.y;
+        geom[3 * i + 2] = t.geom_normal.z;
+        material_ids[i] = t.material_id;
+        has_normals[i] = t.has_vertex_normals ? 1 : 0;
+        ++i;
+    }
+}
+
+// values: 19 floats per material (ambient, diffuse, specular, transmittance, emission, shininess, ior, r_ior,
+// dissolve); names: 64 bytes per material, NUL-terminated (truncated)
+void ref_obj_scene_materials(void* h, float* values, char* names) {
+    const Scene& s = static_cast<RefScene*>(h)->scene;
+    size_t i = 0;
+    for (const Material& m : s.Materials()) {
+        const Vec3* v3[5] = {&m.ambient, &m.diffuse, &m.specular, &m.transmittance, &m.emission};
+        for (int k = 0; k < 5; ++k) {
+            values[19 * i + 3 * k + 0] = v3[k]->x;
+            values[19 * i + 3 * k + 1] = v3[k]->y;
+            values[19 * i + 3 * k + 2] = v3[k]->z;
+        }
+        values[19 * i + 15] = m.shininess;
+        values[19 * i + 16] = m.ior;
+        values[19 * i + 17] = m.r_ior;
+        values[19 * i + 18] = m.dissolve;
+        std::memset(names + 64 * i, 0, 64);
+        std::strncpy(names + 64 * i, m.name.c_str(), 63);
+        ++i;
+    }
+}
+
+// the reference leaves AreaLight::power unset: only id, colour and area are exported
+void ref_obj_scene_area_lights(void* h, int32_t* triangle_ids, float* colors, float* areas) {
+    const Scene& s = static_cast<RefScene*>(h)->scene;
+    size_t i = 0;
+    for (const AreaLight& a : s.AreaLights()) {
+        triangle_ids[i] = a.triangle_id;
+        colors[3 * i + 0] = a.color.x;
+        colors[3 * i + 1] = a.color.y;
+        colors[3 * i + 2] = a.color.z;
+        areas[i] = a.surface_area;
+        ++i;
+    }
+}
+
+// cam: pos, dir, up, fov, far (11 floats); lights: pos, color, power (7 floats each)
+void ref_obj_scene_camera_lights(void* h, float* cam, float* lights) {
+    const Scene& s = static_cast<RefScene*>(h)->scene;
+    const Camera& c = s.GetCamera();
+    const float cv[11] = {c.pos.x, c.pos.y, c.pos.z, c.dir.x, c.dir.y, c.dir.z, c.up.x, c.up.y, c.up.z, c.fov, c.far};
+    std::memcpy(cam, cv, sizeof(cv));
+    size_t i = 0;
+    for (const PointLight& p : s.PointLights()) {
+        const float pv[7] = {p.pos.x, p.pos.y, p.pos.z, p.color.x, p.color.y, p.color.z, p.power};
+        std::memcpy(lights + 7 * i, pv, sizeof(pv));
+        ++i;
+    }
+}
+
+// The reference's console statistics text for the given values (written to stdout; the caller captures it).
+// rt: raytracing_time, primary, secondary, shadow; accel: build_time, node, inner, leaf, memory, query,
+// intersection, traversal (the reference stores the counts as int).
+void ref_console_stats(const double* rt, const double* accel) {
+    Stats s;
+    s.rt_stats.raytracing_time = rt[0];
+    s.rt_stats.primary_ray_count = (int)rt[1];
+    s.rt_stats.secondary_ray_count = (int)rt[2];
+    s.rt_stats.shadow_ray_count = (int)rt[3];
+    s.accel_stats.build_time = accel[0];
+    s.accel_stats.node_count = (int)accel[1];
+    s.accel_stats.inner_node_count = (int)accel[2];
+    s.accel_stats.leaf_node_count = (int)accel[3];
+    s.accel_stats.memory_consumption = (int)accel[4];
+    s.accel_stats.query_count = (int)accel[5];
+    s.accel_stats.intersection_count = (int)accel[6];
+    s.accel_stats.traversal_count = (int)accel[7];
+    ConsoleStatsExporter().ExportOne(StatsExportConfig{}, s);
+    std::cout.flush();
 }
 
 }  // extern "C"

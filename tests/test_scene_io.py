@@ -1,0 +1,163 @@
+"""OBJ scene path and statistics export.
+
+CPU: the host loader (diplodocus_b200/scene_io.py) against the reference ObjSceneLoader's output on the
+hand-written fixture scene (golden vectors from tests/golden/make_obj_golden.py) and, where the reference
+harness is built, against the reference loader directly (fixtures, and the reference's own Cornell scenes when
+its tree is present); the console statistics text against the reference ConsoleStatsExporter; the CSV exporter.
+GPU: a loaded scene built and traced on the device, every primary and bounce hit equal to brute force, and the
+frame's statistics.
+"""
+import io
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN, bits, load_golden
+from diplodocus_b200 import accel as A
+from diplodocus_b200 import scene_io as SI
+from diplodocus_b200 import stats_io as SIO
+
+OBJ_DIR = os.path.join(GOLDEN, "obj")
+
+
+def scene_arrays(sc):
+    mv = np.array([np.concatenate([m.ambient, m.diffuse, m.specular, m.transmittance, m.emission,
+                                   [m.shininess, m.ior, m.r_ior, m.dissolve]]) for m in sc.materials],
+                  np.float32).reshape(-1, 19)
+    return {
+        "positions": sc.positions, "normals": sc.normals, "geom_normals": sc.geom_normals,
+        "material_ids": sc.material_ids, "has_vertex_normals": sc.has_vertex_normals, "material_values": mv,
+        "material_names": [m.name for m in sc.materials],
+        "area_light_triangles": np.array([a.triangle_id for a in sc.area_lights], np.int32),
+        "area_light_colors": np.array([a.color for a in sc.area_lights], np.float32).reshape(-1, 3),
+        "area_light_areas": np.array([a.surface_area for a in sc.area_lights], np.float32),
+        "camera": np.concatenate([sc.camera.pos, sc.camera.dir, sc.camera.up, [sc.camera.fov, sc.camera.far]])
+        .astype(np.float32),
+        "point_lights": np.array([np.concatenate([p.pos, p.color, [p.power]]) for p in sc.point_lights],
+                                 np.float32).reshape(-1, 7),
+    }
+
+
+def assert_same_scene(mine, ref):
+    assert len(mine["positions"]) == len(ref["positions"])
+    for k in ("positions", "normals", "geom_normals", "material_values", "area_light_colors", "area_light_areas",
+              "camera", "point_lights"):
+        np.testing.assert_array_equal(bits(mine[k]), bits(ref[k]), err_msg=k)
+    for k in ("material_ids", "has_vertex_normals", "area_light_triangles"):
+        np.testing.assert_array_equal(mine[k], np.asarray(ref[k]), err_msg=k)
+    assert list(mine["material_names"]) == [str(x) for x in ref["material_names"]]
+
+
+def test_fixture_scene_equals_reference_loader_golden():
+    sc = SI.load_obj_scene(OBJ_DIR, "room")
+    assert sc is not None
+    assert_same_scene(scene_arrays(sc), load_golden("obj_room"))
+    # what the fixture exercises: quads on both diagonals, a convex pentagon, concave hexagon and heptagon,
+    # faces without material (-1), duplicate material names across two MTL files, an emissive pentagon
+    assert len(sc) == 24
+    assert (sc.material_ids == -1).sum() == 2
+    assert [a.triangle_id for a in sc.area_lights] == [12, 13, 14]
+    assert sc.has_vertex_normals.sum() == 8
+
+
+def test_failures_return_none_like_the_reference():
+    assert SI.load_obj_scene(OBJ_DIR, "broken_meta") is None   # unknown metadata token
+    assert SI.load_obj_scene(OBJ_DIR, "missing_obj") is None   # no .obj beside the .meta
+    assert SI.load_obj_scene(OBJ_DIR, "no_such_scene") is None  # no .meta
+
+
+@pytest.mark.parametrize("name", ["room", "broken_meta", "missing_obj"])
+def test_fixtures_equal_reference_loader(ref, name):
+    mine, theirs = SI.load_obj_scene(OBJ_DIR, name), ref.obj_scene(OBJ_DIR, name)
+    assert (mine is None) == (theirs is None)
+    if mine is not None:
+        assert_same_scene(scene_arrays(mine), theirs)
+
+
+@pytest.mark.parametrize("name", ["CornellBox-Original", "CornellBox-Sphere"])
+def test_reference_cornell_scenes_equal_reference_loader(ref, name):
+    import oracle as O
+    res = os.path.join(O.REFERENCE_TREE, "res")
+    if not os.path.exists(os.path.join(res, name + ".obj")):
+        pytest.skip("the reference's scene files are not here")
+    assert_same_scene(scene_arrays(SI.load_obj_scene(res, name)), ref.obj_scene(res, name))
+
+
+def test_number_tokens_read_like_tinyobj():
+    assert SI._num("-0.2200.") == np.float32(-0.22)  # longest decimal prefix
+    assert SI._num("1e") == np.float32(1.0)
+    assert SI._num(".5") == np.float32(0.5)
+    assert np.isinf(SI._num("-inf")) and np.isnan(SI._num("nan"))
+    with pytest.raises(ValueError):
+        SI._num("abc")
+    with pytest.raises(ValueError):
+        SI._num("1e400")
+
+
+def test_quad_split_takes_the_shorter_diagonal():
+    v = np.array([[0, 0, 0], [4, 0, 0], [4, 1, 0], [0, 1, 0]], np.float32)
+    assert SI._triangulate([(i, -1, -1) for i in range(4)], v) in ([(0, 1, 2), (0, 2, 3)], [(0, 1, 3), (1, 2, 3)])
+    w = np.array([[0, 0, 0], [1, 0, 0], [3, 3, 0], [0, 1, 0]], np.float32)  # diagonal 1-3 is the short one
+    assert SI._triangulate([(i, -1, -1) for i in range(4)], w) == [(0, 1, 3), (1, 2, 3)]
+
+
+def test_stats_console_text_equals_reference(ref):
+    cases = [([1.23456, 262144, 100000, 0], [12.5, 1999, 999, 1000, 123456, 362144, 54321, 98765]),
+             ([0, 0, 0, 0], [0, 0, 0, 0, 0, 0, 0, 0]),
+             ([0.000123, 1, 2, 3], [1234.5678, 1, 2, 3, 999, 7, 3, 0])]
+    for rt, ac in cases:
+        s = A.Stats(A.RaytracingStats(rt[0], *map(int, rt[1:])), A.AccelerationStats(ac[0], *map(int, ac[1:])))
+        mine = SIO.ConsoleStatsExporter().text(s).splitlines()
+        theirs = ref.console_stats(rt, ac).splitlines()
+        assert len(mine) == len(theirs)
+        for a, b in zip(mine, theirs):
+            if a.startswith(" Traversals per query:"):
+                # the reference divides the intersection count here; this divides the traversal count
+                q, tcount = int(ac[5]), int(ac[7])
+                want = 0.0 if q == 0 or tcount == 0 else float(np.float32(tcount) / np.float32(q))
+                assert a.split(":")[1].strip() == format(want, ".3g")
+            else:
+                assert a == b
+
+
+def test_stats_csv_round_trip(tmp_path):
+    s1 = A.Stats(A.RaytracingStats(0.5, 10, 4, 0), A.AccelerationStats(1.5, 7, 3, 4, 1024, 14, 9, 33))
+    s2 = A.Stats(A.RaytracingStats(2.0, 1 << 40, 3, 1), A.AccelerationStats(0.25, 1, 0, 1, 64, 5, 1 << 35, 7))
+    cfg = SIO.StatsExportConfig(SIO.parse_stats_export_format("csv"), path=str(tmp_path / "stats.csv"))
+    exp = SIO.CreateStatsExporter(cfg)
+    assert isinstance(exp, SIO.CsvStatsExporter)
+    exp.ExportOne(cfg, s1)
+    exp.ExportOne(cfg, s2)  # appends without a second header
+    text = (tmp_path / "stats.csv").read_text()
+    assert text.splitlines()[0] == ",".join(SIO.CSV_COLUMNS) and text.count("raytracing_time") == 1
+    assert SIO.read_stats_csv(str(tmp_path / "stats.csv")) == [s1, s2]  # 64-bit counts survive
+    buf = io.StringIO()
+    SIO.CsvStatsExporter(buf).ExportAll(cfg, [s1])
+    assert SIO.read_stats_csv(buf.getvalue()) == [s1]
+    with pytest.raises(ValueError):
+        SIO.parse_stats_export_format("json")
+    assert isinstance(SIO.CreateStatsExporter(SIO.StatsExportConfig()), SIO.ConsoleStatsExporter)
+
+
+@pytest.mark.gpu
+def test_obj_scene_frame_hits_equal_brute_force(orc):
+    """file -> device SoA -> PLOC build -> generate -> trace -> bounce -> trace; both hit sets equal brute
+    force on the loaded triangles, and the frame's statistics are filled."""
+    sc = SI.load_obj_scene(OBJ_DIR, "room")
+    stats = A.Stats()
+    bvh, (rays, hits, bounce, bhits) = SI.render_scene_frame(sc, 80, 60, seed=7, stats=stats)
+    tris = sc.triangles()
+    for r, h in ((rays, hits), (bounce, bhits)):
+        want = orc.brute(tris, r.cpu().numpy())
+        np.testing.assert_array_equal(h.prim.cpu().numpy(), want.prim)
+        np.testing.assert_array_equal(bits(h.t.cpu().numpy()), bits(want.t))
+    n_hits = int((hits.prim >= 0).sum().item())
+    assert n_hits > 1000
+    assert stats.rt_stats.primary_ray_count == 80 * 60
+    assert stats.rt_stats.secondary_ray_count == n_hits
+    assert stats.rt_stats.raytracing_time > 0.0
+    assert stats.accel_stats.inner_node_count > 0 and stats.accel_stats.query_count == 2 * 80 * 60
+    text = SIO.ConsoleStatsExporter().text(stats)
+    assert f" Primary ray count:             {80 * 60}" in text
