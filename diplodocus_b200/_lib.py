@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "lib", "libdipl_bvh.so")
 
 DIPL_OK = 0
 STATUS = {0: "DIPL_OK", 1: "DIPL_ERR_INVALID_ARGUMENT", 2: "DIPL_ERR_CUDA", 3: "DIPL_ERR_OUT_OF_MEMORY",
-          4: "DIPL_ERR_TIMEOUT", 5: "DIPL_ERR_INTERNAL", 6: "DIPL_ERR_UNSUPPORTED"}
+          4: "DIPL_ERR_TIMEOUT", 5: "DIPL_ERR_INTERNAL", 6: "DIPL_ERR_UNSUPPORTED", 7: "DIPL_ERR_IO"}
+DIPL_ERR_IO = 7
 
 CODE_MORTON30, CODE_EMC60 = 0, 1
 BV_AABB, BV_SOBB = 0, 1
@@ -30,6 +31,8 @@ EXPORTS = [
     "dipl_bvh_download_topology", "dipl_bvh_download_layout", "dipl_bvh_check_errors", "dipl_bvh_destroy", "dipl_compute_codes",
     "dipl_radix_sort_pairs", "dipl_radix_sort_pairs_noalloc", "dipl_reintersect_f64", "dipl_trace_adjoint",
     "dipl_generate_pinhole_rays", "dipl_generate_bounce_rays", "dipl_selftest_bounded_waits",
+    "dipl_obj_scene_load", "dipl_obj_scene_get_info", "dipl_obj_scene_get_triangles", "dipl_obj_scene_get_soa",
+    "dipl_obj_scene_get_materials", "dipl_obj_scene_get_lights", "dipl_obj_scene_destroy",
     "dipl_status_string",
     "dipl_last_error", "dipl_abi_version", "dipl_kernel_launch_count",
 ]
@@ -48,6 +51,11 @@ class BvhInfo(C.Structure):
                 ("ploc_iterations", C.c_int32), ("code_type", C.c_int32), ("bv_type", C.c_int32),
                 ("layout", C.c_int32), ("max_triangles_per_leaf", C.c_int32), ("nn_search_radius", C.c_int32),
                 ("kdop_size", C.c_int32)]
+
+
+class ObjSceneInfo(C.Structure):
+    _fields_ = [("num_triangles", C.c_int64), ("num_materials", C.c_int64), ("num_area_lights", C.c_int64),
+                ("num_point_lights", C.c_int64), ("camera", C.c_float * 11)]
 
 
 class Camera(C.Structure):
@@ -100,6 +108,13 @@ def load(path: str = LIB_PATH):
         "dipl_generate_pinhole_rays": (i32, [C.POINTER(Camera), i32, i32, vp, vp]),
         "dipl_generate_bounce_rays": (i32, [vp, vp, vp, vp, vp, i64, u32, vp, vp]),
         "dipl_selftest_bounded_waits": (i32, [u32, vp, vp]),
+        "dipl_obj_scene_load": (i32, [C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+        "dipl_obj_scene_get_info": (i32, [vp, C.POINTER(ObjSceneInfo)]),
+        "dipl_obj_scene_get_triangles": (i32, [vp, vp, vp, vp, vp, vp]),
+        "dipl_obj_scene_get_soa": (i32, [vp, vp, vp, vp]),
+        "dipl_obj_scene_get_materials": (i32, [vp, vp, vp]),
+        "dipl_obj_scene_get_lights": (i32, [vp, vp, vp, vp, vp]),
+        "dipl_obj_scene_destroy": (None, [vp]),
         "dipl_status_string": (C.c_char_p, [i32]),
         "dipl_last_error": (C.c_char_p, []),
         "dipl_abi_version": (i32, []),

@@ -113,6 +113,7 @@ const char* dipl_status_string(dipl_status s) {
         case DIPL_ERR_TIMEOUT: return "DIPL_ERR_TIMEOUT";
         case DIPL_ERR_INTERNAL: return "DIPL_ERR_INTERNAL";
         case DIPL_ERR_UNSUPPORTED: return "DIPL_ERR_UNSUPPORTED";
+        case DIPL_ERR_IO: return "DIPL_ERR_IO";
     }
     return "DIPL_ERR_UNKNOWN";
 }

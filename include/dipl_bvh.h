@@ -45,7 +45,8 @@ typedef enum dipl_status {
     DIPL_ERR_OUT_OF_MEMORY = 3,    /* a device allocation failed */
     DIPL_ERR_TIMEOUT = 4,          /* a bounded device-side wait (look-back, grid barrier) gave up */
     DIPL_ERR_INTERNAL = 5,         /* a device-side consistency check failed (e.g. traversal stack) */
-    DIPL_ERR_UNSUPPORTED = 6       /* a valid option this build does not provide */
+    DIPL_ERR_UNSUPPORTED = 6,      /* a valid option this build does not provide */
+    DIPL_ERR_IO = 7                /* a scene file could not be read or parsed */
 } dipl_status;
 
 /* Code used to order primitives before clustering.
@@ -279,6 +280,43 @@ DIPL_API dipl_status dipl_generate_bounce_rays(const float* d_v0, const float* d
  * the follow-up kernel ran. Returns DIPL_ERR_TIMEOUT when all four bits are set (the expected outcome),
  * DIPL_ERR_INTERNAL otherwise. Synchronises `stream`. */
 DIPL_API dipl_status dipl_selftest_bounded_waits(uint32_t spin_limit, uint32_t* out_flags, void* stream);
+
+/* ---- OBJ scenes: the reference's scene files into the engine (host side) --------------------------------- */
+
+/* A loaded scene: triangles in file order with the reference Scene's float bits, materials, lights, camera. */
+typedef struct dipl_obj_scene dipl_obj_scene;
+
+typedef struct dipl_obj_scene_info {
+    int64_t num_triangles;
+    int64_t num_materials;
+    int64_t num_area_lights;
+    int64_t num_point_lights;
+    float camera[11]; /* pos[3], dir[3], up[3], fov, far (the .meta camera) */
+} dipl_obj_scene_info;
+
+/* Replaces ObjSceneLoader::Load (src/io/scene/obj_scene_loader.cc:189-205): reads <dirpath>/<name>.meta
+ * (camera, point lights; LoadMetadata, :120-187) then <name>.obj and the MTL files it names (LoadObj, :20-118,
+ * with its vendored tinyobjloader's quad split, ear clipping and index rules). DIPL_ERR_IO (message in
+ * dipl_last_error) where the reference returns std::nullopt; also when a vertex or normal index is out of
+ * range. Host only: no device is needed. Free with dipl_obj_scene_destroy. */
+DIPL_API dipl_status dipl_obj_scene_load(const char* dirpath, const char* name, dipl_obj_scene** out);
+DIPL_API dipl_status dipl_obj_scene_get_info(const dipl_obj_scene* scene, dipl_obj_scene_info* info);
+/* Host copies (any pointer may be NULL): positions and normals 9 floats per triangle (v0, v1, v2; normals 0
+ * where the triangle has none), geometric normals 3 floats (Normalize(Cross(v1 - v0, v2 - v0)), scene.cc:18-21),
+ * material ids (-1 = none), has_vertex_normals 1 byte per triangle. */
+DIPL_API dipl_status dipl_obj_scene_get_triangles(const dipl_obj_scene* scene, float* positions, float* normals,
+                                                  float* geom_normals, int32_t* material_ids,
+                                                  uint8_t* has_vertex_normals);
+/* The three vertex arrays (float3 each, host memory) in the SoA layout dipl_build_desc takes after upload. */
+DIPL_API dipl_status dipl_obj_scene_get_soa(const dipl_obj_scene* scene, float* v0, float* v1, float* v2);
+/* values: 19 floats per material (ambient, diffuse, specular, transmittance, emission, shininess, ior, r_ior,
+ * dissolve: src/scene/material.h); names: 64 bytes per material, NUL-terminated. Either may be NULL. */
+DIPL_API dipl_status dipl_obj_scene_get_materials(const dipl_obj_scene* scene, float* values, char* names);
+/* Area lights (one per emissive triangle: triangle id, emission colour (3 floats), surface area) and point
+ * lights (7 floats each: pos, color, power). Any pointer may be NULL. */
+DIPL_API dipl_status dipl_obj_scene_get_lights(const dipl_obj_scene* scene, int32_t* area_triangle_ids,
+                                               float* area_colors, float* area_surface_areas, float* point_lights);
+DIPL_API void dipl_obj_scene_destroy(dipl_obj_scene* scene);
 
 DIPL_API const char* dipl_status_string(dipl_status status);
 /* Message of the calling thread's most recent failure ("" if none). */

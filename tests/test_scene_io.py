@@ -1,6 +1,6 @@
 """OBJ scene path and statistics export.
 
-CPU: the host loader (diplodocus_b200/scene_io.py) against the reference ObjSceneLoader's output on the
+CPU: the library's host-side loader (dipl_obj_scene_load, through diplodocus_b200/scene_io.py) against the reference ObjSceneLoader's output on the
 hand-written fixture scene (golden vectors from tests/golden/make_obj_golden.py) and, where the reference
 harness is built, against the reference loader directly (fixtures, and the reference's own Cornell scenes when
 its tree is present); the console statistics text against the reference ConsoleStatsExporter; the CSV exporter.
@@ -85,22 +85,57 @@ def test_reference_cornell_scenes_equal_reference_loader(ref, name):
     assert_same_scene(scene_arrays(SI.load_obj_scene(res, name)), ref.obj_scene(res, name))
 
 
-def test_number_tokens_read_like_tinyobj():
-    assert SI._num("-0.2200.") == np.float32(-0.22)  # longest decimal prefix
-    assert SI._num("1e") == np.float32(1.0)
-    assert SI._num(".5") == np.float32(0.5)
-    assert np.isinf(SI._num("-inf")) and np.isnan(SI._num("nan"))
-    with pytest.raises(ValueError):
-        SI._num("abc")
-    with pytest.raises(ValueError):
-        SI._num("1e400")
+def write_scene(tmp_path, name, obj, meta="cam_pos 0 0 0\n", mtl=None):
+    (tmp_path / f"{name}.meta").write_text(meta)
+    (tmp_path / f"{name}.obj").write_text(obj)
+    if mtl is not None:
+        (tmp_path / f"{name}.mtl").write_text(mtl)
+    return str(tmp_path)
 
 
-def test_quad_split_takes_the_shorter_diagonal():
-    v = np.array([[0, 0, 0], [4, 0, 0], [4, 1, 0], [0, 1, 0]], np.float32)
-    assert SI._triangulate([(i, -1, -1) for i in range(4)], v) in ([(0, 1, 2), (0, 2, 3)], [(0, 1, 3), (1, 2, 3)])
-    w = np.array([[0, 0, 0], [1, 0, 0], [3, 3, 0], [0, 1, 0]], np.float32)  # diagonal 1-3 is the short one
-    assert SI._triangulate([(i, -1, -1) for i in range(4)], w) == [(0, 1, 3), (1, 2, 3)]
+def test_number_tokens_read_like_tinyobj(tmp_path):
+    # the longest decimal prefix of a token (the reference's CornellBox-Sphere.obj has "-0.2200."), nan / inf
+    d = write_scene(tmp_path, "nums", "v 1e -0.2200. .5\nv -inf 2 3\nv 0 0 0\nf 1 2 3\n")
+    sc = SI.load_obj_scene(d, "nums")
+    p = sc.positions[0]
+    assert p[0] == np.float32(1.0) and p[1] == np.float32(-0.22) and p[2] == np.float32(0.5)
+    assert np.isneginf(p[3])
+    assert SI.load_obj_scene(write_scene(tmp_path, "bad", "v abc 0 0\nv 0 0 0\nv 1 1 1\nf 1 2 3\n"), "bad") is None
+    assert SI.load_obj_scene(write_scene(tmp_path, "big", "v 1e400 0 0\nv 0 0 0\nv 1 1 1\nf 1 2 3\n"), "big") is None
+    assert SI.load_obj_scene(write_scene(tmp_path, "zero", "v 0 0 0\nv 1 0 0\nv 1 1 1\nf 0 1 2\n"), "zero") is None
+    assert SI.load_obj_scene(write_scene(tmp_path, "oob", "v 0 0 0\nv 1 0 0\nf 1 2 9\n"), "oob") is None
+    assert SI.load_obj_scene(write_scene(tmp_path, "m", "v 0 0 0\nv 1 0 0\nv 1 1 0\nf 1 2 3\n",
+                                         meta="cam_fov 0.5x\n"), "m") is None
+    import oracle as O
+    if os.path.exists(O.REF_LIB):
+        r = O.RefOracle()
+        assert_same_scene(scene_arrays(sc), r.obj_scene(d, "nums"))
+        for name in ("bad", "big", "zero"):
+            assert r.obj_scene(str(tmp_path), name) is None
+
+
+def test_quad_split_takes_the_shorter_diagonal(tmp_path):
+    obj = ("v 0 0 0\nv 4 0 0\nv 4 1 0\nv 0 1 0\nf 1 2 3 4\n"   # diagonals equal: 0-1-3 / 1-2-3
+           "v 0 0 1\nv 1 0 1\nv 3 3 1\nv 0 1 1\nf 5 6 7 8\n"   # 6-8 is the short one
+           "v 0 0 2\nv 3 0 2\nv 1 1 2\nv 0 3 2\nf 9 10 11 12\n")  # 9-11 is the short one
+    sc = SI.load_obj_scene(write_scene(tmp_path, "q", obj), "q")
+    tri = sc.triangles()
+    assert len(sc) == 6
+    np.testing.assert_array_equal(tri[2], [[0, 0, 1], [1, 0, 1], [0, 1, 1]])
+    np.testing.assert_array_equal(tri[3], [[1, 0, 1], [3, 3, 1], [0, 1, 1]])
+    np.testing.assert_array_equal(tri[4], [[0, 0, 2], [3, 0, 2], [1, 1, 2]])
+    np.testing.assert_array_equal(tri[5], [[0, 0, 2], [1, 1, 2], [0, 3, 2]])
+
+
+def test_loader_needs_no_device_and_checks_arguments():
+    import ctypes as C
+    from diplodocus_b200 import _lib as L
+    lib = L.load()
+    h = C.c_void_p(0)
+    assert lib.dipl_obj_scene_load(None, b"x", C.byref(h)) == 1
+    assert lib.dipl_obj_scene_load(OBJ_DIR.encode(), b"no_such_scene", C.byref(h)) == L.DIPL_ERR_IO
+    assert b"cannot read" in lib.dipl_last_error()
+    assert lib.dipl_status_string(L.DIPL_ERR_IO) == b"DIPL_ERR_IO"
 
 
 def test_stats_console_text_equals_reference(ref):
