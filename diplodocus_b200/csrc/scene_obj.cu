@@ -29,7 +29,9 @@
 #include <set>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
+#include <algorithm>
 
 #include "internal.h"
 
@@ -113,6 +115,66 @@ float obj_number(const std::string& tok) {
     return static_cast<float>(d);
 }
 
+// The same reading for a token [s, e) of a file buffer, without copies: Clinger's exact fast path (a mantissa of
+// at most 2^53 times or over an exactly representable power of ten is one correctly rounded operation), else
+// the general path above.
+constexpr double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                               1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+bool fast_number(const char* s, const char* e, float* out) {
+    const char* p = s;
+    bool neg = false;
+    if (p < e && (*p == '+' || *p == '-')) neg = *p++ == '-';
+    uint64_t mant = 0;
+    int sig = 0, exp10 = 0;
+    bool digits = false;
+    while (p < e && *p >= '0' && *p <= '9') {
+        digits = true;
+        if (mant || *p != '0') {
+            if (++sig > 19) return false;
+            mant = mant * 10 + (uint64_t)(*p - '0');
+        }
+        ++p;
+    }
+    if (p < e && *p == '.') {
+        ++p;
+        while (p < e && *p >= '0' && *p <= '9') {
+            digits = true;
+            if (mant || *p != '0') {
+                if (++sig > 19) return false;
+                mant = mant * 10 + (uint64_t)(*p - '0');
+            }
+            --exp10;
+            ++p;
+        }
+    }
+    if (!digits) return false;
+    if (p < e && (*p == 'e' || *p == 'E')) {
+        const char* q = p + 1;
+        bool eneg = false;
+        if (q < e && (*q == '+' || *q == '-')) eneg = *q++ == '-';
+        if (q < e && *q >= '0' && *q <= '9') {
+            int x = 0;
+            while (q < e && *q >= '0' && *q <= '9') {
+                if (x < 100000) x = x * 10 + (*q - '0');
+                ++q;
+            }
+            exp10 += eneg ? -x : x;
+        }
+    }
+    if (mant > (1ull << 53) || exp10 < -22 || exp10 > 22) return false;
+    double d = (double)mant;
+    d = exp10 >= 0 ? d * kPow10[exp10] : d / kPow10[-exp10];
+    *out = static_cast<float>(neg ? -d : d);
+    return true;
+}
+
+float number(const char* s, const char* e) {
+    float f;
+    if (fast_number(s, e, &f)) return f;
+    return obj_number(std::string(s, e));
+}
+
 // A .meta value: exactly one decimal token.
 float meta_number(const std::string& tok) {
     const char* s = tok.c_str();
@@ -161,9 +223,7 @@ bool pnpoly3(const float* vx, const float* vy, float tx, float ty) {
 }
 
 // Triangles (corner positions within the face) of one polygon, given the vertex positions read so far.
-void triangulate(const std::vector<Corner>& face, const std::vector<float>& v, std::vector<int>& out) {
-    const int n = (int)face.size();
-    const long nv = (long)(v.size() / 3);
+void triangulate(const Corner* face, int n, const float* v, long nv, std::vector<int>& out) {
     auto ok = [&](int k) { return face[k].v >= 0 && face[k].v < nv; };
     auto P = [&](int k) { return V3{v[3 * face[k].v], v[3 * face[k].v + 1], v[3 * face[k].v + 2]}; };
     if (n < 3) return;  // degenerate face: skipped
@@ -327,28 +387,172 @@ bool load_mtl(const std::string& path, std::vector<dipl_obj_scene::Mat>& mats, s
     return true;
 }
 
-// ---- OBJ -----------------------------------------------------------------------------------------------------
-int fix_index(const std::string& tok, long count) {
-    char* end = nullptr;
-    const long i = std::strtol(tok.c_str(), &end, 10);
-    if (end == tok.c_str()) fail("bad index '" + tok + "'");
-    if (i > 0) return (int)(i - 1);
-    if (i < 0) return (int)(count + i);
-    fail("zero index");
+// ---- OBJ: chunks of lines parsed in parallel, then merged in file order -------------------------------------
+struct FaceRec {
+    uint32_t first, count;        // corners [first, first + count) of the chunk's corner array
+    uint32_t nv, nvt, nvn;        // vertices / texcoords / normals of the chunk before this line
+};
+struct EventRec {
+    size_t order;                 // faces of the chunk before this event
+    uint32_t nv;                  // vertices of the chunk before this event
+    std::vector<std::string> tok; // the line's tokens
+};
+struct Chunk {
+    std::vector<float> v, vn;
+    uint32_t nvt = 0;
+    std::vector<int64_t> corners;  // raw v, vt, vn indices per corner (0 = absent)
+    std::vector<FaceRec> faces;
+    std::vector<EventRec> events;
+    std::string error;
+};
+
+const char* skip_ws(const char* p, const char* e) {
+    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f')) ++p;
+    return p;
+}
+const char* token_end(const char* p, const char* e) {
+    while (p < e && !(*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f')) ++p;
+    return p;
+}
+
+int64_t parse_int(const char* s, const char* e) {
+    const char* p = s;
+    bool neg = false;
+    if (p < e && (*p == '+' || *p == '-')) neg = *p++ == '-';
+    if (p >= e || *p < '0' || *p > '9') fail("bad index '" + std::string(s, e) + "'");
+    int64_t x = 0;
+    while (p < e && *p >= '0' && *p <= '9') {
+        if (x < (int64_t)1 << 40) x = x * 10 + (*p - '0');
+        ++p;
+    }
+    if (x == 0) fail("zero index");
+    return neg ? -x : x;
+}
+
+void parse_chunk(const char* b, const char* e, Chunk& c) {
+    try {
+        while (b < e) {
+            const char* nl = static_cast<const char*>(std::memchr(b, '\n', (size_t)(e - b)));
+            const char* le = nl ? nl : e;
+            const char* hash = static_cast<const char*>(std::memchr(b, '#', (size_t)(le - b)));
+            const char* end = hash ? hash : le;
+            const char* p = skip_ws(b, end);
+            b = nl ? nl + 1 : e;
+            if (p >= end) continue;
+            const char* ke = token_end(p, end);
+            const size_t kl = (size_t)(ke - p);
+            if (kl == 1 && *p == 'v') {
+                const char* q = ke;
+                for (int i = 0; i < 3; ++i) {
+                    q = skip_ws(q, end);
+                    const char* te = token_end(q, end);
+                    c.v.push_back(q < te ? number(q, te) : 0.0f);
+                    q = te;
+                }
+            } else if (kl == 2 && p[0] == 'v' && p[1] == 'n') {
+                const char* q = ke;
+                for (int i = 0; i < 3; ++i) {
+                    q = skip_ws(q, end);
+                    const char* te = token_end(q, end);
+                    c.vn.push_back(q < te ? number(q, te) : 0.0f);
+                    q = te;
+                }
+            } else if (kl == 2 && p[0] == 'v' && p[1] == 't') {
+                ++c.nvt;
+            } else if (kl == 1 && *p == 'f') {
+                FaceRec f{(uint32_t)(c.corners.size() / 3), 0, (uint32_t)(c.v.size() / 3), c.nvt,
+                          (uint32_t)(c.vn.size() / 3)};
+                const char* q = skip_ws(ke, end);
+                while (q < end) {
+                    const char* te = token_end(q, end);
+                    const char* s1 = static_cast<const char*>(std::memchr(q, '/', (size_t)(te - q)));
+                    int64_t vi = parse_int(q, s1 ? s1 : te), ti = 0, ni = 0;
+                    if (s1) {
+                        const char* s2 = static_cast<const char*>(std::memchr(s1 + 1, '/', (size_t)(te - s1 - 1)));
+                        const char* t_end = s2 ? s2 : te;
+                        if (t_end > s1 + 1) ti = parse_int(s1 + 1, t_end);
+                        if (s2 && s2 + 1 < te) ni = parse_int(s2 + 1, te);
+                    }
+                    c.corners.insert(c.corners.end(), {vi, ti, ni});
+                    ++f.count;
+                    q = skip_ws(te, end);
+                }
+                c.faces.push_back(f);
+            } else if ((kl == 6 && (std::memcmp(p, "usemtl", 6) == 0 || std::memcmp(p, "mtllib", 6) == 0)) ||
+                       (kl == 1 && (*p == 'g' || *p == 'o'))) {
+                EventRec ev{c.faces.size(), (uint32_t)(c.v.size() / 3), split(std::string(p, end))};
+                c.events.push_back(std::move(ev));
+            }
+        }
+    } catch (const LoadError& err) {
+        c.error = err.msg;
+    }
+}
+
+int resolve(int64_t raw, int64_t count) {
+    if (raw > 0) return (int)(raw - 1);
+    if (raw < 0) return (int)(count + raw);
+    return -1;  // absent
 }
 
 void load_obj(const std::string& path, dipl_obj_scene& sc) {
-    std::ifstream in(path);
-    if (!in) fail("cannot read " + path);
+    std::FILE* fp = std::fopen(path.c_str(), "rb");
+    if (!fp) fail("cannot read " + path);
+    std::string buf;
+    std::fseek(fp, 0, SEEK_END);
+    const long size = std::ftell(fp);
+    std::fseek(fp, 0, SEEK_SET);
+    buf.resize(size > 0 ? (size_t)size : 0);
+    const size_t got = buf.empty() ? 0 : std::fread(&buf[0], 1, buf.size(), fp);
+    std::fclose(fp);
+    if (got != buf.size()) fail("cannot read " + path);
     const size_t slash = path.find_last_of('/');
     const std::string base = slash == std::string::npos ? std::string(".") : path.substr(0, slash);
+
+    // chunks at line starts; one per hardware thread, at least 4 MB each
+    const size_t want = std::max<size_t>(1, std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()),
+                                                                buf.size() / (4u << 20) + 1));
+    std::vector<size_t> cut{0};
+    for (size_t k = 1; k < want; ++k) {
+        size_t at = buf.size() * k / want;
+        const void* nl = std::memchr(buf.data() + at, '\n', buf.size() - at);
+        at = nl ? (size_t)(static_cast<const char*>(nl) - buf.data()) + 1 : buf.size();
+        if (at > cut.back()) cut.push_back(at);
+    }
+    cut.push_back(buf.size());
+    const size_t nc = cut.size() - 1;
+    std::vector<Chunk> chunks(nc);
+    {
+        std::vector<std::thread> th;
+        for (size_t k = 1; k < nc; ++k)
+            th.emplace_back(parse_chunk, buf.data() + cut[k], buf.data() + cut[k + 1], std::ref(chunks[k]));
+        parse_chunk(buf.data() + cut[0], buf.data() + cut[1], chunks[0]);
+        for (auto& t : th) t.join();
+    }
+    for (const Chunk& c : chunks)
+        if (!c.error.empty()) fail(c.error);
+
+    // all positions and normals, in file order
     std::vector<float> v, vn;
-    long nvt = 0;
+    std::vector<uint32_t> v0(nc), vt0(nc), vn0(nc);
+    uint32_t tv = 0, tvt = 0, tvn = 0;
+    for (size_t k = 0; k < nc; ++k) {
+        v0[k] = tv, vt0[k] = tvt, vn0[k] = tvn;
+        tv += (uint32_t)(chunks[k].v.size() / 3), tvt += chunks[k].nvt, tvn += (uint32_t)(chunks[k].vn.size() / 3);
+    }
+    v.reserve(3 * (size_t)tv);
+    vn.reserve(3 * (size_t)tvn);
+    for (const Chunk& c : chunks) {
+        v.insert(v.end(), c.v.begin(), c.v.end());
+        vn.insert(vn.end(), c.vn.begin(), c.vn.end());
+    }
+
+    // faces and events in file order: materials, flush points, triangulation
     std::map<std::string, int> material_map;
     std::set<std::string> loaded;
     int material = -1;
     struct Pending {
-        std::vector<Corner> face;
+        size_t chunk, face;
         int mat;
     };
     std::vector<Pending> pending;
@@ -358,69 +562,58 @@ void load_obj(const std::string& path, dipl_obj_scene& sc) {
     };
     std::vector<OutTri> tris;
     std::vector<int> idx;
-    auto flush = [&]() {
-        for (const Pending& p : pending) {
+    std::vector<Corner> face;
+    auto flush = [&](long nv_now) {
+        for (const Pending& pf : pending) {
+            const Chunk& c = chunks[pf.chunk];
+            const FaceRec& f = c.faces[pf.face];
+            face.clear();
+            for (uint32_t j = 0; j < f.count; ++j) {
+                const int64_t* r = &c.corners[3 * ((size_t)f.first + j)];
+                face.push_back({resolve(r[0], (int64_t)v0[pf.chunk] + f.nv),
+                                resolve(r[1], (int64_t)vt0[pf.chunk] + f.nvt),
+                                resolve(r[2], (int64_t)vn0[pf.chunk] + f.nvn)});
+            }
             idx.clear();
-            triangulate(p.face, v, idx);
+            triangulate(face.data(), (int)face.size(), v.data(), nv_now, idx);
             for (size_t k = 0; k + 2 < idx.size(); k += 3)
-                tris.push_back({{p.face[idx[k]], p.face[idx[k + 1]], p.face[idx[k + 2]]}, p.mat});
+                tris.push_back({{face[idx[k]], face[idx[k + 1]], face[idx[k + 2]]}, pf.mat});
         }
         pending.clear();
     };
-    std::string line;
-    while (std::getline(in, line)) {
-        const size_t hash = line.find('#');
-        if (hash != std::string::npos) line.resize(hash);
-        const std::vector<std::string> t = split(line);
-        if (t.empty()) continue;
-        const std::string& k = t[0];
-        if (k == "v" || k == "vn") {
-            std::vector<float>& dst = k == "v" ? v : vn;
-            // missing components read as 0; a w or colour components do not reach the Scene
-            for (int i = 0; i < 3; ++i) dst.push_back((size_t)(i + 1) < t.size() ? obj_number(t[i + 1]) : 0.0f);
-        } else if (k == "vt") {
-            ++nvt;
-        } else if (k == "f") {
-            Pending p;
-            p.mat = material;
-            for (size_t i = 1; i < t.size(); ++i) {
-                const std::string& c = t[i];
-                const size_t s1 = c.find('/');
-                Corner cr{-1, -1, -1};
-                cr.v = fix_index(c.substr(0, s1), (long)(v.size() / 3));
-                if (s1 != std::string::npos) {
-                    const size_t s2 = c.find('/', s1 + 1);
-                    const std::string vt = c.substr(s1 + 1, s2 == std::string::npos ? std::string::npos : s2 - s1 - 1);
-                    if (!vt.empty()) cr.vt = fix_index(vt, nvt);
-                    if (s2 != std::string::npos && s2 + 1 < c.size())
-                        cr.vn = fix_index(c.substr(s2 + 1), (long)(vn.size() / 3));
+    for (size_t k = 0; k < nc; ++k) {
+        const Chunk& c = chunks[k];
+        size_t fi = 0;
+        for (const EventRec& ev : c.events) {
+            for (; fi < ev.order; ++fi) pending.push_back({k, fi, material});
+            const long nv_now = (long)v0[k] + ev.nv;
+            const std::string& key = ev.tok[0];
+            if (key == "usemtl") {
+                const std::string name = ev.tok.size() > 1 ? ev.tok[1] : "";
+                auto it = material_map.find(name);
+                const int id = it == material_map.end() ? -1 : it->second;
+                if (id != material) {
+                    flush(nv_now);
+                    material = id;
                 }
-                p.face.push_back(cr);
-            }
-            pending.push_back(std::move(p));
-        } else if (k == "usemtl") {
-            const std::string name = t.size() > 1 ? t[1] : "";
-            auto it = material_map.find(name);
-            const int id = it == material_map.end() ? -1 : it->second;
-            if (id != material) {
-                flush();
-                material = id;
-            }
-        } else if (k == "mtllib") {
-            for (size_t i = 1; i < t.size(); ++i) {
-                if (loaded.count(t[i])) continue;
-                if (load_mtl(base + "/" + t[i], sc.materials, material_map)) {
-                    loaded.insert(t[i]);
-                    break;
+            } else if (key == "mtllib") {
+                for (size_t i = 1; i < ev.tok.size(); ++i) {
+                    if (loaded.count(ev.tok[i])) continue;
+                    if (load_mtl(base + "/" + ev.tok[i], sc.materials, material_map)) {
+                        loaded.insert(ev.tok[i]);
+                        break;
+                    }
                 }
+            } else {
+                flush(nv_now);  // g, o
             }
-        } else if (k == "g" || k == "o") {
-            flush();
         }
+        for (; fi < c.faces.size(); ++fi) pending.push_back({k, fi, material});
     }
-    flush();
+    flush((long)tv);
+    chunks.clear();
 
-    const long nv = (long)(v.size() / 3), nn = (long)(vn.size() / 3);
+    const long nv = (long)tv, nn = (long)tvn;
     const size_t n = tris.size();
     sc.positions.assign(9 * n, 0.0f);
     sc.normals.assign(9 * n, 0.0f);
@@ -433,7 +626,7 @@ void load_obj(const std::string& path, dipl_obj_scene& sc) {
         for (int k = 0; k < 3; ++k) {
             const int vi = tr.c[k].v;
             if (vi < 0 || vi >= nv) fail("vertex index out of range");
-            p[k] = {v[3 * vi], v[3 * vi + 1], v[3 * vi + 2]};
+            p[k] = {v[3 * (size_t)vi], v[3 * (size_t)vi + 1], v[3 * (size_t)vi + 2]};
             sc.positions[9 * i + 3 * k + 0] = p[k].x;
             sc.positions[9 * i + 3 * k + 1] = p[k].y;
             sc.positions[9 * i + 3 * k + 2] = p[k].z;
@@ -442,7 +635,7 @@ void load_obj(const std::string& path, dipl_obj_scene& sc) {
             for (int k = 0; k < 3; ++k) {
                 const int ni = tr.c[k].vn;
                 if (ni >= nn) fail("normal index out of range");
-                for (int j = 0; j < 3; ++j) sc.normals[9 * i + 3 * k + j] = vn[3 * ni + j];
+                for (int j = 0; j < 3; ++j) sc.normals[9 * i + 3 * k + j] = vn[3 * (size_t)ni + j];
             }
             sc.has_normals[i] = 1;
         }
@@ -452,10 +645,10 @@ void load_obj(const std::string& path, dipl_obj_scene& sc) {
         sc.geom[3 * i + 2] = g.z;
         sc.material_ids[i] = tr.mat;
         if (tr.mat >= 0) {
-            const float* e = &sc.materials[tr.mat].v[12];
-            if (e[0] != 0.0f || e[1] != 0.0f || e[2] != 0.0f) {
+            const float* em = &sc.materials[tr.mat].v[12];
+            if (em[0] != 0.0f || em[1] != 0.0f || em[2] != 0.0f) {
                 sc.area_ids.push_back((int32_t)i);
-                sc.area_colors.insert(sc.area_colors.end(), {e[0], e[1], e[2]});
+                sc.area_colors.insert(sc.area_colors.end(), {em[0], em[1], em[2]});
                 sc.area_areas.push_back(surface_area(p[0], p[1], p[2]));
             }
         }
