@@ -127,6 +127,51 @@ def test_quad_split_takes_the_shorter_diagonal(tmp_path):
     np.testing.assert_array_equal(tri[5], [[0, 0, 2], [1, 1, 2], [0, 3, 2]])
 
 
+def test_large_file_parsed_in_chunks_equals_file_order(tmp_path):
+    """A file large enough to be parsed in several chunks: relative indices that reach across chunk boundaries,
+    material switches, groups and quads; the triangles, their order and material ids are known by
+    construction (and equal the reference loader's where its harness is built)."""
+    rng = np.random.default_rng(5)
+    n = 150_000
+    tri = rng.uniform(-10, 10, size=(n, 3, 3)).astype(np.float32)
+    lines = ["mtllib m.mtl"]
+    want_pos, want_mat = [], []
+    mat = -1
+    for i in range(n):
+        if i % 997 == 0:
+            mat = (i // 997) % 3
+            lines.append(f"usemtl m{mat}")
+        if i % 4999 == 0:
+            lines.append(f"g group{i}")
+        for k in range(3):
+            lines.append("v %.9g %.9g %.9g" % tuple(tri[i, k]))
+        if i % 7 == 3 and i > 0:
+            # a quad over the previous triangle's v2 and this one's: split along the shorter diagonal
+            lines.append("f -4 -3 -2 -1")
+            q = np.concatenate([tri[i - 1, 2:3], tri[i]])
+            d02, d13 = q[2] - q[0], q[3] - q[1]
+            s02 = np.float32(np.float32(d02[0] * d02[0] + d02[1] * d02[1]) + d02[2] * d02[2])
+            s13 = np.float32(np.float32(d13[0] * d13[0] + d13[1] * d13[1]) + d13[2] * d13[2])
+            for t in ([(0, 1, 2), (0, 2, 3)] if s02 < s13 else [(0, 1, 3), (1, 2, 3)]):
+                want_pos.append(q[list(t)])
+                want_mat.append(mat)
+        else:
+            lines.append(f"f {3 * i + 1 if i % 2 else -3} {3 * i + 2 if i % 2 else -2} -1")
+            want_pos.append(tri[i])
+            want_mat.append(mat)
+    (tmp_path / "big.obj").write_text("\n".join(lines) + "\n")
+    (tmp_path / "big.meta").write_text("cam_pos 0 0 0\n")
+    (tmp_path / "m.mtl").write_text("newmtl m0\nKd 1 0 0\nnewmtl m1\nKd 0 1 0\nnewmtl m2\nKe 1 1 1\n")
+    assert (tmp_path / "big.obj").stat().st_size > 16 << 20
+    sc = SI.load_obj_scene(str(tmp_path), "big")
+    np.testing.assert_array_equal(bits(sc.positions), bits(np.array(want_pos).reshape(-1, 9)))
+    np.testing.assert_array_equal(sc.material_ids, np.array(want_mat, np.int32))
+    assert [a.triangle_id for a in sc.area_lights] == list(np.nonzero(np.array(want_mat) == 2)[0])
+    import oracle as O
+    if os.path.exists(O.REF_LIB):
+        assert_same_scene(scene_arrays(sc), O.RefOracle().obj_scene(str(tmp_path), "big"))
+
+
 def test_loader_needs_no_device_and_checks_arguments():
     import ctypes as C
     from diplodocus_b200 import _lib as L
