@@ -504,6 +504,98 @@ def run_small(args):
         "sbvh_build_ms": round(sb.build_ms, 3)})
 
 
+def write_obj_scene(dirpath, name="sphere_room"):
+    """A Cornell-style OBJ scene of ~1M triangles as the reference's app would load it: the 1024x512 displaced
+    sphere as an indexed mesh (shared vertices), a floor quad, an emissive lamp quad, an MTL file and a .meta
+    camera. Coordinates are written with 9 significant digits, so they read back to the same float32."""
+    from diplodocus_b200 import scenes as S
+    tris, _ = S.displaced_sphere(n_rays=16)
+    flat = tris.reshape(-1, 3)
+    verts, inv = np.unique(flat, axis=0, return_inverse=True)
+    faces = inv.reshape(-1, 3) + 1
+    os.makedirs(dirpath, exist_ok=True)
+    with open(os.path.join(dirpath, name + ".obj"), "w") as f:
+        f.write("mtllib %s.mtl\ng floor\nusemtl floor\n" % name)
+        f.write("v -4 -1.2 -4\nv 4 -1.2 -4\nv 4 -1.2 4\nv -4 -1.2 4\nf -4 -3 -2 -1\n")
+        f.write("g lamp\nusemtl lamp\nv -0.5 2.5 -0.5\nv 0.5 2.5 -0.5\nv 0.5 2.5 0.5\nv -0.5 2.5 0.5\n"
+                "f -1 -2 -3 -4\ng sphere\nusemtl sphere\n")
+        np.savetxt(f, verts, fmt="v %.9g %.9g %.9g")
+        np.savetxt(f, faces + 8, fmt="f %d %d %d")
+    with open(os.path.join(dirpath, name + ".mtl"), "w") as f:
+        f.write("newmtl floor\nKd 0.7 0.7 0.7\nnewmtl lamp\nKd 0.8 0.8 0.8\nKe 12 12 11\n"
+                "newmtl sphere\nKd 0.6 0.3 0.2\nKs 0.1 0.1 0.1\nNs 20\n")
+    with open(os.path.join(dirpath, name + ".meta"), "w") as f:
+        f.write("cam_pos 0 0.2 -3.5\ncam_dir 0 -0.05 1\ncam_up 0 1 0\ncam_fov 0.9\ncam_far 100\n"
+                "point_light 0 2 -1 1 1 1 50\n")
+    return name, len(tris) + 4, os.path.getsize(os.path.join(dirpath, name + ".obj"))
+
+
+def run_obj_scene(args):
+    """OBJ scene path end to end: the reference's scene files (OBJ + MTL + .meta) -> the library's host loader
+    -> host-to-device copy -> PLOC build -> one device frame (pinhole + bounce), beside the reference's own
+    ObjSceneLoader and SBvh build on the same files."""
+    import tempfile
+
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from diplodocus_b200 import accel as A
+    from diplodocus_b200 import scene_io as SI
+    d = tempfile.mkdtemp(prefix="dipl_obj_")
+    name, n, size = write_obj_scene(d)
+    w = h = 512
+
+    def best(fn, k):
+        out = 1e30
+        for _ in range(k):
+            t0 = time.perf_counter()
+            fn()
+            out = min(out, time.perf_counter() - t0)
+        return out * 1e3
+
+    ms_load = best(lambda: SI.load_obj_scene(d, name), 3)
+    sc = SI.load_obj_scene(d, name)
+    host = torch.from_numpy(sc.triangles()).pin_memory()
+    dev = torch.empty_like(host, device="cuda")
+    ms_h2d = _time(lambda: dev.copy_(host, non_blocking=True), 5)
+    cfg = A.AccelerationStructureConfig()
+    ms_build = _time(lambda: A.GpuPlocBvh().Build(cfg, A.Stats(), dev), 5)
+    bvh = A.GpuPlocBvh().Build(cfg, A.Stats(), dev)
+    cam = sc.camera.as_dict()
+    ms_frame = _time(lambda: A.trace_frame(bvh, cam, w, h, 3), 10)
+    stats = A.Stats()
+    rays, hits, bounce, bhits = A.trace_frame(bvh, cam, w, h, 3, stats=stats)
+    n_rays = w * h + stats.rt_stats.secondary_ray_count
+
+    def e2e():
+        s2 = SI.load_obj_scene(d, name)
+        t = torch.from_numpy(s2.triangles()).cuda()
+        b = A.GpuPlocBvh().Build(cfg, A.Stats(), t)
+        A.trace_frame(b, s2.camera.as_dict(), w, h, 3)
+        torch.cuda.synchronize()
+    ms_e2e = best(e2e, 3)
+    ref = O.RefOracle()
+    ms_ref_load = best(lambda: ref.obj_scene(d, name), 2)
+    sb = ref.sbvh(sc.triangles())
+    ms_ref_build = sb.build_ms
+    sb.close()
+    _line("obj_scene", n / (ms_load + ms_h2d + ms_build) / 1e3, "Mtri/s", {
+        "config": {"workload": "obj_scene", "triangles": n, "obj_bytes": size, "frame": f"{w}x{h} pinhole + bounce",
+                   "description": "indexed OBJ: 1024x512 displaced sphere + floor + emissive lamp, MTL, .meta"},
+        "value_note": "scene file to device BVH: host load + host-to-device copy + PLOC build",
+        "load_ms": round(ms_load, 2), "load_mtri_s": round(n / ms_load / 1e3, 2),
+        "h2d_ms": round(ms_h2d, 3), "build_ms": round(ms_build, 3),
+        "frame": {"ms": round(ms_frame, 4), "rays": n_rays, "value": round(n_rays / ms_frame / 1e3, 2),
+                  "unit": "Mrays/s"},
+        "e2e": {"ms": round(ms_e2e, 2), "value": round(n / ms_e2e / 1e3, 3), "unit": "Mtri/s",
+                "steps": "load file, copy to the device, build, one frame, synchronise"},
+        "host_threads": os.cpu_count(),
+        "cpu_baseline": {"kind": "reference", "value": round(n / (ms_ref_load + ms_ref_build) / 1e3, 3),
+                         "unit": "Mtri/s", "cores": 1,
+                         "sample": "ObjSceneLoader::Load of the same files + SBvh::Build (1 thread)",
+                         "load_ms": round(ms_ref_load, 2), "sbvh_build_ms": round(ms_ref_build, 2)}})
+
+
 def run_soup16m(args):
     """16M soup: EMC60+SOBB and the 8-wide quantised form against binary FP32 nodes; t/u/v error vs FP64."""
     import torch
@@ -649,7 +741,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="dipl", choices=["dipl", "reference"])
     ap.add_argument("--workload", default="displaced_sphere",
-                    choices=["displaced_sphere", "small", "soup16m", "batched", "diff"])
+                    choices=["displaced_sphere", "small", "soup16m", "batched", "diff", "obj_scene"])
     ap.add_argument("--soup-tris", type=int, default=16 * 1024 * 1024)
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--code", default="morton30", choices=["morton30", "emc60"])
@@ -665,10 +757,11 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload in ("small", "soup16m", "batched", "diff") and world == 1:
+    if args.workload in ("small", "soup16m", "batched", "diff", "obj_scene") and world == 1:
         import torch
         torch.cuda.set_device(local_rank)
-        {"small": run_small, "soup16m": run_soup16m, "batched": run_batched, "diff": run_diff}[args.workload](args)
+        {"small": run_small, "soup16m": run_soup16m, "batched": run_batched, "diff": run_diff,
+         "obj_scene": run_obj_scene}[args.workload](args)
         return
     if world > 1:
         import datetime
