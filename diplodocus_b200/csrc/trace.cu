@@ -98,6 +98,37 @@ struct Stack {
     }
 };
 
+// Long rays of a warp whose chunk is handed out move to tail_kernel: once at most kTailLanes lanes of the warp
+// are still tracing, a lane whose ray has taken kTailSteps steps or more writes the ray's state (ray index, next
+// node, best hit so far, stack) to a slot and takes no more work; tail_kernel then traverses each such ray with a
+// whole warp. Without it the warp keeps issuing one-lane steps until its longest ray ends (the 1M sphere's
+// grazing rays take up to ~430 steps). With all 32 lanes busy (the soup) nothing is offloaded: the warp is
+// already fully used. Measured (4M rays on the 1M sphere / 1M rays on the 16M soup, identical hits): 0.633 ->
+// 0.497 ms / 52.97 -> 51.85 ms; offloading at 8-32 steps sends rays whose remaining work is too short for a
+// warp (sphere 0.73-0.84 ms), and offloading from full warps slows the soup (55.2 ms).
+constexpr int kTailSteps = 64;
+constexpr int kTailLanes = 8;  // ... and only when at most this many lanes of the warp are still tracing
+constexpr int kTailHeaderInts = 12;  // ray (2), cur, sp, best t/u/v, prim, found, pad
+constexpr size_t kTailBytes = 64u << 20;  // slot storage per trace call, at most
+
+struct TailQueue {
+    int* slots;          // slot_ints ints each: header, then sp (ref, t) pairs
+    unsigned* count;     // [0]: slots written (may exceed cap), [1]: slots taken by tail_kernel
+    int cap;             // slots available
+    int slot_ints;
+    int min_steps;       // 0: no offload
+    int max_lanes;
+};
+
+// Float bits in an order that compares like the floats (for warp minima).
+__device__ __forceinline__ unsigned ordered_bits(float f) {
+    const unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered_bits(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
 // Leaf test dispatch: ref_mt or watertight.
 template <int LEAF>
 __device__ __forceinline__ float leaf_test(float3 a, float3 b, float3 c, const RayState& r, const WtRay& w,
@@ -117,7 +148,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
                                                               int64_t n, int64_t chunk, dipl_hit* __restrict__ hits,
                                                               uint8_t* __restrict__ occluded, uint32_t flags,
                                                               unsigned long long* __restrict__ counters,
-                                                              uint32_t* __restrict__ err) {
+                                                              uint32_t* __restrict__ err, TailQueue tq) {
     __shared__ int2 sh_stack[SHORT > 0 ? SHORT * kTraceThreads : 1];
     const int lane = threadIdx.x & 31;
     const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -139,6 +170,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
     st.sh = sh_stack + threadIdx.x;
     unsigned visits = 0, tests = 0;
     bool bad = false;
+    bool may_offload = tq.min_steps > 0;
     for (;;) {
         // ---- refill idle lanes from the chunk --------------------------------------------------------
         const bool idle = my < 0;
@@ -158,7 +190,8 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
             }
             next = min(end, next + (int64_t)__popc(idle_mask));
         }
-        if (__all_sync(0xffffffffu, my < 0)) break;
+        const uint32_t active_mask = __ballot_sync(0xffffffffu, my >= 0);
+        if (!active_mask) break;
         if (my < 0) continue;
 
         // ---- one step: an inner node or a leaf --------------------------------------------------------
@@ -249,12 +282,200 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
                 reinterpret_cast<int4*>(hits)[my] = out;
             }
             my = -1;
+        } else if (may_offload && next >= end && steps >= (uint32_t)tq.min_steps &&
+                   __popc(active_mask) <= tq.max_lanes) {
+            // the chunk is handed out and this ray is still going: hand it to tail_kernel if a slot is free
+            const unsigned slot = atomicAdd(&tq.count[0], 1u);
+            if (slot < (unsigned)tq.cap) {
+                int* w = tq.slots + (size_t)slot * tq.slot_ints;
+                w[0] = (int)(uint32_t)(uint64_t)my;
+                w[1] = (int)(uint32_t)((uint64_t)my >> 32);
+                w[2] = cur;
+                w[3] = st.sp;
+                w[4] = __float_as_int(best_t);
+                w[5] = __float_as_int(best_u);
+                w[6] = __float_as_int(best_v);
+                w[7] = best_prim;
+                w[8] = found ? 1 : 0;
+                for (int k = 0; k < st.sp; ++k) reinterpret_cast<int2*>(w + kTailHeaderInts)[k] = st.get(k);
+                my = -1;
+            }
+            may_offload = false;  // one try per lane
         }
     }
     if (bad) atomicOr(err, kErrStack);
     if (COUNT) {
         const unsigned v = __reduce_add_sync(0xffffffffu, visits);
         const unsigned t = __reduce_add_sync(0xffffffffu, tests);
+        if (lane == 0) {
+            atomicAdd(&counters[0], (unsigned long long)v);
+            atomicAdd(&counters[1], (unsigned long long)t);
+        }
+    }
+}
+
+// One warp per offloaded ray. Its pending work (the node it was at and its stack entries) is dealt round-robin to
+// the lanes; each lane traverses near-child first with its own stack, lanes without work take the bottom entry
+// (the largest pending subtree) of a lane holding two or more, and every step prunes against the best t of the
+// whole warp (warp minimum, the same conservative slack as the main kernel). Each lane accepts leaf hits by the
+// closest-hit rule against its own best; the warp then keeps the smallest (t, primitive id) over its lanes and
+// the hit carried over from the main kernel, so the record is the one a single thread would produce.
+template <int LEAF, bool ANY, bool COUNT, int STACK>
+__global__ void __launch_bounds__(kTraceThreads) tail_kernel(const BNode* __restrict__ nodes,
+                                                             const float4* __restrict__ tris, int num_nodes,
+                                                             const dipl_ray* __restrict__ rays,
+                                                             dipl_hit* __restrict__ hits, uint8_t* __restrict__ occluded,
+                                                             uint32_t flags, unsigned long long* __restrict__ counters,
+                                                             uint32_t* __restrict__ err, TailQueue tq) {
+    constexpr int kNone = -0x7FFFFFFF - 1;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt_mask = lanemask_lt();
+    const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
+    const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+    const unsigned total = min(*reinterpret_cast<volatile unsigned*>(&tq.count[0]), (unsigned)tq.cap);
+    unsigned visits = 0, tests = 0;
+    bool bad = false;
+    int sref[STACK];
+    float stt[STACK];
+    for (;;) {
+        unsigned slot = 0;
+        if (lane == 0) slot = atomicAdd(&tq.count[1], 1u);
+        slot = __shfl_sync(full, slot, 0);
+        if (slot >= total) break;
+        const int* w = tq.slots + (size_t)slot * tq.slot_ints;
+        const int64_t my = (int64_t)(((uint64_t)(uint32_t)w[1] << 32) | (uint32_t)w[0]);
+        const int sp0 = min(w[3], STACK);
+        const RayState r = load_ray(rays, my);
+        WtRay wt{};
+        if (LEAF == DIPL_LEAF_WATERTIGHT) wt = wt_setup(r.d);
+        float best_t = r.tmax, best_u = 0.0f, best_v = 0.0f;
+        int best_prim = -1;
+        bool found = false;
+        if (lane == 0 && w[8]) {
+            best_t = __int_as_float(w[4]), best_u = __int_as_float(w[5]), best_v = __int_as_float(w[6]);
+            best_prim = w[7];
+            found = true;
+        }
+        // deal the pending items: stack entries 0..sp0-1, then the node the ray was at (always visited)
+        int bot = 0, sp = 0, cur = kNone;
+        for (int k = lane; k <= sp0; k += 32) {
+            int ref;
+            float t;
+            if (k < sp0) {
+                const int2 e = reinterpret_cast<const int2*>(w + kTailHeaderInts)[k];
+                ref = e.x, t = __int_as_float(e.y);
+            } else {
+                ref = w[2], t = -__int_as_float(0x7F800000);
+            }
+            sref[sp] = ref, stt[sp] = t, ++sp;
+        }
+        uint32_t steps = 0;
+        for (;;) {
+            const float gbest = from_ordered_bits(__reduce_min_sync(full, ordered_bits(best_t)));
+            const float lim = prune_limit(gbest);
+            while (cur == kNone && sp > bot) {
+                --sp;
+                if (stt[sp] <= lim) cur = sref[sp];
+            }
+            if (sp == bot) sp = bot = 0;
+            const bool hungry = cur == kNone;
+            const uint32_t hm = __ballot_sync(full, hungry);
+            if (hm == full) break;
+            if (hm) {
+                const uint32_t dm = __ballot_sync(full, sp - bot >= 2);
+                const int nh = __popc(hm), nd = __popc(dm);
+                const bool donate = ((dm >> lane) & 1u) && __popc(dm & lt_mask) < nh;
+                int gref = kNone;
+                float gt = 0.0f;
+                if (donate) {
+                    gref = sref[bot], gt = stt[bot];
+                    ++bot;
+                }
+                const int rank = __popc(hm & lt_mask);
+                const bool receive = hungry && rank < nd;
+                const int src = receive ? (int)__fns(dm, 0, rank + 1) : lane;
+                const int rref = __shfl_sync(full, gref, src);
+                const float rt = __shfl_sync(full, gt, src);
+                if (receive && rref != kNone && rt <= lim) cur = rref;
+            }
+            if (cur != kNone) {
+                if (++steps > step_limit || (cur >= 0 && cur >= num_nodes)) {
+                    bad = true;
+                    cur = kNone;
+                    sp = bot = 0;
+                } else if (cur >= 0) {
+                    const float4* np = reinterpret_cast<const float4*>(nodes + cur);
+                    float4 a, b, c, df;
+                    ldg_v8(np, a, b);
+                    ldg_v8(np + 2, c, df);
+                    if (COUNT) ++visits;
+                    const float t0 = box_entry(r, a.x, a.y, a.z, a.w, c.x, c.y, lim);
+                    const float t1 = box_entry(r, b.x, b.y, b.z, b.w, c.z, c.w, lim);
+                    const bool h0 = t0 != __int_as_float(0x7F800000), h1 = t1 != __int_as_float(0x7F800000);
+                    const int c0 = __float_as_int(df.x), c1 = __float_as_int(df.y);
+                    if (h0 && h1) {
+                        const bool first0 = t0 <= t1;
+                        if (sp >= STACK) {
+                            bad = true;
+                            cur = kNone;
+                        } else {
+                            sref[sp] = first0 ? c1 : c0, stt[sp] = first0 ? t1 : t0, ++sp;
+                            cur = first0 ? c0 : c1;
+                        }
+                    } else {
+                        cur = h0 ? c0 : (h1 ? c1 : kNone);
+                    }
+                } else {
+                    const int first = leaf_first(cur), cnt = leaf_count(cur);
+                    for (int k = 0; k < cnt; ++k) {
+                        const float4* tp = tris + 3 * (int64_t)(first + k);
+                        const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+                        const int prim = __float_as_int(p0.w);
+                        float b1 = 0.0f, b2 = 0.0f;
+                        const float t = leaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
+                                                        make_float3(p2.x, p2.y, p2.z), r, wt, backface, b1, b2);
+                        if (COUNT) ++tests;
+                        if (ANY) {
+                            if (t > r.tmin && t < r.tmax && t < kInfinity) found = true;
+                        } else if (t > r.tmin && t < kInfinity &&
+                                   (t < best_t || (t == best_t && found && prim < best_prim))) {
+                            best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
+                        }
+                    }
+                    cur = kNone;
+                }
+            }
+            if (ANY && __any_sync(full, found)) break;
+        }
+        // the smallest (t, primitive id) of the warp
+        if (ANY) {
+            const bool any = __any_sync(full, found);
+            if (lane == 0) occluded[my] = any ? 1 : 0;
+        } else {
+            const unsigned tk = found ? ordered_bits(best_t) : 0xFFFFFFFFu;
+            const unsigned tmin = __reduce_min_sync(full, tk);
+            const bool cand = found && tk == tmin;
+            const unsigned pmin = __reduce_min_sync(full, cand ? (unsigned)best_prim : 0xFFFFFFFFu);
+            const uint32_t win = __ballot_sync(full, cand && (unsigned)best_prim == pmin);
+            const int wl = win ? __ffs(win) - 1 : 0;
+            const float ft = __shfl_sync(full, best_t, wl), fu = __shfl_sync(full, best_u, wl),
+                        fv = __shfl_sync(full, best_v, wl);
+            const int fp = __shfl_sync(full, best_prim, wl);
+            if (lane == 0) {
+                int4 out;
+                out.x = win ? fp : -1;
+                out.y = __float_as_int(win ? ft : __int_as_float(0x7F800000));
+                out.z = __float_as_int(win ? fu : 0.0f);
+                out.w = __float_as_int(win ? fv : 0.0f);
+                reinterpret_cast<int4*>(hits)[my] = out;
+            }
+        }
+    }
+    if (bad) atomicOr(err, kErrStack);
+    if (COUNT) {
+        const unsigned v = __reduce_add_sync(full, visits);
+        const unsigned t = __reduce_add_sync(full, tests);
         if (lane == 0) {
             atomicAdd(&counters[0], (unsigned long long)v);
             atomicAdd(&counters[1], (unsigned long long)t);
@@ -275,6 +496,9 @@ int persistent_grid(K kernel) {
     return grid;
 }
 
+int tail_min_steps() { return kTailSteps; }
+int tail_max_lanes() { return kTailLanes; }
+
 template <int LEAF, bool ANY, bool COUNT, int STACK, int SHORT>
 dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
                          uint32_t flags, unsigned long long* counters, cudaStream_t s) {
@@ -290,10 +514,36 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
         set_last_error("trace: node array is not 64-byte aligned");
         return DIPL_ERR_INTERNAL;
     }
+    TailQueue tq{nullptr, nullptr, 0, kTailHeaderInts + 2 * STACK, tail_min_steps(), tail_max_lanes()};
+    void* tail_mem = nullptr;
+    if (tq.min_steps > 0) {
+        const size_t slot_bytes = sizeof(int) * (size_t)tq.slot_ints;
+        tq.cap = (int)std::max<int64_t>(1, std::min<int64_t>(n, (int64_t)(kTailBytes / slot_bytes)));
+        const size_t bytes = (size_t)tq.cap * slot_bytes;
+        dipl_status st = device_alloc(&tail_mem, bytes + 16, s);
+        if (st != DIPL_OK) return st;
+        tq.slots = static_cast<int*>(tail_mem);
+        tq.count = reinterpret_cast<unsigned*>(static_cast<char*>(tail_mem) + bytes);
+        const cudaError_t e = cudaMemsetAsync(tq.count, 0, 2 * sizeof(unsigned), s);
+        if (e != cudaSuccess) {
+            device_free(tail_mem, s);
+            return cuda_status(e, "cudaMemsetAsync");
+        }
+    }
     kernel<<<(unsigned)grid, kTraceThreads, 0, s>>>(static_cast<const BNode*>(b->nodes), b->tris, b->root, num_nodes,
-                                                   rays, n, chunk, hits, occ, flags, counters, b->d_err);
+                                                   rays, n, chunk, hits, occ, flags, counters, b->d_err, tq);
     note_launches();
-    DIPL_CUDA(cudaGetLastError());
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && tq.min_steps > 0) {
+        auto tk = tail_kernel<LEAF, ANY, COUNT, STACK>;
+        tk<<<(unsigned)persistent_grid(tk), kTraceThreads, 0, s>>>(static_cast<const BNode*>(b->nodes), b->tris,
+                                                                   num_nodes, rays, hits, occ, flags, counters,
+                                                                   b->d_err, tq);
+        note_launches();
+        e = cudaGetLastError();
+    }
+    device_free(tail_mem, s);
+    DIPL_CUDA(e);
     return DIPL_OK;
 }
 
