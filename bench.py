@@ -193,10 +193,11 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------------------------------
-# DRAM bytes (read + write) of one build and of one 4M-ray closest-hit trace of the default workload, from one
-# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, summed over the build's kernels):
-# profiles/dram_traffic_displaced_sphere_1m.md. Other workloads report null.
-MEASURED_TRAFFIC = {"displaced_sphere": {"build": 526.72e6, "trace": 361.09e6, "rays": 4194304,
+# DRAM bytes (read + write) of one build and of one 4M-ray closest-hit trace of the default workload, from ncu
+# captures (dram__bytes_read.sum + dram__bytes_write.sum, summed over the build's kernels and over the trace's
+# two kernels): profiles/dram_traffic_displaced_sphere_1m.md, profiles/trace_kernel_displaced_sphere_1m.md.
+# Other workloads report null.
+MEASURED_TRAFFIC = {"displaced_sphere": {"build": 526.72e6, "trace": 348.9e6, "rays": 4194304,
                                          "triangles": 1046528}}
 
 
