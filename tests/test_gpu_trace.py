@@ -139,6 +139,28 @@ def test_displaced_sphere_1m_hits_verified(orc):
     np.testing.assert_array_equal(fbits(t[sample]), fbits(h.t))
 
 
+@pytest.mark.gpu
+def test_long_grazing_rays_equal_brute_force(orc):
+    """Rays that skim the displaced sphere take hundreds of steps; traced as a small batch, every warp has handed
+    out its rays at once, so the long ones move to the warp-per-ray tail kernel. All of them equal brute force
+    (closest hit, lowest-id ties), and so do their counts with and without counters."""
+    tris, rays = S.displaced_sphere(n_rays=1 << 20)
+    o, d = rays[:, 0:3].astype(np.float64), rays[:, 4:7].astype(np.float64)
+    closest = np.linalg.norm(np.cross(o, d), axis=1) / np.linalg.norm(d, axis=1)
+    graze = rays[(closest > 0.93) & (closest < 1.07)][:2048]
+    assert len(graze) == 2048
+    bvh = build(tris)
+    prim, t, u, v = trace(bvh, graze)
+    h = orc.brute(tris, graze)
+    np.testing.assert_array_equal(prim, h.prim)
+    np.testing.assert_array_equal(fbits(t), fbits(h.t))
+    np.testing.assert_array_equal(fbits(u), fbits(h.u))
+    st = A.Stats()
+    hc = bvh.Intersect(st, torch.from_numpy(graze), count=True)
+    np.testing.assert_array_equal(hc.prim.cpu().numpy(), prim)
+    assert st.accel_stats.traversal_count / len(graze) > 20  # long rays indeed
+
+
 def _decode_wide(nodes_bytes):
     """Numpy view of the 80-byte wide nodes and their decoded child boxes (FP32 fma emulated exactly)."""
     rec = np.frombuffer(nodes_bytes, dtype=np.dtype([
