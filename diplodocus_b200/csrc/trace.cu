@@ -496,9 +496,6 @@ int persistent_grid(K kernel) {
     return grid;
 }
 
-int tail_min_steps() { return kTailSteps; }
-int tail_max_lanes() { return kTailLanes; }
-
 template <int LEAF, bool ANY, bool COUNT, int STACK, int SHORT>
 dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
                          uint32_t flags, unsigned long long* counters, cudaStream_t s) {
@@ -514,7 +511,7 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
         set_last_error("trace: node array is not 64-byte aligned");
         return DIPL_ERR_INTERNAL;
     }
-    TailQueue tq{nullptr, nullptr, 0, kTailHeaderInts + 2 * STACK, tail_min_steps(), tail_max_lanes()};
+    TailQueue tq{nullptr, nullptr, 0, kTailHeaderInts + 2 * STACK, kTailSteps, kTailLanes};
     void* tail_mem = nullptr;
     if (tq.min_steps > 0) {
         const size_t slot_bytes = sizeof(int) * (size_t)tq.slot_ints;
