@@ -369,6 +369,7 @@ struct PlocParams {
     int num_leaves;
     int num_meshes;
     int radius;
+    int grid_stop;  // ploc_kernel runs while more clusters than this remain (the middle phase's capacity, or kTailMax)
 };
 
 // Parity-selected pointers of PlocParams (a select, so the parameter block is never copied to the stack for
@@ -479,8 +480,11 @@ __device__ __forceinline__ void nn_search_sym(const float4* __restrict__ slo, co
 // oracle's key (distance bits << 32 | gap << 2 | parity << 1 | side). Each thread visits its own gaps in
 // increasing order, so its local strict-"<" minimum is its subset's key minimum.
 template <int NT>
+// slo / shi hold positions [wbase, ...) and nn receives positions [nbase, ...) (both 0 when the whole set is
+// resident).
 __device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, const float4* __restrict__ shi, int n,
-                                                int q0, int q1, int r, int* __restrict__ nn) {
+                                                int q0, int q1, int r, int* __restrict__ nn, int wbase = 0,
+                                                int nbase = 0) {
     const int m = q1 - q0;
     int P = 1;
     while (P < 16 && 2 * P * m <= NT) P *= 2;
@@ -493,13 +497,13 @@ __device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, 
         if (q0 + (int)(threadIdx.x & ~31u) / P + rd * lanes >= q1) break;
         unsigned long long key = ~0ull;
         if (q < q1) {
-            const float4 a = slo[q], b = shi[q];
+            const float4 a = slo[q - wbase], b = shi[q - wbase];
             const int sg = __float_as_int(b.w);
             float bestd = __int_as_float(0x7F800000);
             int bestj = -1;
             auto consider = [&](int j) {
                 if (j < 0 || j >= n) return;
-                const float4 c = slo[j], e = shi[j];
+                const float4 c = slo[j - wbase], e = shi[j - wbase];
                 if (__float_as_int(e.w) != sg) return;
                 const float d = ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, e.x, e.y, e.z);
                 if (d < bestd || bestj < 0) {
@@ -530,7 +534,7 @@ __device__ __forceinline__ void nn_search_split(const float4* __restrict__ slo, 
                 const int gap = (int)(tie >> 2);
                 j = (tie & 1u) ? q + gap : q - gap;
             }
-            nn[q] = j;
+            nn[q - nbase] = j;
         }
     }
 }
@@ -698,7 +702,7 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
         const int n = s.n, mbase = s.mbase;
         const bool ok = s.ok != 0;
         __syncthreads();
-        if (!ok || n <= P.num_meshes || n <= kTailMax) break;
+        if (!ok || n <= P.num_meshes || n <= P.grid_stop) break;
         if (iter >= kMaxPlocIterations) {
             if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
             break;
@@ -738,6 +742,173 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
         ++iter;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) P.ctrl->iterations = iter;
+}
+
+// Iterations between ctas * kMidSlice and kTailMax clusters in one thread-block cluster of 16 (or 8) CTAs of 1024
+// threads.
+// There ploc_kernel pays ~15 us per iteration for a chain of global round trips (tile claim, window load,
+// look-back, grid barrier) while only a few blocks have tiles. Here the clusters stay in global memory (L2):
+// CTA k takes positions [k * slice, (k + 1) * slice), loads them with a halo of r on each side into shared
+// memory and finds their nearest neighbours (same search and key as everywhere); after a cluster barrier the
+// mutual test reads a neighbour's choice from its owner's shared memory when it lies in another slice; the
+// slices' (kept, merged) counts are exchanged the same way, so every CTA derives the same prefix, totals and
+// next cluster count, and writes its kept clusters and new nodes in position order exactly as ploc_kernel
+// numbers them. Every branch depends only on values that are identical in all CTAs, so all of them reach the
+// same barriers.
+constexpr int kMidCtasMax = 16;  // a non-portable cluster size; 8 where 16 cannot be scheduled
+constexpr int kMidSlice = 2048;  // positions per CTA at most: the phase covers up to ctas * kMidSlice clusters
+constexpr int kMidWindow = kMidSlice + 2 * kRadiusMax;
+
+struct MidSmem {
+    float4 lo[kMidWindow];
+    float4 hi[kMidWindow];
+    int4 info[kMidWindow];
+    int nn[kMidSlice];
+    uint32_t warp_sum[kTailThreads / 32];
+    uint32_t totals;  // kept | merged << 16 of this CTA's slice
+};
+
+__global__ void __launch_bounds__(kTailThreads) ploc_mid_kernel(PlocParams P) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    MidSmem& s = *reinterpret_cast<MidSmem*>(s_raw);
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int ctas = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    constexpr int IPT = kMidSlice / kTailThreads;
+    // every CTA reads the same control words: the decisions below are identical across the cluster
+    const bool err0 = ld_acquire_u32(P.err) != 0u;
+    uint32_t iter = P.ctrl->iterations;
+    int n = (int)P.ctrl->n[iter & 1];
+    int mbase = (int)P.ctrl->merges[iter & 1];
+    if (err0 || n <= P.num_meshes || n <= kTailMax) return;
+    if (n > ctas * kMidSlice) {  // cannot happen: ploc_kernel runs until n <= grid_stop
+        if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+        return;
+    }
+    const int r = P.radius;
+    const int max_internal = P.num_leaves - P.num_meshes;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    bool failed = false;
+    cluster.sync();  // all CTAs are running before anyone reads a peer's shared memory
+    while (n > P.num_meshes && n > kTailMax) {
+        if (iter >= kMaxPlocIterations) {
+            if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+            failed = true;
+            break;
+        }
+        const int par = (int)(iter & 1);
+        const int slice = (n + ctas - 1) / ctas;
+        const int q0 = min(n, rank * slice), q1 = min(n, q0 + slice);
+        const int w0 = max(0, q0 - r), w1 = min(n, q1 + r);
+        const float4* __restrict__ glo = by_parity(P.lo, par);
+        const float4* __restrict__ ghi = by_parity(P.hi, par);
+        const int4* __restrict__ gin = by_parity(P.info, par);
+        for (int i = threadIdx.x; i < w1 - w0; i += kTailThreads) {
+            cp_async16(&s.lo[i], glo + w0 + i);
+            cp_async16(&s.hi[i], ghi + w0 + i);
+            cp_async16(&s.info[i], gin + w0 + i);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        nn_search_split<kTailThreads>(s.lo, s.hi, n, q0, q1, r, s.nn, w0, q0);
+        __syncthreads();
+        cluster.sync();  // every slice's neighbours are in its owner's shared memory
+        // ---- merge decisions for this slice ---------------------------------------------------------
+        const int ib = q0 + (int)threadIdx.x * IPT;
+        uint32_t keep_bits = 0, merge_bits = 0;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int i = ib + k;
+            if (i >= q1) break;
+            const int j = s.nn[i - q0];
+            bool mutual = false;
+            if (j >= 0) {
+                int back;
+                if (j >= q0 && j < q1) {
+                    back = s.nn[j - q0];
+                } else {
+                    const int owner = j / slice;
+                    back = cluster.map_shared_rank(s.nn, owner)[j - owner * slice];
+                }
+                mutual = back == i;
+            }
+            if (!(mutual && i > j)) keep_bits |= 1u << k;
+            if (mutual && i < j) merge_bits |= 1u << k;
+        }
+        const uint32_t mine = (uint32_t)__popc(keep_bits) | ((uint32_t)__popc(merge_bits) << 16);
+        uint32_t x = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s.warp_sum[warp] = x;
+        __syncthreads();
+        const uint32_t ws = s.warp_sum[lane];
+        uint32_t wx = ws;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wx, o);
+            if (lane >= o) wx += y;
+        }
+        const uint32_t local_total = __shfl_sync(0xffffffffu, wx, 31);
+        const uint32_t woff = __shfl_sync(0xffffffffu, wx - ws, warp);
+        const uint32_t excl = woff + x - mine;
+        if (threadIdx.x == 0) s.totals = local_total;
+        __syncthreads();
+        cluster.sync();  // every slice's counts are published; every peer has read this CTA's neighbours
+        uint32_t before = 0, all = 0;
+        for (int c = 0; c < ctas; ++c) {
+            const uint32_t t = *cluster.map_shared_rank(&s.totals, c);
+            if (c < rank) before += t;
+            all += t;
+        }
+        // ---- kept clusters and new nodes, in position order ----------------------------------------
+        float4* __restrict__ olo = by_parity(P.lo, par ^ 1);
+        float4* __restrict__ ohi = by_parity(P.hi, par ^ 1);
+        int4* __restrict__ oin = by_parity(P.info, par ^ 1);
+        uint32_t kpos = (before & 0xFFFFu) + (excl & 0xFFFFu);
+        uint32_t mpos = (uint32_t)mbase + (before >> 16) + (excl >> 16);
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            if (!((keep_bits >> k) & 1u)) continue;
+            const int i = ib + k;
+            float4 oa = s.lo[i - w0], ob = s.hi[i - w0];
+            int4 oi = s.info[i - w0];
+            if ((merge_bits >> k) & 1u) {
+                const int j = s.nn[i - q0];
+                const int knew = (int)mpos++;
+                if (knew >= max_internal) {
+                    atomicOr(P.err, kErrIterations);
+                    continue;
+                }
+                emit_node(P, knew, s.lo[i - w0], s.hi[i - w0], s.info[i - w0], s.lo[j - w0], s.hi[j - w0],
+                          s.info[j - w0], oa, ob, oi);
+            }
+            olo[kpos] = oa;
+            ohi[kpos] = ob;
+            oin[kpos] = oi;
+            ++kpos;
+        }
+        const int kept = (int)(all & 0xFFFFu);
+        __threadfence();
+        __syncthreads();
+        cluster.sync();  // this iteration's clusters are written; no peer reads the counts any more
+        if (kept == n) {  // no progress: impossible under a strict total order on pairs
+            if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
+            failed = true;
+            break;
+        }
+        n = kept;
+        mbase += (int)(all >> 16);
+        ++iter;
+    }
+    if (!failed && rank == 0 && threadIdx.x == 0) {
+        P.ctrl->n[iter & 1] = (uint32_t)n;
+        P.ctrl->merges[iter & 1] = (uint32_t)mbase;
+        P.ctrl->iterations = iter;
+    }
 }
 
 // The last iterations (at most kTailMax clusters) in one thread-block cluster of kTailCtas CTAs of 1024 threads.
@@ -1204,6 +1375,48 @@ dipl_status launch_ploc(const PlocParams& P, int initial_tiles, cudaStream_t str
     return DIPL_OK;
 }
 
+// CTAs of the middle phase: the largest cluster of 16 or 8 CTAs the device schedules with its shared memory, 0
+// without one (then ploc_kernel runs down to kTailMax clusters).
+int ploc_mid_ctas() {
+    static int ctas = -1;
+    if (ctas < 0) {
+        ctas = 0;
+        const size_t smem = sizeof(MidSmem);
+        if (cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+                cudaSuccess &&
+            cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            for (int c = kMidCtasMax; c >= 8 && ctas == 0; c /= 2) {
+                cudaLaunchConfig_t cfg = {};
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = c, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
+                cfg.gridDim = dim3(c), cfg.blockDim = dim3(kTailThreads), cfg.dynamicSmemBytes = smem;
+                cfg.attrs = attr, cfg.numAttrs = 1;
+                int clusters = 0;
+                if (cudaOccupancyMaxActiveClusters(&clusters, ploc_mid_kernel, &cfg) == cudaSuccess && clusters > 0)
+                    ctas = c;
+            }
+        }
+        (void)cudaGetLastError();
+    }
+    return ctas;
+}
+
+dipl_status launch_ploc_mid(const PlocParams& P, int ctas, cudaStream_t stream) {
+    const size_t smem = sizeof(MidSmem);
+    DIPL_CUDA(cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DIPL_CUDA(cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ctas, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(ctas), cfg.blockDim = dim3(kTailThreads), cfg.dynamicSmemBytes = smem, cfg.stream = stream;
+    cfg.attrs = attr, cfg.numAttrs = 1;
+    DIPL_CUDA(cudaLaunchKernelEx(&cfg, ploc_mid_kernel, P));
+    note_launches();
+    return DIPL_OK;
+}
+
 dipl_status launch_ploc_tail(const PlocParams& P, cudaStream_t stream) {
     const size_t smem = sizeof(TailSmem);
     DIPL_CUDA(cudaFuncSetAttribute(ploc_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1490,7 +1703,9 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     pp.status[0] = P.status, pp.status[1] = P.status + P.tiles_max + 1;
     pp.ctrl = P.d_ctrl, pp.err = P.d_err;
     pp.num_leaves = (int)N, pp.num_meshes = m, pp.radius = d0.nn_search_radius;
-    if (N > m && N > kTailMax) {
+    const int mid_ctas = ploc_mid_ctas();
+    pp.grid_stop = mid_ctas > 0 ? mid_ctas * kMidSlice : kTailMax;
+    if (N > m && N > pp.grid_stop) {
         switch (P.B) {
             case 128: st = launch_ploc_any<128>(pp, P.tiles0, stream); break;
             case 512: st = launch_ploc_any<512>(pp, P.tiles0, stream); break;
@@ -1498,6 +1713,7 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
         }
         if (st != DIPL_OK) return st;
     }
+    if (N > m && N > kTailMax && mid_ctas > 0 && (st = launch_ploc_mid(pp, mid_ctas, stream)) != DIPL_OK) return st;
     if (N > m && (st = launch_ploc_tail(pp, stream)) != DIPL_OK) return st;
 
     // ---- layout -------------------------------------------------------------------------------------
