@@ -749,21 +749,23 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
 // There ploc_kernel pays ~15 us per iteration for a chain of global round trips (tile claim, window load,
 // look-back, grid barrier) while only a few blocks have tiles. Here the clusters stay in global memory (L2):
 // CTA k takes positions [k * slice, (k + 1) * slice), loads them with a halo of r on each side into shared
-// memory and finds their nearest neighbours (same search and key as everywhere); after a cluster barrier the
-// mutual test reads a neighbour's choice from its owner's shared memory when it lies in another slice; the
-// slices' (kept, merged) counts are exchanged the same way, so every CTA derives the same prefix, totals and
+// memory and finds the nearest neighbours of its slice and of the r positions on either side (same key as
+// everywhere, each pair evaluated once), so the mutual test needs no other CTA; the slices' (kept, merged)
+// counts are exchanged through distributed shared memory, so every CTA derives the same prefix, totals and
 // next cluster count, and writes its kept clusters and new nodes in position order exactly as ploc_kernel
 // numbers them. Every branch depends only on values that are identical in all CTAs, so all of them reach the
 // same barriers.
 constexpr int kMidCtasMax = 16;  // a non-portable cluster size; 8 where 16 cannot be scheduled
 constexpr int kMidSlice = 2048;  // positions per CTA at most: the phase covers up to ctas * kMidSlice clusters
-constexpr int kMidWindow = kMidSlice + 2 * kRadiusMax;
+constexpr int kMidWindow = kMidSlice + 4 * kRadiusMax;  // the slice, its neighbours' positions and theirs
+constexpr int kMidNear = kMidSlice + 2 * kRadiusMax;    // positions whose nearest neighbour the CTA computes
 
 struct MidSmem {
     float4 lo[kMidWindow];
     float4 hi[kMidWindow];
     int4 info[kMidWindow];
-    int nn[kMidSlice];
+    int nn[kMidNear];
+    unsigned long long key[kMidNear];
     uint32_t warp_sum[kTailThreads / 32];
     uint32_t totals;  // kept | merged << 16 of this CTA's slice
 };
@@ -800,7 +802,8 @@ __global__ void __launch_bounds__(kTailThreads) ploc_mid_kernel(PlocParams P) {
         const int par = (int)(iter & 1);
         const int slice = (n + ctas - 1) / ctas;
         const int q0 = min(n, rank * slice), q1 = min(n, q0 + slice);
-        const int w0 = max(0, q0 - r), w1 = min(n, q1 + r);
+        const int e0 = max(0, q0 - r), e1 = min(n, q1 + r);          // positions whose neighbour we need
+        const int w0 = max(0, q0 - 2 * r), w1 = min(n, q1 + 2 * r);  // and their candidates
         const float4* __restrict__ glo = by_parity(P.lo, par);
         const float4* __restrict__ ghi = by_parity(P.hi, par);
         const int4* __restrict__ gin = by_parity(P.info, par);
@@ -811,9 +814,8 @@ __global__ void __launch_bounds__(kTailThreads) ploc_mid_kernel(PlocParams P) {
         }
         cp_async_wait_all();
         __syncthreads();
-        nn_search_split<kTailThreads>(s.lo, s.hi, n, q0, q1, r, s.nn, w0, q0);
+        nn_search_sym<kTailThreads>(s.lo, s.hi, w0, n, e0, e1, r, s.nn, s.key);
         __syncthreads();
-        cluster.sync();  // every slice's neighbours are in its owner's shared memory
         // ---- merge decisions for this slice ---------------------------------------------------------
         const int ib = q0 + (int)threadIdx.x * IPT;
         uint32_t keep_bits = 0, merge_bits = 0;
@@ -821,18 +823,8 @@ __global__ void __launch_bounds__(kTailThreads) ploc_mid_kernel(PlocParams P) {
         for (int k = 0; k < IPT; ++k) {
             const int i = ib + k;
             if (i >= q1) break;
-            const int j = s.nn[i - q0];
-            bool mutual = false;
-            if (j >= 0) {
-                int back;
-                if (j >= q0 && j < q1) {
-                    back = s.nn[j - q0];
-                } else {
-                    const int owner = j / slice;
-                    back = cluster.map_shared_rank(s.nn, owner)[j - owner * slice];
-                }
-                mutual = back == i;
-            }
+            const int j = s.nn[i - e0];
+            const bool mutual = j >= 0 && s.nn[j - e0] == i;  // j is within r of i: inside [e0, e1)
             if (!(mutual && i > j)) keep_bits |= 1u << k;
             if (mutual && i < j) merge_bits |= 1u << k;
         }
@@ -857,7 +849,7 @@ __global__ void __launch_bounds__(kTailThreads) ploc_mid_kernel(PlocParams P) {
         const uint32_t excl = woff + x - mine;
         if (threadIdx.x == 0) s.totals = local_total;
         __syncthreads();
-        cluster.sync();  // every slice's counts are published; every peer has read this CTA's neighbours
+        cluster.sync();  // every slice's counts are published
         uint32_t before = 0, all = 0;
         for (int c = 0; c < ctas; ++c) {
             const uint32_t t = *cluster.map_shared_rank(&s.totals, c);
@@ -877,7 +869,7 @@ __global__ void __launch_bounds__(kTailThreads) ploc_mid_kernel(PlocParams P) {
             float4 oa = s.lo[i - w0], ob = s.hi[i - w0];
             int4 oi = s.info[i - w0];
             if ((merge_bits >> k) & 1u) {
-                const int j = s.nn[i - q0];
+                const int j = s.nn[i - e0];
                 const int knew = (int)mpos++;
                 if (knew >= max_internal) {
                     atomicOr(P.err, kErrIterations);
