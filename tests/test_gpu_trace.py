@@ -141,24 +141,30 @@ def test_displaced_sphere_1m_hits_verified(orc):
 
 @pytest.mark.gpu
 def test_long_grazing_rays_equal_brute_force(orc):
-    """Rays that skim the displaced sphere take hundreds of steps; traced as a small batch, every warp has handed
-    out its rays at once, so the long ones move to the warp-per-ray tail kernel. All of them equal brute force
-    (closest hit, lowest-id ties), and so do their counts with and without counters."""
+    """Rays that skim the displaced sphere take hundreds of steps. Traced first in a batch of 2^19 rays (the
+    smallest batch that uses the offload), the warps whose chunks hold them hand their long rays to the
+    warp-per-ray tail kernel. The first 2048 equal brute force (closest hit, lowest-id ties), and the counted
+    trace returns the same records."""
     tris, rays = S.displaced_sphere(n_rays=1 << 20)
     o, d = rays[:, 0:3].astype(np.float64), rays[:, 4:7].astype(np.float64)
     closest = np.linalg.norm(np.cross(o, d), axis=1) / np.linalg.norm(d, axis=1)
-    graze = rays[(closest > 0.93) & (closest < 1.07)][:2048]
-    assert len(graze) == 2048
+    is_graze = (closest > 0.93) & (closest < 1.07)
+    graze = rays[is_graze]
+    assert len(graze) > 2048
+    batch = np.ascontiguousarray(np.concatenate([graze, rays[~is_graze][: (1 << 19) - len(graze)]]))
+    assert len(batch) == 1 << 19
     bvh = build(tris)
-    prim, t, u, v = trace(bvh, graze)
-    h = orc.brute(tris, graze)
-    np.testing.assert_array_equal(prim, h.prim)
-    np.testing.assert_array_equal(fbits(t), fbits(h.t))
-    np.testing.assert_array_equal(fbits(u), fbits(h.u))
+    prim, t, u, v = trace(bvh, batch)
+    h = orc.brute(tris, graze[:2048])
+    np.testing.assert_array_equal(prim[:2048], h.prim)
+    np.testing.assert_array_equal(fbits(t[:2048]), fbits(h.t))
+    np.testing.assert_array_equal(fbits(u[:2048]), fbits(h.u))
     st = A.Stats()
-    hc = bvh.Intersect(st, torch.from_numpy(graze), count=True)
+    hc = bvh.Intersect(st, torch.from_numpy(batch), count=True)
     np.testing.assert_array_equal(hc.prim.cpu().numpy(), prim)
-    assert st.accel_stats.traversal_count / len(graze) > 20  # long rays indeed
+    long = A.Stats()
+    bvh.Intersect(long, torch.from_numpy(np.ascontiguousarray(graze[:2048])), count=True)
+    assert long.accel_stats.traversal_count / 2048 > 20  # long rays indeed
 
 
 def _decode_wide(nodes_bytes):
