@@ -50,7 +50,8 @@ struct PlocCtrl {
 namespace {
 
 constexpr int kRadiusMax = 32;
-constexpr int kPlocIpt = 2;  // positions per thread at most (4 measured 3% slower: 68 KB of shared memory per 256 threads)
+// Positions per thread at most in a ploc_kernel tile: 1024-position tiles at 256 and 512 threads (512 at 128).
+__host__ __device__ constexpr int ploc_ipt_max(int B) { return B >= 512 ? 2 : 4; }
 constexpr uint32_t kMaxPlocIterations = 1u << 16;
 
 __device__ __forceinline__ int find_mesh(const long long* __restrict__ offsets, int m, long long g) {
@@ -557,7 +558,7 @@ __device__ __forceinline__ void emit_node(const PlocParams& P, int knew, const f
 
 template <int B>
 struct PlocSmem {
-    static constexpr int T = B * kPlocIpt;
+    static constexpr int T = B * ploc_ipt_max(B);
     static constexpr int W = T + 4 * kRadiusMax;
     float4 lo[W];  // min xyz, node id bits
     float4 hi[W];  // max xyz, mesh index bits
@@ -576,7 +577,7 @@ struct PlocSmem {
 template <int B>
 __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int tiles, int n, int mbase, int parity,
                           int ipt) {
-    const int T = B * ipt;  // positions of this tile (ipt <= kPlocIpt)
+    const int T = B * ipt;  // positions of this tile (ipt <= ploc_ipt_max(B))
     const int r = P.radius;
     const int s0 = tile * T;
     const int w0 = max(s0 - 2 * r, 0), w1 = min(s0 + T + 2 * r, n);
@@ -593,11 +594,11 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     nn_search_sym<B>(s.lo, s.hi, w0, n, q0, q1, r, s.nn, s.key);
     __syncthreads();
 
-    // ---- merge decisions (blocked: kPlocIpt consecutive positions per thread) ----------------------
+    // ---- merge decisions (blocked: ipt consecutive positions per thread) ---------------------------
     const int ib = s0 + threadIdx.x * ipt;
     uint32_t keep_bits = 0, merge_bits = 0;
 #pragma unroll
-    for (int k = 0; k < kPlocIpt; ++k) {
+    for (int k = 0; k < ploc_ipt_max(B); ++k) {
         int i = ib + k;
         if (k >= ipt || i >= n) break;
         int j = s.nn[i - q0];
@@ -660,7 +661,7 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     uint32_t mpos = (uint32_t)mbase + merged_before + (excl >> 16);
     const int max_internal = P.num_leaves - P.num_meshes;
 #pragma unroll
-    for (int k = 0; k < kPlocIpt; ++k) {
+    for (int k = 0; k < ploc_ipt_max(B); ++k) {
         if (!((keep_bits >> k) & 1u)) continue;  // also 0 for k >= ipt
         const int i = ib + k, ii = i - w0;
         float4 oa = s.lo[ii], ob = s.hi[ii];
@@ -710,7 +711,7 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
         // Items per thread shrink with the cluster count so that small iterations still spread over many
         // SMs; the same rule in every block.
         const long long cap = (long long)B * gridDim.x;
-        const int ipt = min(kPlocIpt, n >= 4 * cap ? 4 : (n >= 2 * cap ? 2 : 1));
+        const int ipt = min(ploc_ipt_max(B), n >= 4 * cap ? 4 : (n >= 2 * cap ? 2 : 1));
         const int T = B * ipt;
         const int tiles = (n + T - 1) / T;
         // The set of active blocks only shrinks: a block that leaves never comes back, and the barrier
@@ -1337,11 +1338,11 @@ __global__ void roots_kernel(LayoutParams P, const float4* __restrict__ lo0, con
     roots[k] = ri;
 }
 
-// Automatic choice: 512 threads x 2 positions, tiles of 1024 positions at 3 resident CTAs per SM (measured
-// fastest with kPlocIpt = 2: 1.59 ms on the 1M sphere against 1.64 ms with 256 threads).
-int ploc_block_for(int requested) {
+// Automatic choice by size: 512 threads x up to 2 positions below 2M triangles (1M sphere: 1.58 ms against 1.65
+// ms with 256 x 4), 256 x up to 4 above (16M EMC60 soup: 16.3 ms against 18.9 ms with 512 x 2).
+int ploc_block_for(int requested, int64_t n) {
     if (requested == 128 || requested == 256 || requested == 512) return requested;
-    return 512;
+    return n < (int64_t(1) << 21) ? 512 : 256;
 }
 
 template <int B>
@@ -1599,8 +1600,8 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
         (st = W.alloc(&P.tbox, 2 * N)) != DIPL_OK ||
         (st = W.alloc(&P.sort_scratch, radix_sort_scratch_bytes(N, 0, P.key_bits, P.digit_bits))) != DIPL_OK)
         return st;
-    P.B = ploc_block_for(d0.ploc_block_size);
-    P.tiles0 = (int)((N + P.B * kPlocIpt - 1) / (P.B * kPlocIpt));
+    P.B = ploc_block_for(d0.ploc_block_size, (int64_t)N);
+    P.tiles0 = (int)((N + P.B * ploc_ipt_max(P.B) - 1) / (P.B * ploc_ipt_max(P.B)));
     P.tiles_max = (int)((N + P.B - 1) / P.B);
     if ((st = W.alloc(&P.d_ctrl, 1)) != DIPL_OK || (st = O.alloc(&P.child, Kalloc)) != DIPL_OK ||
         (st = O.alloc(&P.nlo, Kalloc)) != DIPL_OK || (st = O.alloc(&P.nhi, Kalloc)) != DIPL_OK ||
