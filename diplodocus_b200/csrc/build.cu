@@ -684,7 +684,7 @@ __device__ void ploc_tile(const PlocParams& P, PlocSmem<B>& s, int tile, int til
     }
 }
 
-// Every PLOC iteration while more than kTailMax clusters remain, in one cooperative launch. Iterations are
+// Every PLOC iteration while more than P.grid_stop clusters remain, in one cooperative launch. Iterations are
 // separated by a grid barrier over the blocks that still have tiles.
 template <int B>
 __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
@@ -936,7 +936,7 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     int n = (int)P.ctrl->n[iter & 1];
     int mbase = (int)P.ctrl->merges[iter & 1];
     if (err0 || n <= P.num_meshes) return;
-    if (n > kTailMax) {  // cannot happen: the grid kernel runs until n <= kTailMax
+    if (n > kTailMax) {  // cannot happen: the grid kernel and the middle phase run until n <= kTailMax
         if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
         return;
     }
