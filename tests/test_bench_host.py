@@ -53,3 +53,21 @@ def test_reference_arm_other_ranks_exit_without_work():
                         "--warmup", "0"], capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_obj_scene_workload_round_trips_the_sphere(tmp_path):
+    """The obj_scene workload's files hold the 1M displaced sphere exactly: loaded back by the library's scene
+    loader, its triangles are the sphere workload's bit for bit (after the floor and lamp quads), the lamp is
+    an area light and the camera comes from the .meta file."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    from diplodocus_b200 import scene_io as SI
+    from diplodocus_b200 import scenes as S
+    name, n, size = bench.write_obj_scene(str(tmp_path))
+    sc = SI.load_obj_scene(str(tmp_path), name)
+    tris, _ = S.displaced_sphere(n_rays=16)
+    assert len(sc) == n == len(tris) + 4
+    np.testing.assert_array_equal(sc.triangles()[4:].view(np.uint32), tris.view(np.uint32))
+    assert [a.triangle_id for a in sc.area_lights] == [2, 3]
+    assert sc.camera.fov == np.float32(0.9) and len(sc.point_lights) == 1
