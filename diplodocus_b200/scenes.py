@@ -33,6 +33,7 @@ The workloads:
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
@@ -246,7 +247,11 @@ def sphere_inward_rays(n, seed, radius=3.0):
 
 def random_rays(n, seed, lo=0.0, hi=1.0):
     """Origins uniform in [lo, hi]^3, directions uniform on the sphere, t_max = kInfinity."""
-    idx = np.arange(n, dtype=np.uint64)
+    return _by_index_ranges(n, lambda a, b: _random_rays_range(a, b, seed, lo, hi), (8,), np.float32)
+
+
+def _random_rays_range(first, last, seed, lo, hi):
+    idx = np.arange(first, last, dtype=np.uint64)
     o = lo + (hi - lo) * np.stack([rand01(seed, _S_RAY_O, idx, k) for k in range(3)], axis=1)
     z = 1.0 - 2.0 * rand01(seed, _S_RAY_D, idx, 0)
     a = 2.0 * np.pi * rand01(seed, _S_RAY_D, idx, 1)
@@ -325,9 +330,33 @@ def displaced_sphere(seed=2, nu=1024, nv=512, n_rays=4 * 1024 * 1024):
     return tris, rays
 
 
-def soup(n, seed=3, skinny_frac=0.2, mu=-6.0, sigma=1.5):
-    """Triangle soup: centroids U[0,1]^3, log-normal edge lengths, ``skinny_frac`` of 1:50 aspect, random rotation."""
-    idx = np.arange(n, dtype=np.uint64)
+def _by_index_ranges(n, make, shape, dtype, threads=None, chunk=1 << 20):
+    """Fills an (n, *shape) array with make(lo, hi) over index ranges on host threads. Generators whose records
+    depend only on their index give the same array for any split; numpy releases the interpreter lock inside its
+    loops, so large workloads are made in parallel."""
+    if n <= chunk:
+        return make(0, n)
+    from concurrent.futures import ThreadPoolExecutor
+    out = np.empty((n, *shape), dtype)
+
+    def part(lo):
+        out[lo:min(n, lo + chunk)] = make(lo, min(n, lo + chunk))
+
+    with ThreadPoolExecutor(max_workers=threads or min(32, os.cpu_count() or 1)) as ex:
+        list(ex.map(part, range(0, n, chunk)))
+    return out
+
+
+def soup(n, seed=3, skinny_frac=0.2, mu=-6.0, sigma=1.5, threads=None):
+    """Triangle soup: centroids U[0,1]^3, log-normal edge lengths, ``skinny_frac`` of 1:50 aspect, random rotation.
+    Triangle i depends only on i, so ``soup(n)[:k]`` equals ``soup(k)``."""
+    return _by_index_ranges(n, lambda lo, hi: _soup_range(lo, hi, seed, skinny_frac, mu, sigma), (3, 3),
+                            np.float32, threads)
+
+
+def _soup_range(lo, hi, seed, skinny_frac, mu, sigma):
+    n = hi - lo
+    idx = np.arange(lo, hi, dtype=np.uint64)
     c = np.stack([rand01(seed, _S_SOUP, idx, k) for k in range(3)], axis=1)
     ell = np.exp(mu + sigma * randn(seed, _S_SOUP, idx, 3))
     skinny = rand01(seed, _S_SOUP, idx, 8) < skinny_frac

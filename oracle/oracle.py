@@ -21,7 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libref_oracle.so")
 ORC_LIB = os.path.join(HERE, "libdipl_oracle.so")
-REFERENCE_TREE = "/root/reference"
+# where the reference tree is compiled from (the reference harness is built only where it exists)
+REFERENCE_TREE = os.environ.get("DIPL_REFERENCE_TREE", "/root/reference")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -81,6 +82,8 @@ class RefOracle:
         L.ref_sbvh_sah_cost.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.ref_brute_trace.argtypes = [_f32p, C.c_int64, _f32p, C.c_int64, _i32p, _f32p, _f32p, _f32p, C.c_int,
                                       C.c_int]
+        L.ref_brute_trace_chunked.argtypes = [_f32p, C.c_int64, _f32p, C.c_int64, _i32p, _f32p, _f32p, _f32p,
+                                              C.c_int, C.c_int, C.c_int64]
         L.ref_intersect_one.restype = C.c_float
         L.ref_intersect_one.argtypes = [_f32p, _f32p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.ref_obj_scene_load.restype = C.c_void_p
@@ -148,11 +151,17 @@ class RefOracle:
             tmp.seek(0)
             return tmp.read().decode()
 
-    def brute(self, tris, rays, backface=False, threads=None):
+    def brute(self, tris, rays, backface=False, threads=None, chunk=None):
+        """DummyAccelerationStucture::Intersect on every ray. With ``chunk``, the same comparisons run chunk by chunk
+        of the triangles (ref_brute_trace_chunked: identical records, far fewer cache misses on large scenes)."""
         tris, rays = _tris(tris), _rays(rays)
         h = Hits(len(rays))
-        self.lib.ref_brute_trace(tris, len(tris), rays, len(rays), h.prim, h.t, h.u, h.v, int(backface),
-                                 int(threads or os.cpu_count() or 1))
+        nt = int(threads or os.cpu_count() or 1)
+        if chunk:
+            self.lib.ref_brute_trace_chunked(tris, len(tris), rays, len(rays), h.prim, h.t, h.u, h.v, int(backface),
+                                             nt, int(chunk))
+        else:
+            self.lib.ref_brute_trace(tris, len(tris), rays, len(rays), h.prim, h.t, h.u, h.v, int(backface), nt)
         return h
 
 
@@ -218,6 +227,10 @@ class Oracle:
         L.orc_test_pairs.argtypes = [_f32p, _f32p, C.c_int64, _i32p, C.c_int, C.c_int, _f32p, _f32p, _f32p]
         L.orc_ploc.restype = C.c_int64
         L.orc_ploc.argtypes = [_f32p, C.c_int64, _i32p, C.c_void_p, C.c_int64, C.c_int, _i32p, _f32p, _i32p]
+        L.orc_hploc.restype = C.c_int64
+        L.orc_hploc.argtypes = [_f32p, C.c_int64, _i32p, _u64p, C.c_void_p, C.c_int, C.c_int, _i32p, _f32p, _i32p]
+        L.orc_retrace_binary.argtypes = [_f32p, C.c_int64, _f32p, C.c_int32, _f32p, C.c_int64, C.c_int, _i64p, _i64p,
+                                         _u8p, _i32p, _f32p]
         L.orc_pinhole_rays.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
         L.orc_bounce_rays.argtypes = [_f32p, _f32p, _i32p, _f32p, C.c_int64, C.c_uint32, _f32p]
 
@@ -305,6 +318,39 @@ class Oracle:
         self.lib.orc_emc60_plan(cmin, cmax, diag, bits, masks)
         return bits, masks
 
+    def hploc(self, tris, perm, sorted_keys, radius=16, seg=None, threshold=16):
+        """Hierarchical PLOC over the radix tree of the sorted keys (orc_hploc). Returns (children (n-1, 2) int32,
+        boxes (n-1, 6) float32, iterations): row k is internal node id n + k; rows of the splits between segments
+        stay unused (-1 children)."""
+        tris = _tris(tris)
+        perm = np.ascontiguousarray(perm, np.int32)
+        keys = np.ascontiguousarray(sorted_keys).astype(np.uint64)
+        n = len(tris)
+        rows = max(n - 1, 1)
+        children = np.full(2 * rows, -1, np.int32)
+        boxes = np.zeros(6 * rows, np.float32)
+        it = np.zeros(1, np.int32)
+        seg_arr = None if seg is None else np.ascontiguousarray(seg, np.int32)
+        segp = None if seg_arr is None else seg_arr.ctypes.data_as(C.c_void_p)
+        k = self.lib.orc_hploc(tris, n, perm, keys, segp, int(radius), int(threshold), children, boxes, it)
+        if k < 0:
+            raise ValueError("orc_hploc: bad input")
+        return children[: 2 * (n - 1)].reshape(-1, 2), boxes[: 6 * (n - 1)].reshape(-1, 6), int(it[0])
+
+    def retrace_binary(self, nodes, tris, root, rays, backface=False):
+        """Re-traversal of a downloaded binary layout (orc_retrace_binary): per ray (visits, tests, stable, prim, t).
+        ``nodes`` are the layout's bytes (64 per node), ``tris`` its leaf triangles (N, 3, 4) float32."""
+        nodes = np.ascontiguousarray(np.frombuffer(np.ascontiguousarray(nodes).tobytes(), np.float32))
+        tris = np.ascontiguousarray(tris, np.float32).reshape(-1)
+        rays = _rays(rays)
+        n = len(rays)
+        visits, tests = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        stable = np.zeros(n, np.uint8)
+        prim, t = np.zeros(n, np.int32), np.zeros(n, np.float32)
+        self.lib.orc_retrace_binary(nodes, len(nodes) // 16, tris, int(root), rays, n, int(backface), visits, tests,
+                                    stable, prim, t)
+        return visits, tests, stable.astype(bool), prim, t
+
     def ploc(self, tris, perm, radius=16, seg=None, nseg=1):
         """Returns (children (K,2) int32, boxes (K,6) float32, iterations)."""
         tris = _tris(tris)
@@ -322,6 +368,30 @@ class Oracle:
         return children[: 2 * k].reshape(-1, 2), boxes[: 6 * k].reshape(-1, 6), int(it[0])
 
 
+def classify_hits(prim, t, u, v, brute, sbvh=None):
+    """Agreement classes of GPU closest hits (ref_mt leaf test) against the reference's brute force and SBvh.
+
+    Against brute force: E = id, t, u and v bit-equal; T = a different id at a bit-equal t (an exact tie broken
+    another way); F = anything else. Against SBvh (optional): same = equal id; S = SBvh differs, the GPU record
+    is brute force's (E) and SBvh's t is not nearer (SBvh missed, took a farther hit or broke a tie by traversal
+    order: its bounds are not conservative); F = any other difference."""
+    def b(a):
+        return np.ascontiguousarray(a, np.float32).view(np.uint32)
+    prim = np.asarray(prim)
+    same_id = prim == brute.prim
+    same_t = b(t) == b(brute.t)
+    exact = same_id & same_t & (b(u) == b(brute.u)) & (b(v) == b(brute.v))
+    tie = ~same_id & same_t & (prim >= 0)
+    out = {"rays": int(len(prim)), "E": int(exact.sum()), "T": int(tie.sum()), "F": int((~exact & ~tie).sum())}
+    if sbvh is not None:
+        diff = prim != sbvh.prim
+        sb_t = np.where(sbvh.prim >= 0, sbvh.t, np.inf)
+        gt = np.where(prim >= 0, np.asarray(t, np.float32), np.inf)
+        s_cls = diff & exact & (sb_t >= gt)
+        out["vs_sbvh"] = {"same_id": int((~diff).sum()), "S": int(s_cls.sum()), "F": int((diff & ~s_cls).sum())}
+    return out
+
+
 def sort_perm(codes, seg=None):
     """Stable order of the codes (ties keep triangle order), optionally by (segment, code)."""
     if seg is None:
@@ -330,22 +400,32 @@ def sort_perm(codes, seg=None):
 
 
 def sah_cost_binary(children, boxes, n_leaves, leaf_boxes, max_leaf_exclusive=4):
-    """FP64 SAH cost of a PLOC tree after the leaf rule "a node with < L triangles is a leaf"."""
+    """FP64 SAH cost of a clustering tree after the leaf rule "a node with < L triangles is a leaf". Row k of
+    children/boxes is internal node n_leaves + k (rows with children -1 are unused); the root is the one node that
+    is nobody's child."""
     k = len(children)
     if n_leaves == 1:
         return 1.0
-    count = np.zeros(k, np.int64)
-    for i in range(k):  # children are created before parents
-        c = 0
-        for ch in children[i]:
-            c += 1 if ch < n_leaves else count[ch - n_leaves]
-        count[i] = c
+    used = children[:, 0] >= 0
+    is_child = np.zeros(n_leaves + k, bool)
+    is_child[children[used].ravel()] = True
+    roots = [n_leaves + i for i in np.nonzero(used)[0] if not is_child[n_leaves + i]]
+    assert len(roots) == 1, roots
+    root = roots[0]
+    order, stack = [], [root]
+    while stack:  # parents before children
+        x = stack.pop()
+        order.append(x)
+        if x >= n_leaves:
+            stack.extend(children[x - n_leaves].tolist())
+    count = np.zeros(n_leaves + k, np.int64)
+    for x in reversed(order):
+        count[x] = 1 if x < n_leaves else count[children[x - n_leaves][0]] + count[children[x - n_leaves][1]]
 
     def sa(b):
         d = b[3:6].astype(np.float64) - b[0:3].astype(np.float64)
         return 2.0 * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0])
 
-    root = n_leaves + k - 1
     total = 0.0
     stack = [root]
     while stack:
@@ -353,10 +433,10 @@ def sah_cost_binary(children, boxes, n_leaves, leaf_boxes, max_leaf_exclusive=4)
         if x < n_leaves:
             total += sa(leaf_boxes[x])
             continue
-        i = x - n_leaves
-        if count[i] < max_leaf_exclusive:
-            total += sa(boxes[i]) * count[i]
+        b = boxes[x - n_leaves]
+        if count[x] < max_leaf_exclusive:
+            total += sa(b) * count[x]
             continue
-        total += sa(boxes[i])
-        stack.extend(children[i].tolist())
+        total += sa(b)
+        stack.extend(children[x - n_leaves].tolist())
     return total / sa(boxes[root - n_leaves])

@@ -208,6 +208,52 @@ void ref_brute_trace(const float* tris, int64_t n, const float* rays, int64_t nr
     TraceWith(dummy, rays, nrays, prim, t, u, v, backface, nthreads, nullptr);
 }
 
+// The same brute force over large scenes, with the triangles cut into consecutive chunks of `chunk` triangles so
+// that one chunk stays in the host's cache while a thread's rays run over it. For each chunk, in ascending order,
+// the reference's DummyAccelerationStucture::Intersect runs over the chunk with the ray's t_max lowered to the best
+// t found so far. Its loop starts from t_hit = ray.t_max and keeps t > kEpsilon && t < t_hit
+// (dummy_acceleration_structure.cc:24-41), so the chunked pass makes exactly the comparisons of one pass over all
+// triangles: the same id, t, b1 and b2, exact-t ties kept by the lowest id. Only the loop order differs.
+void ref_brute_trace_chunked(const float* tris, int64_t n, const float* rays, int64_t nrays, int32_t* prim, float* t,
+                             float* u, float* v, int backface, int nthreads, int64_t chunk) {
+    Logger::init(Logger::LogLevel::Error);
+    if (chunk <= 0) chunk = 8192;
+    std::vector<Triangle> tv = MakeTriangles(tris, n);
+    const int64_t nchunks = (n + chunk - 1) / chunk;
+    std::vector<DummyAccelerationStucture> parts(static_cast<size_t>(nchunks));
+    AccelerationStructureConfig cfg;
+    Stats st;
+    for (int64_t c = 0; c < nchunks; ++c) {
+        const int64_t b = c * chunk, len = std::min(chunk, n - b);
+        parts[c].Build(cfg, st, std::span<const Triangle>(tv.data() + b, static_cast<size_t>(len)));
+    }
+    ParallelFor(nrays, nthreads, [&](int64_t b, int64_t e, int) {
+        Stats s;
+        std::vector<Ray> rs;
+        rs.reserve(static_cast<size_t>(e - b));
+        for (int64_t i = b; i < e; ++i) {
+            rs.push_back(MakeRay(rays + 8 * i));
+            prim[i] = -1;
+            t[i] = INFINITY;
+            u[i] = 0.0f;
+            v[i] = 0.0f;
+        }
+        for (int64_t c = 0; c < nchunks; ++c) {
+            for (int64_t i = b; i < e; ++i) {
+                Ray& ray = rs[static_cast<size_t>(i - b)];
+                RayHit hit;
+                if (parts[c].Intersect(s, ray, hit, backface != 0)) {
+                    prim[i] = static_cast<int32_t>(c * chunk + hit.triangle_id);
+                    t[i] = hit.t;
+                    u[i] = hit.b1;
+                    v[i] = hit.b2;
+                    ray.t_max = hit.t;  // the next chunk starts from the best t so far
+                }
+            }
+        }
+    });
+}
+
 // One reference Moller-Trumbore test (triangle.cc:10-43), returning t (kInfinity on a miss).
 float ref_intersect_one(const float* tri9, const float* ray8, int backface, float* b1, float* b2) {
     std::vector<Triangle> tv = MakeTriangles(tri9, 1);

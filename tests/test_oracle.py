@@ -123,3 +123,60 @@ def test_sah_cost_single_leaf_and_pair():
     assert O.sah_cost_binary(children, boxes, 2, leaf_boxes, 4) == pytest.approx(2.0)
     # with L=2 the root is inner: 1 + 2 * SA(face)/SA(cube) = 1 + 2 * 2/6
     assert O.sah_cost_binary(children, boxes, 2, leaf_boxes, 2) == pytest.approx(1 + 2 * 2 / 6)
+
+
+def test_chunked_reference_brute_force_equals_one_pass(ref):
+    """The chunked brute force (used on large scenes) makes the comparisons of DummyAccelerationStucture::Intersect
+    over all triangles: bit-identical records, including exact-t ties across chunk boundaries."""
+    from diplodocus_b200 import scenes as S
+    g = load_golden("duplicates_ties")
+    for tris, rays in ((S.soup(30000, seed=7), S.random_rays(700, seed=7)), (g["tris"], g["rays"])):
+        a = ref.brute(tris, rays)
+        for chunk in (1, 7, 1000):
+            b = ref.brute(tris, rays, chunk=chunk)
+            for k in ("prim", "t", "u", "v"):
+                np.testing.assert_array_equal(np.asarray(getattr(a, k)).view(np.uint32),
+                                              np.asarray(getattr(b, k)).view(np.uint32))
+
+
+@pytest.mark.parametrize("n", [2, 3, 7, 15, 16])
+def test_hierarchical_clustering_equals_ploc_on_one_node(orc, n):
+    """Up to 16 triangles no radix-tree node below the root is large enough to merge, so the root holds every leaf
+    in position order, its pool is every split's id in order, and it runs global PLOC on that list: the same
+    children, boxes and node ids as orc_ploc."""
+    import oracle as O
+    tris = S.soup(n, seed=40 + n)
+    codes = orc.morton30(tris)
+    perm = O.sort_perm(codes)
+    ch_p, bx_p, _ = orc.ploc(tris, perm)
+    ch_h, bx_h, _ = orc.hploc(tris, perm, codes[perm])
+    np.testing.assert_array_equal(ch_h, ch_p)
+    np.testing.assert_array_equal(bx_h.view(np.uint32), bx_p.view(np.uint32))
+
+
+@pytest.mark.parametrize("n,nseg", [(1000, 1), (5000, 1), (3000, 5)])
+def test_hierarchical_clustering_makes_one_binary_tree_per_segment(orc, n, nseg):
+    """Every leaf has exactly one parent, each segment has one root, node ids are the splits inside segments
+    (each used once), and a node's box is the union of its children's."""
+    import oracle as O
+    tris = S.soup(n, seed=n)
+    codes = orc.morton30(tris).astype(np.uint64)
+    seg = np.sort(np.random.default_rng(n).integers(0, nseg, n)).astype(np.int32)
+    perm = np.lexsort((codes, seg)).astype(np.int32)
+    sorted_keys = (seg.astype(np.uint64) << np.uint64(32)) | codes[perm]  # seg is per sorted position
+    ch, bx, _ = orc.hploc(tris, perm, sorted_keys, seg=seg)
+    used = ch[:, 0] >= 0
+    boundary = np.nonzero(seg[1:] != seg[:-1])[0]
+    assert not used[boundary].any() and used.sum() == n - nseg
+    kids = ch[used].ravel()
+    assert len(np.unique(kids)) == len(kids)
+    roots = set(n + np.nonzero(used)[0]) - set(kids.tolist())
+    assert len(roots) + (np.bincount(seg) == 1).sum() == nseg
+    leaf_lo = tris[perm].min(axis=1)
+    leaf_hi = tris[perm].max(axis=1)
+    lo = lambda x: leaf_lo[x] if x < n else bx[x - n, :3]
+    hi = lambda x: leaf_hi[x] if x < n else bx[x - n, 3:]
+    for k in np.nonzero(used)[0]:
+        a, b = ch[k]
+        np.testing.assert_array_equal(bx[k, :3], np.minimum(lo(a), lo(b)))
+        np.testing.assert_array_equal(bx[k, 3:], np.maximum(hi(a), hi(b)))
