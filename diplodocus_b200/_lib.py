@@ -20,7 +20,9 @@ CODE_MORTON30, CODE_EMC60 = 0, 1
 BV_AABB, BV_SOBB = 0, 1
 LAYOUT_BINARY, LAYOUT_WIDE8_Q8 = 0, 1
 LEAF_REF_MT, LEAF_WATERTIGHT = 0, 1
+CLUSTER_HPLOC, CLUSTER_PLOC = 0, 1
 TRACE_BACKFACE_CULLING = 1
+TRACE_KEEP_ORDER = 2
 
 # Every entry point include/dipl_bvh.h declares.
 EXPORTS = [
@@ -33,7 +35,7 @@ EXPORTS = [
     "dipl_generate_pinhole_rays", "dipl_generate_bounce_rays", "dipl_selftest_bounded_waits",
     "dipl_obj_scene_load", "dipl_obj_scene_get_info", "dipl_obj_scene_get_triangles", "dipl_obj_scene_get_soa",
     "dipl_obj_scene_get_materials", "dipl_obj_scene_get_lights", "dipl_obj_scene_destroy",
-    "dipl_status_string",
+    "dipl_set_limits", "dipl_get_limits", "dipl_status_string",
     "dipl_last_error", "dipl_abi_version", "dipl_kernel_launch_count",
 ]
 
@@ -42,7 +44,8 @@ class BuildDesc(C.Structure):
     _fields_ = [("d_v0", C.c_void_p), ("d_v1", C.c_void_p), ("d_v2", C.c_void_p), ("num_triangles", C.c_int64),
                 ("code_type", C.c_int32), ("bv_type", C.c_int32), ("layout", C.c_int32),
                 ("max_triangles_per_leaf", C.c_int32), ("nn_search_radius", C.c_int32), ("kdop_size", C.c_int32),
-                ("ploc_block_size", C.c_int32), ("sort_digit_bits", C.c_int32)]
+                ("ploc_block_size", C.c_int32), ("sort_digit_bits", C.c_int32), ("clustering", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class BvhInfo(C.Structure):
@@ -50,7 +53,12 @@ class BvhInfo(C.Structure):
                 ("node_bytes", C.c_int64), ("triangle_bytes", C.c_int64), ("depth", C.c_int32),
                 ("ploc_iterations", C.c_int32), ("code_type", C.c_int32), ("bv_type", C.c_int32),
                 ("layout", C.c_int32), ("max_triangles_per_leaf", C.c_int32), ("nn_search_radius", C.c_int32),
-                ("kdop_size", C.c_int32)]
+                ("kdop_size", C.c_int32), ("clustering", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Limits(C.Structure):
+    _fields_ = [("device_memory_bytes", C.c_uint64), ("clustering_iterations", C.c_uint32),
+                ("trace_steps", C.c_uint32)]
 
 
 class ObjSceneInfo(C.Structure):
@@ -115,6 +123,8 @@ def load(path: str = LIB_PATH):
         "dipl_obj_scene_get_materials": (i32, [vp, vp, vp]),
         "dipl_obj_scene_get_lights": (i32, [vp, vp, vp, vp, vp]),
         "dipl_obj_scene_destroy": (None, [vp]),
+        "dipl_set_limits": (i32, [C.POINTER(Limits)]),
+        "dipl_get_limits": (i32, [C.POINTER(Limits), C.POINTER(C.c_uint64)]),
         "dipl_status_string": (C.c_char_p, [i32]),
         "dipl_last_error": (C.c_char_p, []),
         "dipl_abi_version": (i32, []),
@@ -138,3 +148,16 @@ def default_desc() -> BuildDesc:
     d = BuildDesc()
     load().dipl_build_desc_init(C.byref(d))
     return d
+
+
+def get_limits():
+    """(Limits, device bytes the library holds now)."""
+    lim, used = Limits(), C.c_uint64(0)
+    check(load().dipl_get_limits(C.byref(lim), C.byref(used)), "dipl_get_limits")
+    return lim, used.value
+
+
+def set_limits(device_memory_bytes=0, clustering_iterations=0, trace_steps=0):
+    """Process-wide limits (dipl_set_limits); all zero restores the defaults."""
+    lim = Limits(int(device_memory_bytes), int(clustering_iterations), int(trace_steps))
+    check(load().dipl_set_limits(C.byref(lim)), "dipl_set_limits")

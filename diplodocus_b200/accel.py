@@ -67,6 +67,7 @@ class AccelerationStructureConfig:
     leaf_test: str = "ref_mt"           # "ref_mt" | "watertight"
     ploc_block_size: int = 0
     sort_digit_bits: int = 0
+    clustering: str = "hploc"           # "hploc" (hierarchical, default) | "ploc" (global iterations)
 
 
 @dataclass
@@ -161,6 +162,7 @@ def make_desc(v0, v1, v2, config: AccelerationStructureConfig) -> L.BuildDesc:
     d.kdop_size = config.kdop_size
     d.ploc_block_size = config.ploc_block_size
     d.sort_digit_bits = config.sort_digit_bits
+    d.clustering = {"hploc": L.CLUSTER_HPLOC, "ploc": L.CLUSTER_PLOC}[config.clustering]
     return d
 
 
@@ -202,11 +204,13 @@ class GpuPlocBvh:
 
     # -- AccelerationStructure::Intersect (batched) ---------------------------------------------------
     def Intersect(self, stats: Stats, rays, backface_culling: bool = False, leaf_test: str | None = None,
-                  count: bool = False) -> Hits:
+                  count: bool = False, keep_order: bool = False) -> Hits:
+        """Closest hits of a ray batch. Large batches are traced in a coherent order chosen on the device unless
+        ``keep_order``; the records are the same either way."""
         rays = as_device_rays(rays)
         n = rays.shape[0]
         raw = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
-        flags = L.TRACE_BACKFACE_CULLING if backface_culling else 0
+        flags = (L.TRACE_BACKFACE_CULLING if backface_culling else 0) | (L.TRACE_KEEP_ORDER if keep_order else 0)
         lt = _leaf_test(leaf_test or self.config.leaf_test)
         if count:
             ctr = torch.zeros(2, dtype=torch.int64, device=rays.device)

@@ -4,6 +4,7 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 
 #include "internal.h"
 
@@ -23,28 +24,62 @@ dipl_status cuda_status(cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? DIPL_ERR_OUT_OF_MEMORY : DIPL_ERR_CUDA;
 }
 
-static std::once_flag g_pool_once;
+// ---- process-wide limits (dipl_set_limits) -----------------------------------------------------------
+static std::atomic<uint64_t> g_mem_limit{0};
+static std::atomic<uint32_t> g_clustering_iterations{0};
+static std::atomic<uint32_t> g_trace_steps{0};
+static std::mutex g_mem_mu;
+static uint64_t g_mem_in_use = 0;                    // bytes of live device allocations (under g_mem_mu)
+static std::unordered_map<void*, size_t> g_mem_sizes;  // live allocation -> bytes (under g_mem_mu)
+
+uint32_t clustering_iteration_limit() { return g_clustering_iterations.load(std::memory_order_relaxed); }
+uint32_t trace_step_limit() { return g_trace_steps.load(std::memory_order_relaxed); }
+
+static DeviceProbe g_pool_configured;  // per device: each device has its own default pool
 
 dipl_status device_alloc(void** ptr, size_t bytes, cudaStream_t stream) {
-    std::call_once(g_pool_once, [] {
+    {
+        std::lock_guard<std::mutex> lock(g_mem_mu);
+        const uint64_t limit = g_mem_limit.load(std::memory_order_relaxed);
+        if (limit != 0 && g_mem_in_use + bytes > limit) {
+            *ptr = nullptr;
+            set_last_error("device memory limit of " + std::to_string(limit) + " bytes reached (" +
+                           std::to_string(g_mem_in_use) + " in use, " + std::to_string(bytes) + " requested)");
+            return DIPL_ERR_OUT_OF_MEMORY;
+        }
+        g_mem_in_use += bytes;  // reserved before the allocation, so concurrent callers cannot both pass the cap
+    }
+    probe_per_device(g_pool_configured, [] {
         int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess) return;
+        if (cudaGetDevice(&dev) != cudaSuccess) return 0;
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
             uint64_t threshold = ~0ull;  // keep freed blocks for reuse: builds allocate the same sizes repeatedly
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
         }
+        (void)cudaGetLastError();
+        return 1;
     });
     cudaError_t e = cudaMallocAsync(ptr, bytes, stream);
+    std::lock_guard<std::mutex> lock(g_mem_mu);
     if (e != cudaSuccess) {
+        g_mem_in_use -= bytes;
         *ptr = nullptr;
         return cuda_status(e, "cudaMallocAsync");
     }
+    g_mem_sizes[*ptr] = bytes;
     return DIPL_OK;
 }
 
 void device_free(void* ptr, cudaStream_t stream) {
-    if (ptr) cudaFreeAsync(ptr, stream);
+    if (!ptr) return;
+    cudaFreeAsync(ptr, stream);
+    std::lock_guard<std::mutex> lock(g_mem_mu);
+    auto it = g_mem_sizes.find(ptr);
+    if (it != g_mem_sizes.end()) {
+        g_mem_in_use -= it->second;
+        g_mem_sizes.erase(it);
+    }
 }
 
 unsigned char* pinned_host_buffer(size_t bytes) {
@@ -100,6 +135,30 @@ extern "C" {
 
 int32_t dipl_abi_version(void) { return DIPL_ABI_VERSION; }
 
+dipl_status dipl_set_limits(const dipl_limits* limits) {
+    if (!limits) {
+        set_last_error("dipl_set_limits: limits must be non-NULL");
+        return DIPL_ERR_INVALID_ARGUMENT;
+    }
+    g_mem_limit.store(limits->device_memory_bytes, std::memory_order_relaxed);
+    g_clustering_iterations.store(limits->clustering_iterations, std::memory_order_relaxed);
+    g_trace_steps.store(limits->trace_steps, std::memory_order_relaxed);
+    return DIPL_OK;
+}
+
+dipl_status dipl_get_limits(dipl_limits* limits, uint64_t* device_memory_in_use) {
+    if (limits) {
+        limits->device_memory_bytes = g_mem_limit.load(std::memory_order_relaxed);
+        limits->clustering_iterations = g_clustering_iterations.load(std::memory_order_relaxed);
+        limits->trace_steps = g_trace_steps.load(std::memory_order_relaxed);
+    }
+    if (device_memory_in_use) {
+        std::lock_guard<std::mutex> lock(g_mem_mu);
+        *device_memory_in_use = g_mem_in_use;
+    }
+    return DIPL_OK;
+}
+
 uint64_t dipl_kernel_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 const char* dipl_last_error(void) { return g_last_error.c_str(); }
@@ -129,6 +188,8 @@ void dipl_build_desc_init(dipl_build_desc* d) {
     d->kdop_size = 32;
     d->ploc_block_size = 0;
     d->sort_digit_bits = 0;
+    d->clustering = DIPL_CLUSTER_HPLOC;
+    d->reserved = 0;
 }
 
 dipl_status dipl_bvh_build(const dipl_build_desc* desc, dipl_bvh** out, void* stream) {
@@ -208,6 +269,7 @@ dipl_status dipl_bvh_get_info(const dipl_bvh* b, dipl_bvh_info* info) {
     info->max_triangles_per_leaf = b->max_leaf;
     info->nn_search_radius = b->radius;
     info->kdop_size = b->kdop;
+    info->clustering = b->clustering;
     return DIPL_OK;
 }
 

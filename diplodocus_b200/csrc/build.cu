@@ -42,7 +42,7 @@ struct PlocCtrl {
     uint32_t n[2];       // cluster count at the start of an iteration (by parity)
     uint32_t merges[2];  // internal nodes created before an iteration (by parity)
     uint32_t iterations;
-    uint32_t pad;
+    uint32_t roots_second;    // 1: the roots are in the second cluster buffer (hierarchical clustering)
     uint32_t tiles_taken[2];  // tiles claimed in an iteration (by parity)
     GridBarrier barrier;
 };
@@ -371,6 +371,7 @@ struct PlocParams {
     int num_meshes;
     int radius;
     int grid_stop;  // ploc_kernel runs while more clusters than this remain (the middle phase's capacity, or kTailMax)
+    uint32_t max_iterations;  // the build gives up (kErrIterations) at this many iterations
 };
 
 // Parity-selected pointers of PlocParams (a select, so the parameter block is never copied to the stack for
@@ -704,7 +705,7 @@ __global__ void __launch_bounds__(B) ploc_kernel(PlocParams P) {
         const bool ok = s.ok != 0;
         __syncthreads();
         if (!ok || n <= P.num_meshes || n <= P.grid_stop) break;
-        if (iter >= kMaxPlocIterations) {
+        if (iter >= P.max_iterations) {
             if (threadIdx.x == 0) atomicOr(P.err, kErrIterations);
             break;
         }
@@ -795,7 +796,7 @@ __global__ void __launch_bounds__(kTailThreads) ploc_mid_kernel(PlocParams P) {
     bool failed = false;
     cluster.sync();  // all CTAs are running before anyone reads a peer's shared memory
     while (n > P.num_meshes && n > kTailMax) {
-        if (iter >= kMaxPlocIterations) {
+        if (iter >= P.max_iterations) {
             if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
             failed = true;
             break;
@@ -957,7 +958,7 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     bool failed = false;
     bool solo = ctas == 1;  // CTA 0 alone: the peers have left the cluster
     while (n > P.num_meshes) {
-        if (iter + tail_iters >= kMaxPlocIterations) {
+        if (iter + tail_iters >= P.max_iterations) {
             if (rank == 0 && threadIdx.x == 0) atomicOr(P.err, kErrIterations);
             failed = true;
             break;
@@ -1087,6 +1088,247 @@ __global__ void __launch_bounds__(kTailThreads) ploc_tail_kernel(PlocParams P) {
     if (threadIdx.x == 0) P.ctrl->iterations = final_iter;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Hierarchical PLOC, after Benthin, Meister, Barczak, Mehalwal, Tsakok and Kensler, "H-PLOC" (HPG 2024): PLOC
+// merging confined to the nodes of the binary radix tree of the sorted keys, bottom up in one launch, with no
+// global iteration and no grid barrier.
+//
+// The radix tree (Apetrei 2014): split s lies between sorted positions s and s+1 with the order key
+// (keys[s] ^ keys[s+1], s ^ (s+1), s), lexicographic; a node [l, r] joins the neighbour across the split with the
+// smaller key (split r if l is its mesh's first position or r is not its mesh's last and key(r) < key(l-1), else
+// split l-1). Mesh bits above the code make every split between meshes larger than any split inside one, so a
+// mesh is a subtree. One thread starts at each leaf; at a split, the first child to arrive leaves its far boundary
+// (atomic exchange) and stops, the second goes on with the union.
+//
+// Each node holds a list of clusters in position order, stored at its first position: a node of at most T
+// positions (T = kHplocThreshold) is its leaves, untouched; a larger one is processed by the whole warp of the
+// thread that reached it: the left child's list then the right child's, one cluster per lane, and PLOC
+// iterations (nearest neighbour by the key of ploc_kernel over list indices within the radius, by warp shuffles;
+// mutual pairs merge into the lower index; ballot compaction) until at most T clusters are left, or one at a
+// mesh's root. Node ids are deterministic: split s of mesh k owns id N + s - k; a list of c clusters carries
+// c - 1 ids not yet used, a node's pool is the left list's unused ids, its own split's id, the right list's;
+// merges take ids from the front of the pool (iteration, then position order) and the rest go up with the list.
+// oracle/dipl_oracle.c orc_hploc restates the whole procedure sequentially.
+// ------------------------------------------------------------------------------------------------
+constexpr int kHplocThreshold = 16;
+constexpr int kHplocThreads = 256;
+constexpr int kHplocMaxSteps = 192;  // tree levels: key bits (<= 64) + index bits (<= 32), with room to spare
+
+struct HplocParams {
+    const void* keys;           // sorted keys (uint32 or uint64)
+    const long long* offsets;   // first sorted position of each mesh (+ the total)
+    float4* lo;                 // cluster records by sorted position: min xyz, node id bits
+    float4* hi;                 //                                     max xyz, mesh index bits
+    int4* info;                 //                                     triangle count, first position, height, 0
+    int4* child;                // internal node k: left, right, height, 0
+    float4* node_lo;            // internal node k: min xyz, triangle count bits
+    float4* node_hi;            // internal node k: max xyz, first sorted position bits
+    int* parent;
+    int* other;                 // per split: the first arriving child's far boundary (-1 before)
+    int* cnt;                   // per first position of a processed node: the length of its list
+    int* fid;                   // per position of a processed node's list: its unused node ids
+    float4* root_lo;            // per mesh: the root cluster (the second cluster buffer)
+    float4* root_hi;
+    PlocCtrl* ctrl;
+    uint32_t* err;
+    int num_leaves;
+    int num_inner;              // internal nodes of all meshes (num_leaves - num_meshes)
+    int num_meshes;
+    int radius;
+    int max_node_iterations;    // iterations within one node before the build gives up (kErrIterations)
+};
+
+template <typename K>
+__device__ __forceinline__ bool split_before(const K* __restrict__ keys, int a, int b) {
+    const K xa = __ldg(keys + a) ^ __ldg(keys + a + 1), xb = __ldg(keys + b) ^ __ldg(keys + b + 1);
+    if (xa != xb) return xa < xb;
+    const unsigned ia = (unsigned)a ^ (unsigned)(a + 1), ib = (unsigned)b ^ (unsigned)(b + 1);
+    if (ia != ib) return ia < ib;
+    return a < b;
+}
+
+__device__ __forceinline__ float4 shfl4(float4 v, int src) {
+    return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                       __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+__device__ __forceinline__ int4 shfl4(int4 v, int src) {
+    return make_int4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                     __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+
+// One node [nl, nr] with split nm, processed by the whole warp (every lane calls this with the same arguments).
+// Returns the PLOC iterations it ran.
+__device__ __forceinline__ int hploc_node(const HplocParams& P, int nl, int nr, int nm, int id_base, bool whole) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int T = kHplocThreshold;
+    const int lsize = nm - nl + 1, rsize = nr - nm;
+    int cl = lsize > T ? __ldcg(P.cnt + nl) : lsize;
+    int cr = rsize > T ? __ldcg(P.cnt + nm + 1) : rsize;
+    if (cl < 1 || cl > T || cr < 1 || cr > T) {  // a processed child left 1..T clusters; never read past a list
+        if (lane == 0) atomicOr(P.err, kErrIterations);
+        cl = min(max(cl, 1), min(lsize, T));
+        cr = min(max(cr, 1), min(rsize, T));
+    }
+    int c = cl + cr;
+    const bool have = lane < c;
+    const int p = lane < cl ? nl + lane : nm + 1 + (lane - cl);
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+    int4 inf = make_int4(0, 0, 0, 0);
+    if (have) {
+        a = __ldcg(P.lo + p);
+        b = __ldcg(P.hi + p);
+        inf = __ldcg(P.info + p);
+    }
+    int pool = -1;  // lane q holds the pool's entry q (c - 1 entries)
+    if (lane < cl - 1) pool = lsize > T ? __ldcg(P.fid + nl + lane) : id_base + nl + lane;
+    else if (lane == cl - 1) pool = id_base + nm;
+    else if (lane < c - 1) {
+        const int j = lane - cl;
+        pool = rsize > T ? __ldcg(P.fid + nm + 1 + j) : id_base + nm + 1 + j;
+    }
+    const int target = whole ? 1 : T;
+    const int R = min(P.radius, 31);
+    int used = 0, iters = 0;
+    while (c > target) {
+        if (iters >= P.max_node_iterations) {
+            if (lane == 0) atomicOr(P.err, kErrIterations);
+            break;
+        }
+        float bestd = __int_as_float(0x7F800000);
+        int bestj = -1;
+        for (int d = 1; d <= R && d < c; ++d) {
+            const float fx = __shfl_down_sync(full, a.x, d), fy = __shfl_down_sync(full, a.y, d);
+            const float fz = __shfl_down_sync(full, a.z, d), gx = __shfl_down_sync(full, b.x, d);
+            const float gy = __shfl_down_sync(full, b.y, d), gz = __shfl_down_sync(full, b.z, d);
+            const bool fwd_ok = lane + d < c;
+            const float df = fwd_ok ? ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, fx, fy, fz, gx, gy, gz)
+                                    : __int_as_float(0x7F800000);
+            const float db = __shfl_up_sync(full, df, d);  // the pair (lane - d, lane), evaluated by lane - d
+            const bool back_ok = lane >= d && lane < c;
+            // equal distances: the candidate with the even lower index first, then the one below (the key's tie
+            // fields after the gap: parity of the lower index, side)
+            if (((lane - d) & 1) <= (lane & 1)) {
+                if (back_ok && (db < bestd || bestj < 0)) bestd = db, bestj = lane - d;
+                if (fwd_ok && (df < bestd || bestj < 0)) bestd = df, bestj = lane + d;
+            } else {
+                if (fwd_ok && (df < bestd || bestj < 0)) bestd = df, bestj = lane + d;
+                if (back_ok && (db < bestd || bestj < 0)) bestd = db, bestj = lane - d;
+            }
+        }
+        const int partner = bestj >= 0 ? bestj : lane;
+        const int nn_of_partner = __shfl_sync(full, bestj, partner);
+        const bool valid = lane < c;
+        const bool mutual = valid && bestj >= 0 && nn_of_partner == lane;
+        const bool creator = mutual && lane < bestj;
+        const float4 pa = shfl4(a, partner), pb = shfl4(b, partner);
+        const int4 pi = shfl4(inf, partner);
+        const unsigned cm = __ballot_sync(full, creator);
+        const int t = __popc(cm & ((1u << lane) - 1u));
+        const int id = __shfl_sync(full, pool, (used + t) & 31);
+        const int k = id - P.num_leaves;
+        const int left = __float_as_int(a.w), right = __float_as_int(pa.w);
+        const bool in_range = k >= 0 && k < P.num_inner && left >= 0 && left < P.num_leaves + P.num_inner &&
+                              right >= 0 && right < P.num_leaves + P.num_inner;
+        if (creator && !in_range) atomicOr(P.err, kErrIterations);  // never write outside the node arrays
+        if (creator && in_range) {
+            const float3 lo = make_float3(fminf(a.x, pa.x), fminf(a.y, pa.y), fminf(a.z, pa.z));
+            const float3 hi = make_float3(fmaxf(b.x, pb.x), fmaxf(b.y, pb.y), fmaxf(b.z, pb.z));
+            const int count = inf.x + pi.x, pmin = min(inf.y, pi.y), height = max(inf.z, pi.z) + 1;
+            P.child[k] = make_int4(left, right, height, 0);
+            P.node_lo[k] = make_float4(lo.x, lo.y, lo.z, __int_as_float(count));
+            P.node_hi[k] = make_float4(hi.x, hi.y, hi.z, __int_as_float(pmin));
+            P.parent[left] = id;
+            P.parent[right] = id;
+            a = make_float4(lo.x, lo.y, lo.z, __int_as_float(id));
+            b = make_float4(hi.x, hi.y, hi.z, b.w);
+            inf = make_int4(count, pmin, height, 0);
+        }
+        used += __popc(cm);
+        const bool keep = valid && !(mutual && lane > bestj);
+        const unsigned km = __ballot_sync(full, keep);
+        const int nc = __popc(km);
+        ++iters;
+        if (nc == c) {  // no pair merged: impossible under a strict order on pairs
+            if (lane == 0) atomicOr(P.err, kErrIterations);
+            break;
+        }
+        const int src = lane < nc ? (int)__fns(km, 0, lane + 1) : lane;
+        a = shfl4(a, src);
+        b = shfl4(b, src);
+        inf = shfl4(inf, src);
+        c = nc;
+    }
+    if (lane < c) {
+        __stcg(P.lo + nl + lane, a);
+        __stcg(P.hi + nl + lane, b);
+        __stcg(P.info + nl + lane, inf);
+    }
+    const int f = __shfl_sync(full, pool, (used + lane) & 31);
+    if (lane < c - 1) __stcg(P.fid + nl + lane, f);
+    if (lane == 0) __stcg(P.cnt + nl, c);
+    return iters;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kHplocThreads) hploc_kernel(HplocParams P) {
+    const unsigned full = 0xffffffffu;
+    const K* __restrict__ keys = static_cast<const K*>(P.keys);
+    const int N = P.num_leaves;
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = pos < N;
+    int l = pos, r = pos, mesh = 0, mstart = 0, mend = N - 1;
+    if (active && P.num_meshes > 1) {
+        mesh = find_mesh(P.offsets, P.num_meshes, pos);
+        mstart = (int)__ldg(P.offsets + mesh);
+        mend = (int)__ldg(P.offsets + mesh + 1) - 1;
+    }
+    const int id_base = N - mesh;
+    int iters = 0;
+    for (int step = 0;; ++step) {
+        bool todo = false;
+        int split = -1;
+        if (active) {
+            if (l == mstart && r == mend) {
+                // this mesh's root, processed by this warp in the previous step (its list is one cluster), or a
+                // one-triangle mesh's leaf: the root goes to the second cluster buffer, where the layout reads it
+                P.root_lo[mesh] = __ldcg(P.lo + mstart);
+                P.root_hi[mesh] = __ldcg(P.hi + mstart);
+                active = false;
+            } else if (step >= kHplocMaxSteps) {
+                active = false;
+                atomicOr(P.err, kErrIterations);
+            } else {
+                const bool left_child = l == mstart || (r != mend && split_before(keys, r, l - 1));
+                split = left_child ? r : l - 1;
+                __threadfence();  // this node's list (written by its warp) before the arrival
+                const int prev = atomicExch(P.other + split, left_child ? l : r);
+                if (prev < 0) {
+                    active = false;  // first to arrive: the sibling's thread goes on
+                } else {
+                    __threadfence();  // the sibling's list before the loads
+                    if (left_child) r = prev;
+                    else l = prev;
+                    todo = (r - l + 1 > kHplocThreshold) || (l == mstart && r == mend);
+                }
+            }
+        }
+        unsigned pending = __ballot_sync(full, todo);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1u;
+            const int nl = __shfl_sync(full, l, src), nr = __shfl_sync(full, r, src);
+            const int nm = __shfl_sync(full, split, src), nbase = __shfl_sync(full, id_base, src);
+            const bool whole = __shfl_sync(full, (int)(l == mstart && r == mend), src) != 0;
+            iters += hploc_node(P, nl, nr, nm, nbase, whole);
+        }
+        __syncwarp();
+        if (!__any_sync(full, active)) break;
+    }
+    // every lane ran the same node iterations: one count per warp
+    if ((threadIdx.x & 31) == 0 && iters) atomicAdd(&P.ctrl->iterations, (uint32_t)iters);
+}
+
 __global__ void ploc_init_kernel(const MeshDesc* __restrict__ meshes, const long long* __restrict__ offsets, int m,
                                  long long n, const uint32_t* __restrict__ perm, const float4* __restrict__ tbox,
                                  float4* __restrict__ lo, float4* __restrict__ hi, int4* __restrict__ info,
@@ -1103,8 +1345,9 @@ __global__ void ploc_init_kernel(const MeshDesc* __restrict__ meshes, const long
     parent[p] = -1;
 }
 
-__global__ void ploc_ctrl_init_kernel(PlocCtrl* ctrl, uint32_t n) {
+__global__ void ploc_ctrl_init_kernel(PlocCtrl* ctrl, uint32_t n, uint32_t roots_second) {
     ctrl->n[0] = n;  // the rest was cleared by a memset
+    ctrl->roots_second = roots_second;
 }
 
 __global__ void fill_int_kernel(int* p, long long n, int v) {
@@ -1317,7 +1560,7 @@ __global__ void roots_kernel(LayoutParams P, const float4* __restrict__ lo0, con
         roots[k] = ri;
         return;
     }
-    const bool odd = (ctrl->iterations & 1u) != 0u;
+    const bool odd = ctrl->roots_second != 0u || (ctrl->iterations & 1u) != 0u;
     const float4* final_lo = odd ? lo1 : lo0;
     const float4* final_hi = odd ? hi1 : hi0;
     int id = __float_as_int(final_lo[k].w);
@@ -1372,30 +1615,29 @@ dipl_status launch_ploc(const PlocParams& P, int initial_tiles, cudaStream_t str
 
 // CTAs of the middle phase: the largest cluster of 16 or 8 CTAs the device schedules with its shared memory, 0
 // without one (then ploc_kernel runs down to kTailMax clusters).
-int ploc_mid_ctas() {
-    static int ctas = -1;
-    if (ctas < 0) {
-        ctas = 0;
-        const size_t smem = sizeof(MidSmem);
-        if (cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-                cudaSuccess &&
-            cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
-            for (int c = kMidCtasMax; c >= 8 && ctas == 0; c /= 2) {
-                cudaLaunchConfig_t cfg = {};
-                cudaLaunchAttribute attr[1];
-                attr[0].id = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = c, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
-                cfg.gridDim = dim3(c), cfg.blockDim = dim3(kTailThreads), cfg.dynamicSmemBytes = smem;
-                cfg.attrs = attr, cfg.numAttrs = 1;
-                int clusters = 0;
-                if (cudaOccupancyMaxActiveClusters(&clusters, ploc_mid_kernel, &cfg) == cudaSuccess && clusters > 0)
-                    ctas = c;
-            }
+int ploc_mid_ctas_probe() {
+    int ctas = 0;
+    const size_t smem = sizeof(MidSmem);
+    if (cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+        cudaFuncSetAttribute(ploc_mid_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        for (int c = kMidCtasMax; c >= 8 && ctas == 0; c /= 2) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = c, attr[0].val.clusterDim.y = 1, attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(c), cfg.blockDim = dim3(kTailThreads), cfg.dynamicSmemBytes = smem;
+            cfg.attrs = attr, cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, ploc_mid_kernel, &cfg) == cudaSuccess && clusters > 0)
+                ctas = c;
         }
-        (void)cudaGetLastError();
     }
+    (void)cudaGetLastError();
     return ctas;
 }
+
+DeviceProbe g_mid_ctas;
+int ploc_mid_ctas() { return probe_per_device(g_mid_ctas, ploc_mid_ctas_probe); }
 
 dipl_status launch_ploc_mid(const PlocParams& P, int ctas, cudaStream_t stream) {
     const size_t smem = sizeof(MidSmem);
@@ -1412,11 +1654,13 @@ dipl_status launch_ploc_mid(const PlocParams& P, int ctas, cudaStream_t stream) 
     return DIPL_OK;
 }
 
+DeviceProbe g_tail_ctas;
+
 dipl_status launch_ploc_tail(const PlocParams& P, cudaStream_t stream) {
     const size_t smem = sizeof(TailSmem);
     DIPL_CUDA(cudaFuncSetAttribute(ploc_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    static int ctas = 0;  // the largest cluster size the device can schedule with this footprint
-    if (ctas == 0) {
+    // the largest cluster size the device can schedule with this footprint
+    const int ctas = probe_per_device(g_tail_ctas, [smem] {
         for (int c = kTailCtasMax; c >= 1; c /= 2) {
             cudaLaunchConfig_t cfg = {};
             cudaLaunchAttribute attr[1];
@@ -1425,14 +1669,12 @@ dipl_status launch_ploc_tail(const PlocParams& P, cudaStream_t stream) {
             cfg.gridDim = dim3(c), cfg.blockDim = dim3(kTailThreads), cfg.dynamicSmemBytes = smem;
             cfg.attrs = attr, cfg.numAttrs = 1;
             int clusters = 0;
-            if (cudaOccupancyMaxActiveClusters(&clusters, ploc_tail_kernel, &cfg) == cudaSuccess && clusters > 0) {
-                ctas = c;
-                break;
-            }
+            if (cudaOccupancyMaxActiveClusters(&clusters, ploc_tail_kernel, &cfg) == cudaSuccess && clusters > 0)
+                return c;
             (void)cudaGetLastError();
         }
-        if (ctas == 0) ctas = 1;
-    }
+        return 1;
+    });
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1471,6 +1713,9 @@ static dipl_status validate_desc(const dipl_build_desc& d) {
     DIPL_CHECK_ARG(d.sort_digit_bits == 0 || d.sort_digit_bits == 6 || d.sort_digit_bits == 7 ||
                        d.sort_digit_bits == 8 || d.sort_digit_bits == 10,
                    "sort_digit_bits must be 0, 6, 7, 8 or 10");
+    DIPL_CHECK_ARG(d.clustering == DIPL_CLUSTER_HPLOC || d.clustering == DIPL_CLUSTER_PLOC,
+                   "clustering must be DIPL_CLUSTER_HPLOC or DIPL_CLUSTER_PLOC");
+    DIPL_CHECK_ARG(d.reserved == 0, "reserved must be 0");
     return DIPL_OK;
 }
 
@@ -1508,6 +1753,7 @@ struct BuildPlan {
     unsigned long long* status = nullptr;
     float4 *c_lo[2] = {nullptr, nullptr}, *c_hi[2] = {nullptr, nullptr};
     int4* c_in[2] = {nullptr, nullptr};
+    int *hp_other = nullptr, *hp_cnt = nullptr, *hp_fid = nullptr;  // hierarchical clustering
     uint32_t *rev_flags = nullptr, *contrib = nullptr, *d_counts = nullptr;
     int *owner_leaf = nullptr, *leaf_start_of = nullptr;
     unsigned char* scan_scratch = nullptr;
@@ -1543,7 +1789,7 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
                            descs[i].layout == d0.layout && descs[i].max_triangles_per_leaf == d0.max_triangles_per_leaf &&
                            descs[i].nn_search_radius == d0.nn_search_radius && descs[i].kdop_size == d0.kdop_size &&
                            descs[i].ploc_block_size == d0.ploc_block_size &&
-                           descs[i].sort_digit_bits == d0.sort_digit_bits,
+                           descs[i].sort_digit_bits == d0.sort_digit_bits && descs[i].clustering == d0.clustering,
                        "batched builds need one set of build options");
     }
     P.descs.assign(descs, descs + count);
@@ -1611,6 +1857,10 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
         if ((st = W.alloc(&P.c_lo[k], N)) != DIPL_OK || (st = W.alloc(&P.c_hi[k], N)) != DIPL_OK ||
             (st = W.alloc(&P.c_in[k], N)) != DIPL_OK)
             return st;
+    if (d0.clustering == DIPL_CLUSTER_HPLOC &&
+        ((st = W.alloc(&P.hp_other, N)) != DIPL_OK || (st = W.alloc(&P.hp_cnt, N)) != DIPL_OK ||
+         (st = W.alloc(&P.hp_fid, N)) != DIPL_OK))
+        return st;
     if ((st = W.alloc(&P.rev_flags, Kalloc)) != DIPL_OK || (st = W.alloc(&P.contrib, N)) != DIPL_OK ||
         (st = W.alloc(&P.owner_leaf, N)) != DIPL_OK || (st = W.alloc(&P.leaf_start_of, N + Kalloc)) != DIPL_OK ||
         (st = W.alloc(&P.scan_scratch, scan_scratch_bytes(std::max(N, Kalloc)))) != DIPL_OK ||
@@ -1683,24 +1933,44 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     // ---- PLOC ------------------------------------------------------------------------------------------
     PlocParams pp{};
     DIPL_CUDA(cudaMemsetAsync(P.d_ctrl, 0, sizeof(PlocCtrl), stream));
-    ploc_ctrl_init_kernel<<<1, 1, 0, stream>>>(P.d_ctrl, (uint32_t)N);
+    const bool hier = d0.clustering == DIPL_CLUSTER_HPLOC;
+    ploc_ctrl_init_kernel<<<1, 1, 0, stream>>>(P.d_ctrl, (uint32_t)N, hier ? 1u : 0u);
     note_launches();
-    DIPL_CUDA(cudaMemsetAsync(P.status, 0, sizeof(unsigned long long) * (2 * P.tiles_max + 2), stream));
+    if (!hier)
+        DIPL_CUDA(cudaMemsetAsync(P.status, 0, sizeof(unsigned long long) * (2 * P.tiles_max + 2), stream));
     fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(P.parent, N + K, -1);
     note_launches();
     ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.perm, P.tbox,
                                                              P.c_lo[0], P.c_hi[0], P.c_in[0], P.parent);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
+    if (hier) {
+        DIPL_CUDA(cudaMemsetAsync(P.hp_other, 0xFF, sizeof(int) * N, stream));
+        HplocParams hp{};
+        hp.keys = P.keys_sorted, hp.offsets = P.d_offsets;
+        hp.lo = P.c_lo[0], hp.hi = P.c_hi[0], hp.info = P.c_in[0];
+        hp.child = P.child, hp.node_lo = P.nlo, hp.node_hi = P.nhi, hp.parent = P.parent;
+        hp.other = P.hp_other, hp.cnt = P.hp_cnt, hp.fid = P.hp_fid;
+        hp.root_lo = P.c_lo[1], hp.root_hi = P.c_hi[1];
+        hp.ctrl = P.d_ctrl, hp.err = P.d_err;
+        hp.num_leaves = (int)N, hp.num_inner = (int)K, hp.num_meshes = m, hp.radius = d0.nn_search_radius;
+        hp.max_node_iterations = clustering_iteration_limit() ? (int)clustering_iteration_limit() : 64;
+        const unsigned grid = blocks_for(N, kHplocThreads);
+        if (P.key_bytes == 4) hploc_kernel<uint32_t><<<grid, kHplocThreads, 0, stream>>>(hp);
+        else hploc_kernel<unsigned long long><<<grid, kHplocThreads, 0, stream>>>(hp);
+        note_launches();
+        DIPL_CUDA(cudaGetLastError());
+    }
     pp.lo[0] = P.c_lo[0], pp.hi[0] = P.c_hi[0], pp.lo[1] = P.c_lo[1], pp.hi[1] = P.c_hi[1];
     pp.info[0] = P.c_in[0], pp.info[1] = P.c_in[1];
     pp.child = P.child, pp.node_lo = P.nlo, pp.node_hi = P.nhi, pp.parent = P.parent;
     pp.status[0] = P.status, pp.status[1] = P.status + P.tiles_max + 1;
     pp.ctrl = P.d_ctrl, pp.err = P.d_err;
     pp.num_leaves = (int)N, pp.num_meshes = m, pp.radius = d0.nn_search_radius;
-    const int mid_ctas = ploc_mid_ctas();
+    pp.max_iterations = clustering_iteration_limit() ? clustering_iteration_limit() : kMaxPlocIterations;
+    const int mid_ctas = hier ? 0 : ploc_mid_ctas();
     pp.grid_stop = mid_ctas > 0 ? mid_ctas * kMidSlice : kTailMax;
-    if (N > m && N > pp.grid_stop) {
+    if (!hier && N > m && N > pp.grid_stop) {
         switch (P.B) {
             case 128: st = launch_ploc_any<128>(pp, P.tiles0, stream); break;
             case 512: st = launch_ploc_any<512>(pp, P.tiles0, stream); break;
@@ -1708,8 +1978,9 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
         }
         if (st != DIPL_OK) return st;
     }
-    if (N > m && N > kTailMax && mid_ctas > 0 && (st = launch_ploc_mid(pp, mid_ctas, stream)) != DIPL_OK) return st;
-    if (N > m && (st = launch_ploc_tail(pp, stream)) != DIPL_OK) return st;
+    if (!hier && N > m && N > kTailMax && mid_ctas > 0 && (st = launch_ploc_mid(pp, mid_ctas, stream)) != DIPL_OK)
+        return st;
+    if (!hier && N > m && (st = launch_ploc_tail(pp, stream)) != DIPL_OK) return st;
 
     // ---- layout -------------------------------------------------------------------------------------
     LayoutParams LP{P.child, P.nlo, P.nhi, P.parent, (int)N, (int)K, P.L};
@@ -1769,6 +2040,7 @@ static dipl_status plan_finish(BuildPlan& P, dipl_bvh** out, bool allow_wide) {
         h->max_leaf = P.descs[i].max_triangles_per_leaf;
         h->radius = P.descs[i].nn_search_radius;
         h->kdop = P.descs[i].kdop_size;
+        h->clustering = P.descs[i].clustering;
         h->d_err = P.d_err;
         h->root = 0;
         return h;

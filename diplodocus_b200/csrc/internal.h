@@ -3,11 +3,38 @@
 
 #include <algorithm>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
 
 namespace dipl {
+
+// ---- launch-shape probes -----------------------------------------------------------------------
+// A launch-shape probe answered once per device: the answer depends on the device's limits (SMs, shared memory,
+// schedulable cluster sizes), so each device gets its own, computed under a lock so that concurrent builds on
+// other host threads never see a half-made answer.
+constexpr int kMaxProbeDevices = 64;
+struct DeviceProbe {
+    std::mutex mu;
+    bool done[kMaxProbeDevices] = {};
+    int value[kMaxProbeDevices] = {};
+};
+
+template <class F>
+int probe_per_device(DeviceProbe& p, F&& probe) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxProbeDevices) {
+        (void)cudaGetLastError();
+        return probe();  // no cache slot: answer without caching
+    }
+    std::lock_guard<std::mutex> lock(p.mu);
+    if (!p.done[dev]) {
+        p.value[dev] = probe();
+        p.done[dev] = true;
+    }
+    return p.value[dev];
+}
 
 // ---- sort ----------------------------------------------------------------------------------------
 size_t radix_sort_scratch_bytes(int64_t n, int begin_bit, int end_bit, int digit_bits);
@@ -30,6 +57,10 @@ struct DeviceBuffer {
 };
 dipl_status device_alloc(void** ptr, size_t bytes, cudaStream_t stream);
 void device_free(void* ptr, cudaStream_t stream);
+
+// Process-wide limits set by dipl_set_limits (0 = the built-in bound).
+uint32_t clustering_iteration_limit();
+uint32_t trace_step_limit();
 
 // Scope guard for scratch allocations of one call.
 class ScratchArena {
@@ -83,7 +114,7 @@ struct dipl_bvh {
     int32_t root = 0;           // root reference (node index or leaf reference)
     int32_t depth = 0;
     int32_t ploc_iterations = 0;
-    int32_t code_type = 0, bv_type = 0, layout = 0, max_leaf = 4, radius = 16, kdop = 32;
+    int32_t code_type = 0, bv_type = 0, layout = 0, max_leaf = 4, radius = 16, kdop = 32, clustering = 0;
     // traced arrays (device)
     void* nodes = nullptr;      // BNode / SNode / WNode
     int64_t node_size = 64;     // bytes per node of the traced layout

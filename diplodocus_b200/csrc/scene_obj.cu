@@ -17,6 +17,11 @@
 //
 // Deliberate differences: an out-of-range vertex or normal index fails the load (the reference reads out of
 // bounds); a .meta value must be one complete number token.
+//
+// Attribution: the quad split, the ear-clipping loop and its point-in-polygon test follow the rules of
+// tinyobjloader (MIT licence, Copyright (c) 2012-present Syoyo Fujita and contributors), which the reference
+// vendors; the point-in-polygon crossing test is W. Randolph Franklin's PNPOLY (BSD-style licence,
+// Copyright (c) 1970-2003 Wm. Randolph Franklin). They are restated here so the triangles match the reference's.
 #include <cctype>
 #include <cerrno>
 #include <cmath>

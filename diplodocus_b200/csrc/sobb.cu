@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
                                                                int64_t n, dipl_hit* __restrict__ hits,
                                                                uint8_t* __restrict__ occluded, uint32_t flags,
                                                                unsigned long long* __restrict__ counters,
-                                                               uint32_t* __restrict__ err) {
+                                                               uint32_t* __restrict__ err, uint32_t step_limit) {
     __shared__ float s_o[kDirs][kSThreads];
     __shared__ float s_inv[kDirs][kSThreads];
     __shared__ float s_tol[kDirs][kSThreads];
@@ -305,7 +305,6 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
         int sp = 0;
         int cur = num_nodes >= 0 ? root : 0x7FFFFFFF;
         uint32_t steps = 0;
-        const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
         auto slab_box = [&](int axes, float l0, float h0, float l1, float h1, float l2, float h2, float lim) {
             float tn = __int_as_float(0xFF800000), tf = __int_as_float(0x7F800000);
             const float ls[3] = {l0, l1, l2}, hs[3] = {h0, h1, h2};
@@ -417,7 +416,8 @@ dipl_status launch_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl
     const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
     sobb_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kSThreads - 1) / kSThreads), kSThreads, 0, s>>>(
         static_cast<const SNode*>(b->nodes), b->tris, b->root, num_nodes, b->kdop / 2, rays, n, hits, occ, flags,
-        counters, b->d_err);
+        counters, b->d_err,
+        trace_step_limit() ? trace_step_limit() : 2u * (uint32_t)std::max(num_nodes, 0) + 64u);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
     return DIPL_OK;
@@ -431,7 +431,7 @@ dipl_status launch_sobb_stack(const dipl_bvh* b, const dipl_ray* rays, int64_t n
     return launch_sobb<LEAF, ANY, COUNT, 512>(b, rays, n, hits, occ, flags, counters, s);
 }
 
-std::once_flag g_triples_once;
+DeviceProbe g_triples_uploaded;  // per device: the table lives in each device's constant memory
 int g_triples = 0;
 
 dipl_status upload_triples() {
@@ -471,8 +471,10 @@ dipl_status upload_triples() {
 // Allocations of the SOBB refit (and the one-time upload of the direction triples).
 dipl_status sobb_prepare(long long N, long long K, Storage& work, Storage& out, SobbScratch* sc, SNode** snodes) {
     dipl_status st = DIPL_OK;
-    std::call_once(g_triples_once, [&] { st = upload_triples(); });
-    if (st != DIPL_OK) return st;
+    if (!probe_per_device(g_triples_uploaded, [] { return upload_triples() == DIPL_OK ? 1 : 0; })) {
+        set_last_error("SOBB: upload of the direction-triple table failed");
+        return DIPL_ERR_CUDA;
+    }
     const long long Kalloc = std::max<long long>(K, 1);
     Kdop* kdop;
     if ((st = work.alloc(&kdop, (size_t)(N + Kalloc))) != DIPL_OK ||

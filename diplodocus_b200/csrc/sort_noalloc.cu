@@ -8,14 +8,19 @@
 //
 // Limits and rules of use:
 //  - at most kNoAllocMaxKeys (2^18 = 262,144) pairs per call; larger sorts are rejected;
-//  - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
-//    current and caches it, so make that first call before any stream capture;
+//  - the first call in a CUDA context looks up the array's device address (cudaGetSymbolAddress) with that
+//    context current and caches it under the context's id, so make that first call before any stream capture.
+//    Each context loads the library's device image anew, so after a device reset, or when another context is
+//    made current, the array may sit at another address: a call from a context the cache has not seen looks it
+//    up again (context ids are never reused within a process, so a stale address is never handed out);
 //  - every call on a device uses the same array, which keeps whatever the last call left in it; the parts
 //    that must start at zero (digit histograms, look-back words, the error word) are cleared by each call,
 //    but two calls whose work overlaps on the GPU (different streams, no ordering between them) race on it
 //    and give wrong results: order them;
 //  - like dipl_radix_sort_pairs, the call synchronises `stream` once at the end to report device errors.
 #include <mutex>
+
+#include <cuda.h>  // CUcontext and CUresult types only: the two driver calls are resolved at run time
 
 #include "internal.h"
 
@@ -37,26 +42,74 @@ constexpr size_t kNoAllocScratchBytes = kErrBytes + kAltKeyBytes + kAltValBytes 
 // comes from cudaGetSymbolAddress below, never from taking the address of the name.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
+// Identity of the calling thread's current context, through the driver's cuCtxGetCurrent / cuCtxGetId (resolved
+// at run time through the runtime, so the library needs no link-time dependency on the driver library). 0 when no
+// context is current yet.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
-// Device address of the scratch array on the current device (looked up once per device).
-dipl_status scratch_for_current_device(unsigned char** out) {
+dipl_status current_context_id(unsigned long long* id) {
+    static std::once_flag once;
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+        (void)cudaGetLastError();
+    });
+    if (!get_current || !get_id) {
+        set_last_error("dipl_radix_sort_pairs_noalloc: cuCtxGetCurrent / cuCtxGetId unavailable from the driver");
+        return DIPL_ERR_CUDA;
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) {
+        set_last_error("dipl_radix_sort_pairs_noalloc: cuCtxGetCurrent failed");
+        return DIPL_ERR_CUDA;
+    }
+    *id = 0;
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS) {
+        set_last_error("dipl_radix_sort_pairs_noalloc: cuCtxGetId failed");
+        return DIPL_ERR_CUDA;
+    }
+    return DIPL_OK;
+}
+
+constexpr int kMaxDevices = 64;
+struct ScratchAddress {
+    unsigned long long context_id = 0;  // 0: nothing cached
+    void* ptr = nullptr;
+};
+std::mutex g_scratch_mu;
+ScratchAddress g_scratch[kMaxDevices];
+
+// Device address of the scratch array in the current context (looked up once per context).
+dipl_status scratch_for_current_context(unsigned char** out) {
     int dev = 0;
     DIPL_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) {
         set_last_error("dipl_radix_sort_pairs_noalloc: device ordinal out of range");
         return DIPL_ERR_UNSUPPORTED;
     }
+    unsigned long long id = 0;
+    dipl_status st = current_context_id(&id);
+    if (st != DIPL_OK) return st;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (id == 0 || g_scratch[dev].context_id != id || !g_scratch[dev].ptr) {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // binds the device's context if none was
         if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_scratch_ptr[dev] = p;
+        if ((st = current_context_id(&id)) != DIPL_OK) return st;
+        g_scratch[dev].context_id = id;
+        g_scratch[dev].ptr = p;
     }
-    *out = static_cast<unsigned char*>(g_scratch_ptr[dev]);
+    *out = static_cast<unsigned char*>(g_scratch[dev].ptr);
     return DIPL_OK;
 }
 
@@ -90,7 +143,7 @@ extern "C" dipl_status dipl_radix_sort_pairs_noalloc(const void* d_keys_in, cons
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* base = nullptr;
-    dipl_status st = scratch_for_current_device(&base);
+    dipl_status st = scratch_for_current_context(&base);
     if (st != DIPL_OK) return st;
     uint32_t* err = reinterpret_cast<uint32_t*>(base);
     void* kalt = base + kErrBytes;

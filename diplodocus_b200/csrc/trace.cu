@@ -122,6 +122,7 @@ struct TailQueue {
     int slot_ints;
     int min_steps;       // 0: no offload
     int max_lanes;
+    uint32_t step_limit; // steps one ray may take (both kernels), beyond which it is given up and flagged
 };
 
 // Float bits in an order that compares like the floats (for warp minima).
@@ -152,7 +153,8 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
                                                               int64_t n, int64_t chunk, dipl_hit* __restrict__ hits,
                                                               uint8_t* __restrict__ occluded, uint32_t flags,
                                                               unsigned long long* __restrict__ counters,
-                                                              uint32_t* __restrict__ err, TailQueue tq) {
+                                                              uint32_t* __restrict__ err, TailQueue tq,
+                                                              const uint32_t* __restrict__ order) {
     __shared__ int2 sh_stack[SHORT > 0 ? SHORT * kTraceThreads : 1];
     const int lane = threadIdx.x & 31;
     const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
     const int64_t end = min(n, beg + chunk);
     const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
     const uint32_t lt_mask = lanemask_lt();
-    const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+    const uint32_t step_limit = tq.step_limit;
     int64_t next = beg;  // next ray of the chunk (warp-uniform)
     int64_t my = -1;     // this lane's ray, -1 when idle
     RayState r{};
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
             if (idle) {
                 const int64_t cand = next + __popc(idle_mask & lt_mask);
                 if (cand < end) {
-                    my = cand;
+                    my = order ? (int64_t)__ldg(order + cand) : cand;  // the ray's own index (hits go there)
                     r = load_ray(rays, my);
                     if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(r.d);
                     best_t = r.tmax, best_u = 0.0f, best_v = 0.0f, best_prim = -1, found = false;
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(kTraceThreads) tail_kernel(const BNode* __rest
     const int lane = threadIdx.x & 31;
     const uint32_t lt_mask = lanemask_lt();
     const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
-    const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
+    const uint32_t step_limit = tq.step_limit;
     const unsigned total = min(*reinterpret_cast<volatile unsigned*>(&tq.count[0]), (unsigned)tq.cap);
     if (total == 0) return;  // nothing was handed on: the whole grid leaves at once
     unsigned visits = 0, tests = 0;
@@ -490,17 +492,112 @@ __global__ void __launch_bounds__(kTraceThreads) tail_kernel(const BNode* __rest
     }
 }
 
+// ---- ray order ----------------------------------------------------------------------------------------
+// Batches of at least kReorderMinRays rays are traced in the order of a 30-bit key: the direction's octant
+// above a 9-bit-per-axis Morton code of the origin within the batch's origin bounds. A warp's chunk of rays then
+// starts in one small region and heads the same way, so its lanes fetch the same nodes and branch alike.
+// Records still go to each ray's own index; only the order of work changes, never a result.
+constexpr int64_t kReorderMinRays = int64_t(1) << 20;
+constexpr int kReorderBits = 30;
+
+__global__ void __launch_bounds__(256) ray_bounds_kernel(const dipl_ray* __restrict__ rays, int64_t n,
+                                                         int* __restrict__ box) {
+    float lo[3] = {__int_as_float(0x7F800000), __int_as_float(0x7F800000), __int_as_float(0x7F800000)};
+    float hi[3] = {__int_as_float(0xFF800000), __int_as_float(0xFF800000), __int_as_float(0xFF800000)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 o = __ldg(reinterpret_cast<const float4*>(rays) + 2 * i);
+        const float v[3] = {o.x, o.y, o.z};
+        for (int a = 0; a < 3; ++a)
+            if (isfinite(v[a])) lo[a] = fminf(lo[a], v[a]), hi[a] = fmaxf(hi[a], v[a]);
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(box + a, float_to_ordered(lo[a]));
+            atomicMax(box + 3 + a, float_to_ordered(hi[a]));
+        }
+    }
+}
+
+__global__ void ray_box_init_kernel(int* box) {
+    if (threadIdx.x < 6)
+        box[threadIdx.x] = float_to_ordered(__int_as_float(threadIdx.x < 3 ? 0x7F800000 : 0xFF800000));
+}
+
+__device__ __forceinline__ uint32_t spread3_9(uint32_t x) {  // 9 bits to every third bit
+    x &= 0x1FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__global__ void __launch_bounds__(256) ray_keys_kernel(const dipl_ray* __restrict__ rays, int64_t n,
+                                                       const int* __restrict__ box, uint32_t* __restrict__ keys) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 o = __ldg(reinterpret_cast<const float4*>(rays) + 2 * i);
+    const float4 d = __ldg(reinterpret_cast<const float4*>(rays) + 2 * i + 1);
+    const float v[3] = {o.x, o.y, o.z};
+    uint32_t cell[3];
+    for (int a = 0; a < 3; ++a) {
+        const float lo = ordered_to_float(__ldg(box + a)), hi = ordered_to_float(__ldg(box + 3 + a));
+        const float ext = hi - lo;
+        const float q = ext > 0.0f ? (v[a] - lo) * (512.0f / ext) : 0.0f;
+        cell[a] = (uint32_t)fminf(fmaxf(q, 0.0f), 511.0f);  // NaN -> 0
+    }
+    const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    keys[i] = (oct << 27) | (spread3_9(cell[0]) << 2) | (spread3_9(cell[1]) << 1) | spread3_9(cell[2]);
+}
+
+// Device memory of one reordered trace: keys, the order and the sort's scratch (released in stream order).
+struct RayOrder {
+    void* mem = nullptr;
+    uint32_t* order = nullptr;
+};
+
+dipl_status make_ray_order(const dipl_ray* rays, int64_t n, uint32_t* d_err, cudaStream_t s, RayOrder& ro) {
+    const size_t sort_bytes = radix_sort_scratch_bytes(n, 0, kReorderBits, 8);
+    const size_t key_bytes = sizeof(uint32_t) * (size_t)n;
+    const size_t bytes = 256 + 5 * key_bytes + sort_bytes;
+    dipl_status st = device_alloc(&ro.mem, bytes, s);
+    if (st != DIPL_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ro.mem);
+    int* box = reinterpret_cast<int*>(base);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(base + 256);
+    uint32_t* keys_sorted = keys + n;
+    uint32_t* keys_alt = keys_sorted + n;
+    ro.order = keys_alt + n;
+    uint32_t* order_alt = ro.order + n;
+    unsigned char* scratch = reinterpret_cast<unsigned char*>(order_alt + n);
+    ray_box_init_kernel<<<1, 32, 0, s>>>(box);
+    note_launches();
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    ray_bounds_kernel<<<grid, 256, 0, s>>>(rays, n, box);
+    note_launches();
+    ray_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rays, n, box, keys);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return radix_sort_pairs(keys, nullptr, keys_sorted, ro.order, keys_alt, order_alt, n, 4, 0, kReorderBits, 8,
+                            scratch, s, d_err);
+}
+
+// Blocks of a persistent trace launch: every resident block on every SM (per kernel instantiation and device).
 template <typename K>
 int persistent_grid(K kernel) {
-    static int grid = 0;  // per instantiation
-    if (grid == 0) {
+    static DeviceProbe probe;  // per instantiation
+    return probe_per_device(probe, [kernel] {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceThreads, 0);
-        grid = std::max(1, sms * std::max(1, per_sm));
-    }
-    return grid;
+        (void)cudaGetLastError();
+        return std::max(1, sms * std::max(1, per_sm));
+    });
 }
 
 template <int LEAF, bool ANY, bool COUNT, int STACK, int SHORT>
@@ -518,7 +615,9 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
         set_last_error("trace: node array is not 64-byte aligned");
         return DIPL_ERR_INTERNAL;
     }
-    TailQueue tq{nullptr, nullptr, 0, kTailHeaderInts + 2 * STACK, n >= kTailMinRays ? kTailSteps : 0, kTailLanes};
+    const uint32_t steps_cap = trace_step_limit() ? trace_step_limit() : 2u * (uint32_t)std::max(num_nodes, 0) + 64u;
+    TailQueue tq{nullptr, nullptr, 0, kTailHeaderInts + 2 * STACK, n >= kTailMinRays ? kTailSteps : 0, kTailLanes,
+                 steps_cap};
     void* tail_mem = nullptr;
     if (tq.min_steps > 0) {
         const size_t slot_bytes = sizeof(int) * (size_t)tq.slot_ints;
@@ -534,8 +633,18 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
             return cuda_status(e, "cudaMemsetAsync");
         }
     }
+    RayOrder ro;
+    if (n >= kReorderMinRays && (flags & DIPL_TRACE_KEEP_ORDER) == 0u) {
+        dipl_status st = make_ray_order(rays, n, b->d_err, s, ro);
+        if (st != DIPL_OK) {
+            if (ro.mem) device_free(ro.mem, s);
+            device_free(tail_mem, s);
+            return st;
+        }
+    }
     kernel<<<(unsigned)grid, kTraceThreads, 0, s>>>(static_cast<const BNode*>(b->nodes), b->tris, b->root, num_nodes,
-                                                   rays, n, chunk, hits, occ, flags, counters, b->d_err, tq);
+                                                   rays, n, chunk, hits, occ, flags, counters, b->d_err, tq,
+                                                   ro.order);
     note_launches();
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && tq.min_steps > 0) {
@@ -547,6 +656,7 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
         e = cudaGetLastError();
     }
     device_free(tail_mem, s);
+    if (ro.mem) device_free(ro.mem, s);
     DIPL_CUDA(e);
     return DIPL_OK;
 }

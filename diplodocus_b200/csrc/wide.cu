@@ -295,7 +295,7 @@ template <int LEAF, bool ANY, bool COUNT, int STACK>
 __global__ void __launch_bounds__(kWTraceThreads) wide_trace_kernel(
     const WNode* __restrict__ nodes, const float4* __restrict__ tris, int root, int num_nodes,
     const dipl_ray* __restrict__ rays, int64_t n, dipl_hit* __restrict__ hits, uint8_t* __restrict__ occluded,
-    uint32_t flags, unsigned long long* __restrict__ counters, uint32_t* __restrict__ err) {
+    uint32_t flags, unsigned long long* __restrict__ counters, uint32_t* __restrict__ err, uint32_t step_limit) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned visits = 0, tests = 0;
     if (i < n) {
@@ -342,7 +342,6 @@ __global__ void __launch_bounds__(kWTraceThreads) wide_trace_kernel(
             node = root;
         }
         uint32_t steps = 0;
-        const uint32_t step_limit = 2u * (uint32_t)max(num_nodes, 0) + 64u;
         while (!done) {
             if (++steps > step_limit) {
                 bad = true;
@@ -452,7 +451,9 @@ dipl_status launch_wide(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl
     const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
     wide_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kWTraceThreads - 1) / kWTraceThreads), kWTraceThreads,
                                                   0, s>>>(static_cast<const WNode*>(b->nodes), b->tris, b->root,
-                                                          num_nodes, rays, n, hits, occ, flags, counters, b->d_err);
+                                                          num_nodes, rays, n, hits, occ, flags, counters, b->d_err,
+                                                          trace_step_limit() ? trace_step_limit()
+                                                                             : 2u * (uint32_t)std::max(num_nodes, 0) + 64u);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
     return DIPL_OK;

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define DIPL_ABI_VERSION 1
+#define DIPL_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define DIPL_API __attribute__((visibility("default")))
@@ -56,6 +56,13 @@ typedef enum dipl_code_type { DIPL_CODE_MORTON30 = 0, DIPL_CODE_EMC60 = 1 } dipl
 /* Bounding volume of the nodes. Mirrors BoundingVolumeType (gpu_acceleration_structure_config.h:7). */
 typedef enum dipl_bv_type { DIPL_BV_AABB = 0, DIPL_BV_SOBB = 1 } dipl_bv_type;
 
+/* Clustering of the build. HPLOC (default): PLOC merging confined to the nodes of the binary radix tree of the
+ * sorted codes, bottom up in one launch (hierarchical PLOC, Benthin et al. 2024); PLOC: the global PLOC loop
+ * (Meister & Bittner 2017), every iteration over all clusters of the scene. Both merge by the same distance and
+ * tie rule; HPLOC's trees have about the same SAH cost (within 1% on the 1M sphere and the soup) and build in a
+ * fraction of the time. The reference names PLOC as its planned builder (README.md:156-161). */
+typedef enum dipl_clustering { DIPL_CLUSTER_HPLOC = 0, DIPL_CLUSTER_PLOC = 1 } dipl_clustering;
+
 /* Node layout used by traces. BINARY: two FP32 child boxes per 64-byte node (80 bytes with SOBB).
  * WIDE8_Q8: 8-wide nodes with 8-bit conservatively quantised child bounds (80 bytes), FP32 leaf re-test. */
 typedef enum dipl_layout { DIPL_LAYOUT_BINARY = 0, DIPL_LAYOUT_WIDE8_Q8 = 1 } dipl_layout;
@@ -67,6 +74,11 @@ typedef enum dipl_leaf_test { DIPL_LEAF_REF_MT = 0, DIPL_LEAF_WATERTIGHT = 1 } d
 /* Trace flags. BACKFACE_CULLING has the reference's meaning (triangle.cc:18-21): with it, a triangle
  * is hit only when e1 . (dir x e2) > 0. */
 #define DIPL_TRACE_BACKFACE_CULLING 1u
+/* Trace the rays in the order given. Without it, batches of 2^20 rays or more are traced in the order of a key
+ * of each ray's origin cell and direction octant (computed and sorted on the device inside the call), so that
+ * the rays of a warp start close together and head the same way; each record still goes to its ray's index and
+ * the records are the same either way. */
+#define DIPL_TRACE_KEEP_ORDER 2u
 
 /* Build description. The three vertex arrays are the reference GPU scene's SoA positions
  * tri_v0_pos / tri_v1_pos / tri_v2_pos (src/gpu/scene/gpu_scene.h:18-20): float3 per triangle,
@@ -84,8 +96,10 @@ typedef struct dipl_build_desc {
                                        meaning, sbvh.cc:273-276); 2..8, default 4 */
     int32_t nn_search_radius;       /* PLOC radius r, 1..32 (GpuAccelerationStructureConfig::nn_search_radius) */
     int32_t kdop_size;              /* SOBB direction set: kdop_size/2 directions, 6..32 (kdop_size) */
-    int32_t ploc_block_size;        /* PLOC threads per block: 0 = auto, else 128, 256 or 512 */
+    int32_t ploc_block_size;        /* clustering threads per block: 0 = auto, else 128, 256 or 512 */
     int32_t sort_digit_bits;        /* radix sort digit width: 0 = auto (8), else 6, 7, 8 or 10 */
+    int32_t clustering;             /* dipl_clustering (ABI version 2) */
+    int32_t reserved;               /* 0 */
 } dipl_build_desc;
 
 /* A ray: origin, hit interval lower bound, direction, upper bound (32 bytes). A hit needs
@@ -111,12 +125,13 @@ typedef struct dipl_bvh_info {
     int64_t num_leaves;
     int64_t node_bytes;          /* bytes of the traced node array */
     int64_t triangle_bytes;      /* bytes of the leaf triangle array */
-    int32_t depth;               /* levels of the PLOC tree (bounds the traversal stack) */
-    int32_t ploc_iterations;
+    int32_t depth;               /* levels of the clustering tree (bounds the traversal stack) */
+    int32_t ploc_iterations;     /* PLOC: global iterations; HPLOC: iterations of all tree nodes, summed */
     int32_t code_type, bv_type, layout, max_triangles_per_leaf, nn_search_radius, kdop_size;
+    int32_t clustering, reserved; /* dipl_clustering (ABI version 2) */
 } dipl_bvh_info;
 
-/* Fills a description with the defaults (Morton30, AABB, binary, leaves < 4, r = 16, 32-DOP, auto). */
+/* Fills a description with the defaults (Morton30, AABB, binary, leaves < 4, r = 16, 32-DOP, auto, HPLOC). */
 DIPL_API void dipl_build_desc_init(dipl_build_desc* desc);
 
 /* Builds a BVH over desc->num_triangles triangles (0 is allowed: every ray misses).
@@ -181,7 +196,8 @@ DIPL_API dipl_status dipl_bvh_get_info(const dipl_bvh* bvh, dipl_bvh_info* info)
 
 /* Copies the clustering result to HOST buffers (any may be NULL): h_perm[num_triangles] = triangle id at
  * each sorted-code position (leaf node id = position); h_children[2*(num_triangles-1)] = left/right node
- * ids of internal node k in creation order (id num_triangles + k); h_boxes[6*(num_triangles-1)] = its box
+ * ids of internal node k (id num_triangles + k; PLOC numbers nodes in creation order, HPLOC gives node k the
+ * id of radix-tree split k or of a split below it); h_boxes[6*(num_triangles-1)] = its box
  * (lo xyz, hi xyz). Synchronises `stream`. For checking and debugging. */
 DIPL_API dipl_status dipl_bvh_download_topology(const dipl_bvh* bvh, int32_t* h_perm, int32_t* h_children, float* h_boxes,
                                        void* stream);
@@ -217,8 +233,9 @@ DIPL_API dipl_status dipl_radix_sort_pairs(const void* d_keys_in, const uint32_t
  * allocate device memory (a host application that owns the whole GPU heap and gives plug-ins fixed
  * buffers, or a loop that must not stall on cudaMalloc). Its scratch is one fixed array in the library's
  * device image (about 5 MB on every GPU that loads the library, held until the process exits); no memory is
- * allocated per call. At most 262,144 pairs (larger n: DIPL_ERR_INVALID_ARGUMENT). The first call on a
- * device looks up the array's address, so make it before any stream capture. All calls on a device share
+ * allocated per call. At most 262,144 pairs (larger n: DIPL_ERR_INVALID_ARGUMENT). The first call in each
+ * CUDA context looks up the array's address in that context (a context made current later, or the one after a
+ * device reset, gets its own lookup), so make it before any stream capture. All calls on a device share
  * the array: the call clears what must start at zero, but calls whose GPU work overlaps race on it, so
  * order them. Synchronises `stream` at the end, like dipl_radix_sort_pairs. */
 DIPL_API dipl_status dipl_radix_sort_pairs_noalloc(const void* d_keys_in, const uint32_t* d_vals_in, void* d_keys_out,
@@ -317,6 +334,30 @@ DIPL_API dipl_status dipl_obj_scene_get_materials(const dipl_obj_scene* scene, f
 DIPL_API dipl_status dipl_obj_scene_get_lights(const dipl_obj_scene* scene, int32_t* area_triangle_ids,
                                                float* area_colors, float* area_surface_areas, float* point_lights);
 DIPL_API void dipl_obj_scene_destroy(dipl_obj_scene* scene);
+
+/* ---- limits -------------------------------------------------------------------------------------------------- */
+
+/* No counterpart in the reference, which has no limits and aborts on any CUDA error (CUDA_CHECK -> abort,
+ * src/gpu/cuda_utils.h:12-18). Process-wide limits of this library (every device and thread), for callers that
+ * share the GPU with other work and for exercising the failure paths without a GPU fault:
+ *   device_memory_bytes    device memory the library may hold at once (all live allocations of builds, handles and
+ *                          traces); an allocation beyond it fails like a failed cudaMallocAsync, with
+ *                          DIPL_ERR_OUT_OF_MEMORY, and the call releases what it had taken. 0 = no limit.
+ *   clustering_iterations  iterations the clustering may take before the build gives up with DIPL_ERR_INTERNAL:
+ *                          global iterations (PLOC) or iterations within one radix-tree node (HPLOC). 0 = the
+ *                          built-in bounds (65536, 64). Read when a build is enqueued: a build plan keeps the value
+ *                          of its capture.
+ *   trace_steps            traversal steps (inner nodes and leaves) one ray may take; a ray that needs more is
+ *                          finished with what it has and DIPL_ERR_INTERNAL is recorded for dipl_bvh_check_errors.
+ *                          0 = the built-in bound (twice the node count, plus 64).
+ * dipl_get_limits also reports the device memory the library holds now (may be NULL). */
+typedef struct dipl_limits {
+    uint64_t device_memory_bytes;
+    uint32_t clustering_iterations;
+    uint32_t trace_steps;
+} dipl_limits;
+DIPL_API dipl_status dipl_set_limits(const dipl_limits* limits);
+DIPL_API dipl_status dipl_get_limits(dipl_limits* limits, uint64_t* device_memory_in_use);
 
 DIPL_API const char* dipl_status_string(dipl_status status);
 /* Message of the calling thread's most recent failure ("" if none). */

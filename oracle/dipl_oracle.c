@@ -14,7 +14,8 @@
  *    so exact-t ties go to the lowest id. The same loop runs with the watertight test.
  *  - orc_brute_any: DummyAccelerationStucture::IntersectAny (dummy_acceleration_structure.cc:66-79).
  *  - orc_wt: watertight ray/triangle test of Woop, Benthin and Wald (JCGT 2013), FP32 with the
- *    paper's FP64 recomputation of zero edge functions. Absent from the reference.
+ *    paper's FP64 recomputation of zero edge functions. Absent from the reference (README.md:156-161 lists
+ *    the accelerated path as planned).
  *  - orc_morton30 / orc_emc60: this project's Morton and extended-Morton codes (absent from the
  *    reference; README.md:14-16 names Vinkler et al. 2017 for EMC).
  *  - orc_ploc: this project's PLOC (Meister & Bittner 2017) merge loop with its deterministic
@@ -538,6 +539,326 @@ int64_t orc_ploc(const float* tris, int64_t n, const int32_t* perm, const int32_
     free(nxt);
     free(nn);
     return made;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Hierarchical PLOC (after Benthin et al., "H-PLOC", HPG 2024) as built on the device, restated  */
+/* sequentially.                                                                                */
+/*                                                                                              */
+/* The sorted codes define a binary radix tree (LBVH): split s sits between sorted positions s  */
+/* and s+1 and has the order key (codes[s] ^ codes[s+1], s ^ (s+1), s), compared                */
+/* lexicographically; a split between two segments (meshes) has a key above every other. A node */
+/* [l, r] joins its neighbour across the split with the smaller key (Apetrei 2014): split r if   */
+/* l == 0 or (r != n-1 and key(r) < key(l-1)), else split l-1; the second of the two children to */
+/* arrive at a split goes on with the union of their ranges. Each node holds a list of clusters  */
+/* in position order: a leaf holds its triangle; an internal node the left child's list followed */
+/* by the right child's, on which PLOC iterations run (the key and mutual-pair rule of orc_ploc, */
+/* positions being list indices, radius r) while the list is longer than `threshold`, or longer  */
+/* than 1 when the node spans a whole segment (a mesh root: the walk stops there).               */
+/*                                                                                              */
+/* Node ids are deterministic: internal node ids are n + s for the n - 1 splits s. A list of c   */
+/* clusters carries c - 1 unused ids; a node's pool is the left list's unused ids, then n + m    */
+/* (its own split m), then the right list's; its merges take ids from the front of the pool in   */
+/* creation order (iteration, then position) and the rest go up with its list.                   */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct {
+    uint64_t cx;
+    uint32_t ix;
+    int64_t s;
+    int boundary;
+} orc_split_key;
+
+static orc_split_key split_key(const uint64_t* codes, const int32_t* seg, int64_t s) {
+    orc_split_key k;
+    k.boundary = seg && seg[s] != seg[s + 1];
+    k.cx = codes[s] ^ codes[s + 1];
+    k.ix = (uint32_t)s ^ (uint32_t)(s + 1);
+    k.s = s;
+    return k;
+}
+
+static int split_less(orc_split_key a, orc_split_key b) {
+    if (a.boundary != b.boundary) return a.boundary < b.boundary;
+    if (a.cx != b.cx) return a.cx < b.cx;
+    if (a.ix != b.ix) return a.ix < b.ix;
+    return a.s < b.s;
+}
+
+/* PLOC on list L[0..c) in place until c <= target; returns the new count. Merges take ids from pool. */
+static int hploc_merge(orc_cluster* L, int c, int target, int radius, const int32_t* pool, int* pool_next,
+                       int64_t n, int32_t* children, float* boxes, int32_t* iterations) {
+    int nn[64];
+    orc_cluster tmp[64];
+    while (c > target) {
+        for (int i = 0; i < c; ++i) {
+            uint64_t best = ~(uint64_t)0;
+            int bj = -1;
+            int jlo = i - radius < 0 ? 0 : i - radius;
+            int jhi = i + radius > c - 1 ? c - 1 : i + radius;
+            for (int j = jlo; j <= jhi; ++j) {
+                if (j == i) continue;
+                uint64_t k = ploc_key(&L[i], &L[j], i, j);
+                if (k < best) {
+                    best = k;
+                    bj = j;
+                }
+            }
+            nn[i] = bj;
+        }
+        int w = 0;
+        for (int i = 0; i < c; ++i) {
+            int j = nn[i];
+            int mutual = (j >= 0 && nn[j] == i);
+            if (mutual && i > j) continue;
+            if (mutual) {
+                orc_cluster m;
+                for (int a = 0; a < 3; ++a) {
+                    m.lo[a] = fminf(L[i].lo[a], L[j].lo[a]);
+                    m.hi[a] = fmaxf(L[i].hi[a], L[j].hi[a]);
+                }
+                int32_t id = pool[(*pool_next)++];
+                int64_t k = (int64_t)id - n;
+                children[2 * k] = L[i].node;
+                children[2 * k + 1] = L[j].node;
+                for (int a = 0; a < 3; ++a) {
+                    boxes[6 * k + a] = m.lo[a];
+                    boxes[6 * k + 3 + a] = m.hi[a];
+                }
+                m.node = id;
+                m.seg = L[i].seg;
+                tmp[w++] = m;
+            } else {
+                tmp[w++] = L[i];
+            }
+        }
+        if (iterations) ++*iterations;
+        if (w == c) break; /* cannot happen: the pair key is a strict total order */
+        memcpy(L, tmp, sizeof(orc_cluster) * (size_t)w);
+        c = w;
+    }
+    return c;
+}
+
+/* codes: sorted codes (one per sorted position); perm, seg as in orc_ploc. threshold in [1, 32].
+ * children/boxes are indexed by id - n for ids n .. 2n - 2 (minus one per extra segment).
+ * Returns the number of internal nodes, or -1 on bad input. */
+int64_t orc_hploc(const float* tris, int64_t n, const int32_t* perm, const uint64_t* codes, const int32_t* seg,
+                  int radius, int threshold, int32_t* children, float* boxes, int32_t* iterations) {
+    if (n <= 0) return 0;
+    if (radius < 1 || threshold < 1 || threshold > 32) return -1;
+    orc_cluster* clus = (orc_cluster*)malloc(sizeof(orc_cluster) * (size_t)n);
+    int32_t* fid = (int32_t*)malloc(sizeof(int32_t) * (size_t)n); /* unused ids of the list starting at l */
+    int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)n); /* list length of the node starting at l */
+    int64_t* other = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 1 ? n - 1 : 1));
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = tris + 9 * (int64_t)perm[i];
+        const int fin = tri_finite(p);
+        for (int a = 0; a < 3; ++a) {
+            clus[i].lo[a] = fin ? fminf(fminf(p[a], p[3 + a]), p[6 + a]) : INFINITY;
+            clus[i].hi[a] = fin ? fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]) : -INFINITY;
+        }
+        clus[i].node = (int32_t)i;
+        clus[i].seg = seg ? seg[i] : 0;
+        cnt[i] = 1;
+    }
+    for (int64_t s = 0; s + 1 < n; ++s) other[s] = -1;
+    int64_t made = 0;
+    int32_t iters = 0;
+    orc_cluster L[64];
+    int32_t pool[64];
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t l = i, r = i;
+        for (;;) {
+            int segroot = (l == 0 || (seg && seg[l - 1] != seg[l])) && (r == n - 1 || (seg && seg[r] != seg[r + 1]));
+            if (segroot) {
+                if (l == r) break; /* a one-triangle mesh: its leaf is the root */
+                break;
+            }
+            int64_t split;
+            int right_child;
+            if (l == 0 || (r != n - 1 && split_less(split_key(codes, seg, r), split_key(codes, seg, l - 1)))) {
+                split = r; /* this node is the left child of split r */
+                right_child = 0;
+            } else {
+                split = l - 1;
+                right_child = 1;
+            }
+            if (other[split] < 0) { /* first to arrive: leave the boundary, stop */
+                other[split] = right_child ? r : l;
+                break;
+            }
+            int64_t m = split;
+            if (right_child) {
+                l = other[split];
+            } else {
+                r = other[split];
+            }
+            /* combine: left list at [l, l + cl), right list at [m + 1, m + 1 + cr) */
+            int cl = cnt[l], cr = cnt[m + 1], c = 0, np = 0;
+            for (int k = 0; k < cl; ++k) L[c++] = clus[l + k];
+            for (int k = 0; k + 1 < cl; ++k) pool[np++] = fid[l + k];
+            pool[np++] = (int32_t)(n + m);
+            for (int k = 0; k < cr; ++k) L[c++] = clus[m + 1 + k];
+            for (int k = 0; k + 1 < cr; ++k) pool[np++] = fid[m + 1 + k];
+            int whole = (l == 0 || (seg && seg[l - 1] != seg[l])) && (r == n - 1 || (seg && seg[r] != seg[r + 1]));
+            int used = 0;
+            int c_out = hploc_merge(L, c, whole ? 1 : threshold, radius, pool, &used, n, children, boxes, &iters);
+            made += used;
+            for (int k = 0; k < c_out; ++k) clus[l + k] = L[k];
+            for (int k = 0; k + 1 < c_out; ++k) fid[l + k] = pool[used + k];
+            cnt[l] = c_out;
+        }
+    }
+    if (iterations) *iterations = iters;
+    free(clus);
+    free(fid);
+    free(cnt);
+    free(other);
+    return made;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Re-traversal of the engine's binary layout (as downloaded by dipl_bvh_download_layout), for   */
+/* checking its node-visit and triangle-test counters. The traversal is the device's: one step   */
+/* is an inner node or a leaf; both child boxes get the conservative slab test (slab distances    */
+/* widened by 1e-6 relative, entry beyond the best t + 1e-5 relative pruned), the nearer child is */
+/* visited first and the other pushed with its entry t; a leaf tests its triangles with the      */
+/* reference Moller-Trumbore (closest-hit rule: t > tmin, smaller t or an equal t at a lower id).  */
+/* The device forms the slab distances with an approximate reciprocal of the direction (relative */
+/* error below 2^-22) where this uses the IEEE one, so a decision whose two sides lie within     */
+/* 1e-6 relative of each other may go either way: such rays are flagged unstable (stable[r] = 0)  */
+/* and checks leave them out.                                                                     */
+/*                                                                                                */
+/* Node: 16 floats: (lx0, hx0, ly0, hy0), (lx1, hx1, ly1, hy1), (lz0, hz0, lz1, hz1), then the two */
+/* child references as int bits; a reference < 0 is a leaf ~(first << 3 | count). Leaf triangles: */
+/* 12 floats each (v0 xyz, primitive id bits, v1 xyz, 0, v2 xyz, 0).                              */
+/* ------------------------------------------------------------------------------------------ */
+static int close_rel(float a, float b) {
+    float m = fmaxf(fabsf(a), fabsf(b));
+    return fabsf(a - b) <= 1e-6f * m;
+}
+
+/* entry t of one box (INFINITY when missed); *unstable |= a decision too close to call */
+static float retrace_box(const float* o, const float* inv, float tmin, float lx, float hx, float ly, float hy, float lz,
+                         float hz, float t_limit, int* unstable, int* axis, float* numer) {
+    float lo[3] = {lx, ly, lz}, hi[3] = {hx, hy, hz};
+    float tn = -INFINITY, tf = INFINITY, nn = 0.0f;
+    int an = 0;
+    for (int a = 0; a < 3; ++a) {
+        float d0 = lo[a] - o[a], d1 = hi[a] - o[a];
+        float t0 = d0 * inv[a], t1 = d1 * inv[a];
+        float n = fminf(t0, t1), f = fmaxf(t0, t1);
+        if (a == 0 || n > tn) {
+            if (a > 0 && close_rel(n, tn)) *unstable = 1;
+            tn = n;
+            an = a;
+            nn = t0 <= t1 ? d0 : d1;
+        } else if (close_rel(n, tn)) {
+            *unstable = 1;
+        }
+        if (a > 0 && close_rel(f, tf)) *unstable = 1;
+        tf = a == 0 ? f : fminf(tf, f);
+    }
+    tn = tn - fabsf(tn) * 1e-6f;
+    tf = tf + fabsf(tf) * 1e-6f;
+    if (close_rel(tn, tf) || close_rel(tf, tmin) || close_rel(tn, t_limit)) *unstable = 1;
+    *axis = an;
+    *numer = nn;
+    return (tn <= tf && tf >= tmin && tn <= t_limit) ? tn : INFINITY;
+}
+
+static float retrace_prune(float best_t) { return best_t + fabsf(best_t) * 1e-5f; }
+
+void orc_retrace_binary(const float* nodes, int64_t num_nodes, const float* tris, int32_t root, const float* rays,
+                        int64_t nr, int backface, int64_t* visits, int64_t* tests, uint8_t* stable, int32_t* prim_out,
+                        float* t_out) {
+    int32_t* sref = (int32_t*)malloc(sizeof(int32_t) * 4096);
+    float* st = (float*)malloc(sizeof(float) * 4096);
+    for (int64_t r = 0; r < nr; ++r) {
+        const float* ray = rays + 8 * r;
+        const float* o = ray;
+        const float* d = ray + 4;
+        float inv[3];
+        for (int a = 0; a < 3; ++a) {
+            float x = d[a];
+            if (fabsf(x) < 1e-20f) x = copysignf(1e-20f, x);
+            inv[a] = 1.0f / x;
+        }
+        float tmin = ray[3], best_t = ray[7];
+        int32_t best_prim = -1;
+        int found = 0, unstable = 0, sp = 0;
+        int64_t v = 0, te = 0;
+        int32_t cur = num_nodes > 0 || root < 0 ? root : INT32_MAX;
+        const int32_t POP = INT32_MIN, END = INT32_MAX;
+        for (int64_t guard = 0; cur != END && guard < 4 * num_nodes + 1024; ++guard) {
+            if (cur >= 0) {
+                const float* nd = nodes + 16 * (int64_t)cur;
+                int32_t ref0, ref1;
+                memcpy(&ref0, nd + 12, 4);
+                memcpy(&ref1, nd + 13, 4);
+                ++v;
+                float lim = retrace_prune(best_t);
+                int ax0 = 0, ax1 = 0;
+                float n0 = 0.0f, n1 = 0.0f;
+                float t0 = retrace_box(o, inv, tmin, nd[0], nd[1], nd[2], nd[3], nd[8], nd[9], lim, &unstable, &ax0,
+                                       &n0);
+                float t1 = retrace_box(o, inv, tmin, nd[4], nd[5], nd[6], nd[7], nd[10], nd[11], lim, &unstable, &ax1,
+                                       &n1);
+                int h0 = t0 != INFINITY, h1 = t1 != INFINITY;
+                if (h0 && h1) {
+                    /* two entries from the same slab distance on the same axis are equal under any reciprocal */
+                    if (close_rel(t0, t1) && !(ax0 == ax1 && n0 == n1)) unstable = 1;
+                    int first0 = t0 <= t1;
+                    if (sp >= 4096) { unstable = 1; break; }
+                    sref[sp] = first0 ? ref1 : ref0;
+                    st[sp] = first0 ? t1 : t0;
+                    ++sp;
+                    cur = first0 ? ref0 : ref1;
+                } else if (h0) {
+                    cur = ref0;
+                } else if (h1) {
+                    cur = ref1;
+                } else {
+                    cur = POP;
+                }
+            } else if (cur != POP) {
+                int first = (~cur) >> 3, cnt = (~cur) & 7;
+                for (int k = 0; k < cnt; ++k) {
+                    const float* tp = tris + 12 * (int64_t)(first + k);
+                    int32_t pid;
+                    memcpy(&pid, tp + 3, 4);
+                    float b1 = 0.0f, b2 = 0.0f;
+                    float t = orc_mt(tp, tp + 4, tp + 8, o, d, backface, &b1, &b2);
+                    ++te;
+                    if (t > tmin && t < ORC_INF && (t < best_t || (t == best_t && found && pid < best_prim))) {
+                        best_t = t;
+                        best_prim = pid;
+                        found = 1;
+                    }
+                }
+                cur = POP;
+            }
+            if (cur == POP) {
+                float lim = retrace_prune(best_t);
+                cur = END;
+                while (sp > 0) {
+                    --sp;
+                    if (close_rel(st[sp], lim)) unstable = 1;
+                    if (st[sp] <= lim) {
+                        cur = sref[sp];
+                        break;
+                    }
+                }
+            }
+        }
+        visits[r] = v;
+        tests[r] = te;
+        stable[r] = (uint8_t)!unstable;
+        prim_out[r] = found ? best_prim : -1;
+        t_out[r] = found ? best_t : INFINITY;
+    }
+    free(sref);
+    free(st);
 }
 
 /* ------------------------------------------------------------------------------------------ */

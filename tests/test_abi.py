@@ -33,7 +33,7 @@ def test_library_exports_nothing_else():
 
 def test_version_and_status_strings_need_no_gpu():
     lib = L.load()
-    assert lib.dipl_abi_version() == 1
+    assert lib.dipl_abi_version() == 2
     assert lib.dipl_status_string(0) == b"DIPL_OK"
     assert lib.dipl_status_string(4) == b"DIPL_ERR_TIMEOUT"
 

@@ -67,37 +67,51 @@ def test_radix_sort_rejects_bad_arguments():
         A.radix_sort_pairs(k, None, 0, 32, 9)
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 31, 32, 33, 1000, 1025, 4097, 30000])
+CLUSTERINGS = ["hploc", "ploc"]
+
+
+def _expected_topology(orc, tris, codes, perm, clustering, radius=16):
+    """The restatement of the clustering the device ran: (children, boxes, iterations) by internal node id."""
+    if clustering == "ploc":
+        return orc.ploc(tris, perm, radius=radius)
+    return orc.hploc(tris, perm, np.asarray(codes)[perm], radius=radius)
+
+
+@pytest.mark.parametrize("clustering", CLUSTERINGS)
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 17, 31, 32, 33, 1000, 1025, 4097, 30000])
 @pytest.mark.parametrize("radius", [1, 4, 16, 32])
-def test_ploc_topology_matches_oracle(orc, n, radius):
+def test_ploc_topology_matches_oracle(orc, n, radius, clustering):
     tris = S.soup(n, seed=100 + n)
-    bvh = build(tris, nn_search_radius=radius)
+    bvh = build(tris, nn_search_radius=radius, clustering=clustering)
     perm, ch, bx = bvh.download_topology()
-    exp_perm = O.sort_perm(orc.morton30(tris))
+    codes = orc.morton30(tris)
+    exp_perm = O.sort_perm(codes)
     np.testing.assert_array_equal(perm, exp_perm)
     if n < 2:
         return
-    ech, ebx, it = orc.ploc(tris, exp_perm, radius=radius)
+    ech, ebx, it = _expected_topology(orc, tris, codes, exp_perm, clustering, radius)
     np.testing.assert_array_equal(ch, ech)
     np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
     assert bvh.info().ploc_iterations == it
 
 
+@pytest.mark.parametrize("clustering", CLUSTERINGS)
 @pytest.mark.parametrize("kind", [A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmc])
-def test_ploc_topology_duplicates_and_emc(orc, kind):
+def test_ploc_topology_duplicates_and_emc(orc, kind, clustering):
     tris = np.concatenate([np.repeat(S.open_box(), 200, axis=0), S.soup(3000, seed=4)])
-    bvh = build(tris, kind)
+    bvh = build(tris, kind, clustering=clustering)
     perm, ch, bx = bvh.download_topology()
     codes = orc.morton30(tris) if kind is A.AccelerationStructureType.kPloc else orc.emc60(tris)
     exp_perm = O.sort_perm(codes)
     np.testing.assert_array_equal(perm, exp_perm)
-    ech, ebx, it = orc.ploc(tris, exp_perm, radius=16)
+    ech, ebx, it = _expected_topology(orc, tris, codes, exp_perm, clustering)
     np.testing.assert_array_equal(ch, ech)
     np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
 
 
+@pytest.mark.parametrize("clustering", CLUSTERINGS)
 @pytest.mark.parametrize("kind", [A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmc])
-def test_ploc_topology_with_non_finite_triangles(orc, kind):
+def test_ploc_topology_with_non_finite_triangles(orc, kind, clustering):
     """Triangles with NaN or infinite coordinates (never hittable) get empty boxes and stay out of the scene
     bounds on the device exactly as in the restatement: same codes, same topology, same boxes."""
     tris = S.soup(5000, seed=21).copy()
@@ -106,35 +120,46 @@ def test_ploc_topology_with_non_finite_triangles(orc, kind):
     for k, i in enumerate(bad):
         tris[i, rng.integers(3), rng.integers(3)] = [np.nan, np.inf, -np.inf][k % 3]
     tris[bad[:20]] = np.nan
-    bvh = build(tris, kind)
+    bvh = build(tris, kind, clustering=clustering)
     perm, ch, bx = bvh.download_topology()
     codes = orc.morton30(tris) if kind is A.AccelerationStructureType.kPloc else orc.emc60(tris)
     exp_perm = O.sort_perm(codes)
     np.testing.assert_array_equal(perm, exp_perm)
-    ech, ebx, it = orc.ploc(tris, exp_perm, radius=16)
+    ech, ebx, it = _expected_topology(orc, tris, codes, exp_perm, clustering)
     np.testing.assert_array_equal(ch, ech)
     np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
     assert np.isfinite(ebx[~np.isinf(ebx).all(axis=1)]).all()
 
 
-def test_ploc_topology_1m_displaced_sphere(orc):
+@pytest.mark.parametrize("clustering", CLUSTERINGS)
+def test_ploc_topology_1m_displaced_sphere(orc, clustering):
     tris = S.uv_sphere(1024, 512, 1.0, (0, 0, 0), displacement=0.05, seed=2)
-    bvh = build(tris)
+    bvh = build(tris, clustering=clustering)
     perm, ch, bx = bvh.download_topology()
-    exp_perm = O.sort_perm(orc.morton30(tris))
+    codes = orc.morton30(tris)
+    exp_perm = O.sort_perm(codes)
     np.testing.assert_array_equal(perm, exp_perm)
-    ech, ebx, it = orc.ploc(tris, exp_perm, radius=16)
+    ech, ebx, it = _expected_topology(orc, tris, codes, exp_perm, clustering)
     np.testing.assert_array_equal(ch, ech)
     assert bvh.info().ploc_iterations == it
 
 
-def test_sah_cost_matches_oracle_on_same_topology(orc):
+@pytest.mark.parametrize("clustering", CLUSTERINGS)
+def test_sah_cost_matches_oracle_on_same_topology(orc, clustering):
     tris = S.soup(20000, seed=21)
-    bvh = build(tris)
+    bvh = build(tris, clustering=clustering)
     perm, ch, bx = bvh.download_topology()
     leaf_boxes = np.concatenate([tris[perm].min(axis=1), tris[perm].max(axis=1)], axis=1)
     expect = O.sah_cost_binary(ch, bx, len(tris), leaf_boxes, 4)
     assert bvh.sah_cost() == pytest.approx(expect, rel=1e-9)
+
+
+def test_hierarchical_clustering_sah_close_to_global_ploc(orc):
+    """The hierarchical clustering's tree costs about what the global PLOC loop's does (same distance, same tie
+    rule, merges confined to radix-tree nodes): within 2% on a soup and on a displaced sphere."""
+    for tris in (S.soup(200_000, seed=8), S.uv_sphere(256, 128, 1.0, (0, 0, 0), displacement=0.05, seed=2)):
+        costs = [build(tris, clustering=c).sah_cost() for c in CLUSTERINGS]
+        assert costs[0] == pytest.approx(costs[1], rel=0.02), costs
 
 
 def test_build_rejects_bad_options():

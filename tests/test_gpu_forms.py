@@ -54,70 +54,110 @@ def test_reintersect_f64_matches_oracle(orc):
     assert np.max(np.abs(t32 - t64[hit]) / t64[hit]) < 1e-4
 
 
-def test_adjoint_matches_fp64_central_differences():
-    """dL/dvertex of L = sum (t - t_target)^2 against FP64 central differences (h = 1e-4) with hit ids fixed."""
+def _tuv64(T, O, D):
+    """FP64 (t, u, v) of rays O + t D against triangles T (K, 3, 3): the closest-hit system solved by Cramer's rule
+    (the Moller-Trumbore algebra of src/scene/triangle.cc:10-43 without its culling)."""
+    a, b, c = T[:, 0], T[:, 1], T[:, 2]
+    e1, e2, s = b - a, c - a, O - a
+    p = np.cross(D, e2)
+    det = (e1 * p).sum(1)
+    q = np.cross(s, e1)
+    return (e2 * q).sum(1) / det, (s * p).sum(1) / det, (D * q).sum(1) / det
+
+
+@pytest.mark.parametrize("loss_kind", ["depth", "depth_and_barycentrics"])
+def test_adjoint_matches_fp64_central_differences(loss_kind):
+    """The differentiation configuration at full size: a 256x128 displaced sphere (65,024 triangles, indexed, so a
+    mesh vertex is shared by up to six triangles) and 1024x1024 pinhole rays. Loss = sum over rays hitting both
+    meshes of (t - t*)^2, and with "depth_and_barycentrics" also (u - u*)^2 + (v - v*)^2, where t*, u*, v* are
+    the hits of a second, differently displaced sphere (the seeded target). The adjoint's gradients with respect
+    to 1000 sampled mesh vertices and to 200 ray origins and directions are checked against FP64 central
+    differences (h = 1e-4) of the same loss with the hit ids held fixed."""
     from diplodocus_b200.autograd import closest_hit_tuv
-    verts, idx, rays = S.diff_scene(nu=64, nv=32, width=64, height=64)
+    verts, idx, rays = S.diff_scene()
+    tverts, tidx = S.uv_sphere_indexed(256, 128, 1.0, (0.0, 0.0, 0.0), displacement=0.05, seed=6)
+    assert len(idx) == 65024 and len(rays) == 1 << 20
     tris = verts[idx].astype(np.float32)
     bvh = build(tris)
-    v0, v1, v2 = (torch.from_numpy(np.ascontiguousarray(tris[:, k])).cuda().requires_grad_(True) for k in range(3))
+    tp, tt, tu, tv = trace(build(tverts[tidx].astype(np.float32)), rays)
+    V = torch.from_numpy(verts.astype(np.float32)).cuda().requires_grad_(True)
+    it = torch.from_numpy(idx).cuda()
+    v0, v1, v2 = (V[it[:, k]] for k in range(3))  # per-triangle corners gathered from the shared vertices
     o = torch.from_numpy(rays[:, 0:3].copy()).cuda().requires_grad_(True)
     d = torch.from_numpy(rays[:, 4:7].copy()).cuda().requires_grad_(True)
     t, u, v, prim = closest_hit_tuv(v0, v1, v2, o, d, bvh, tmax=100.0)
-    hit = prim >= 0
-    assert hit.sum() > 500
-    target = torch.where(hit, t.detach() * 0.97, torch.zeros_like(t))
-    loss = torch.where(hit, (t - target) ** 2, torch.zeros_like(t)).sum()
-    loss.backward()
-    g = [x.grad.detach().cpu().numpy().astype(np.float64) for x in (v0, v1, v2)]
-    # FP64 oracle: the loss as a function of one vertex coordinate, hit ids held fixed
     prim_np = prim.cpu().numpy()
-    tgt = target.cpu().numpy().astype(np.float64)
-    R = rays.astype(np.float64)
-    T = tris.astype(np.float64)
-
-    def loss64(Tm, Rm=R):
-        sel = prim_np >= 0
-        a, b, c = Tm[prim_np[sel], 0], Tm[prim_np[sel], 1], Tm[prim_np[sel], 2]
-        oo, dd = Rm[sel, 0:3], Rm[sel, 4:7]
-        e1, e2, s = b - a, c - a, oo - a
-        p = np.cross(dd, e2)
-        det = (e1 * p).sum(1)
-        q = np.cross(s, e1)
-        tt = (e2 * q).sum(1) / det
-        return ((tt - tgt[sel]) ** 2).sum()
-
-    rng = np.random.default_rng(0)
-    hit_tris = np.unique(prim_np[prim_np >= 0])
-    errs = []
-    for _ in range(1000):
-        tri = int(rng.choice(hit_tris))
-        k = int(rng.integers(0, 3))
-        a = int(rng.integers(0, 3))
-        h = 1e-4
-        Tp = T.copy()
-        Tp[tri, k, a] += h
-        Tm = T.copy()
-        Tm[tri, k, a] -= h
-        fd = (loss64(Tp) - loss64(Tm)) / (2 * h)
-        ad = g[k][tri, a]
-        errs.append(abs(ad - fd) / max(abs(fd), 1e-3))
-    errs = np.array(errs)
-    assert np.median(errs) < 1e-3 and np.quantile(errs, 0.95) < 2e-2, (np.median(errs), np.quantile(errs, 0.95))
-    # ray origins and directions against the same FP64 central differences
+    sel = (prim_np >= 0) & (tp >= 0)
+    assert sel.sum() > 200_000
+    w_uv = 1.0 if loss_kind == "depth_and_barycentrics" else 0.0
+    m = torch.from_numpy(sel).cuda()
+    tgt = [torch.from_numpy(x.astype(np.float32)).cuda() for x in (tt, tu, tv)]
+    zero = torch.zeros_like(t)
+    loss = (torch.where(m, (t - tgt[0]) ** 2, zero).sum()
+            + w_uv * torch.where(m, (u - tgt[1]) ** 2 + (v - tgt[2]) ** 2, zero).sum())
+    loss.backward()
+    gV = V.grad.detach().cpu().numpy().astype(np.float64)
     go = o.grad.detach().cpu().numpy().astype(np.float64)
     gd = d.grad.detach().cpu().numpy().astype(np.float64)
+
+    # FP64 oracle. Only the rays that hit a triangle touching the perturbed vertex change, so each difference is
+    # taken over those rays (the other terms cancel exactly).
+    Vd = verts.astype(np.float32).astype(np.float64)
+    R = rays.astype(np.float64)
+    T64 = (tt.astype(np.float64), tu.astype(np.float64), tv.astype(np.float64))
+    rays_sel = np.nonzero(sel)[0]
+    order = np.argsort(prim_np[rays_sel], kind="stable")
+    by_tri = rays_sel[order]
+    starts = np.searchsorted(prim_np[by_tri], np.arange(len(idx) + 1))
+    tris_of_vertex = [[] for _ in range(len(verts))]
+    for tri, corners in enumerate(idx):
+        for c in corners:
+            tris_of_vertex[c].append(tri)
+
+    def loss_terms(Vm, ray_ids):
+        T = Vm[idx[prim_np[ray_ids]]]
+        t64, u64, v64 = _tuv64(T, R[ray_ids, 0:3], R[ray_ids, 4:7])
+        out = (t64 - T64[0][ray_ids]) ** 2
+        if w_uv:
+            out = out + (u64 - T64[1][ray_ids]) ** 2 + (v64 - T64[2][ray_ids]) ** 2
+        return out.sum()
+
+    rng = np.random.default_rng(7)
+    hit_vertices = np.unique(idx[np.unique(prim_np[rays_sel])])
+    h = 1e-4
+    errs = []
+    for vert in rng.choice(hit_vertices, 1000, replace=False):
+        ray_ids = np.concatenate([by_tri[starts[tri]:starts[tri + 1]] for tri in tris_of_vertex[vert]])
+        a = int(rng.integers(0, 3))
+        Vp, Vm = Vd.copy(), Vd.copy()
+        Vp[vert, a] += h
+        Vm[vert, a] -= h
+        fd = (loss_terms(Vp, ray_ids) - loss_terms(Vm, ray_ids)) / (2 * h)
+        errs.append(abs(gV[vert, a] - fd) / max(abs(fd), 1e-3))
+    errs = np.array(errs)
+    assert np.median(errs) < 1e-3 and np.quantile(errs, 0.95) < 2e-2, (np.median(errs), np.quantile(errs, 0.95))
+
+    def ray_loss(Rm, ray):
+        T = Vd[idx[prim_np[ray]]][None]
+        t64, u64, v64 = _tuv64(T, Rm[None, 0:3], Rm[None, 4:7])
+        out = (t64[0] - T64[0][ray]) ** 2
+        if w_uv:
+            out += (u64[0] - T64[1][ray]) ** 2 + (v64[0] - T64[2][ray]) ** 2
+        return out
+
     rerr = []
-    for ray in rng.choice(np.nonzero(prim_np >= 0)[0], 100, replace=False):
+    for ray in rng.choice(rays_sel, 200, replace=False):
         for col, grad in ((0, go), (4, gd)):
             a = int(rng.integers(0, 3))
-            Rp, Rm = R.copy(), R.copy()
-            Rp[ray, col + a] += 1e-4
-            Rm[ray, col + a] -= 1e-4
-            fd = (loss64(T, Rp) - loss64(T, Rm)) / 2e-4
+            Rp, Rm = R[ray].copy(), R[ray].copy()
+            Rp[col + a] += h
+            Rm[col + a] -= h
+            fd = (ray_loss(Rp, ray) - ray_loss(Rm, ray)) / (2 * h)
             rerr.append(abs(grad[ray, a] - fd) / max(abs(fd), 1e-3))
     rerr = np.array(rerr)
     assert np.median(rerr) < 1e-3 and np.quantile(rerr, 0.95) < 2e-2, (np.median(rerr), np.quantile(rerr, 0.95))
+    # rays outside the loss get no gradient
+    assert np.all(go[~sel] == 0.0) and np.all(gd[~sel] == 0.0)
 
 
 def test_build_plan_graph_replay_matches_fresh_builds(orc):

@@ -321,3 +321,42 @@ def test_nan_and_inf_vertices(orc, kind, layout):
     np.testing.assert_array_equal(fbits(t), fbits(ref.t))
     np.testing.assert_array_equal(fbits(u), fbits(ref.u))
     bvh.check_errors()
+
+
+@pytest.mark.parametrize("workload", ["sphere", "soup"])
+def test_reordered_trace_equals_given_order(workload):
+    """Batches of 2^20 rays or more are traced in a coherent order of their own; the records are bit-identical to
+    tracing in the given order (and, with counters, so are the visit and test totals)."""
+    if workload == "sphere":
+        tris, rays = S.displaced_sphere(nu=256, nv=128, n_rays=1 << 20)
+    else:
+        tris, rays = S.soup(200_000, seed=5), S.random_rays((1 << 20) + 77, seed=5)
+    bvh = build(tris, A.AccelerationStructureType.kPlocEmc)
+    rd = torch.from_numpy(rays).cuda()
+    st_a, st_b = A.Stats(), A.Stats()
+    a = bvh.Intersect(st_a, rd, count=True)
+    b = bvh.Intersect(st_b, rd, count=True, keep_order=True)
+    torch.cuda.synchronize()
+    bvh.check_errors()
+    assert torch.equal(a.raw, b.raw)
+    assert st_a.accel_stats.traversal_count == st_b.accel_stats.traversal_count
+    assert st_a.accel_stats.intersection_count == st_b.accel_stats.intersection_count
+
+
+@pytest.mark.parametrize("name", ["small_scene", "displaced_sphere_64x32", "soup_2k"])
+@pytest.mark.parametrize("clustering", ["hploc", "ploc"])
+def test_counted_trace_totals_equal_a_host_retraversal(orc, name, clustering):
+    """The node-visit and triangle-test counters (the reference's traversal_count / intersection_count, sbvh.cc:76,83)
+    equal a host re-traversal of the downloaded layout, ray for ray summed: the rays whose slab decisions are too
+    close to call under the device's approximate reciprocal are left out of both sides."""
+    g = load_golden(name)
+    bvh = build(g["tris"], clustering=clustering)
+    nodes, tris, root = bvh.download_layout()
+    visits, tests, stable, prim, t = orc.retrace_binary(nodes, tris, root, g["rays"])
+    assert stable.mean() > 0.95
+    np.testing.assert_array_equal(prim[stable], g["brute_prim"][stable])  # the re-traversal is a correct trace
+    st = A.Stats()
+    bvh.Intersect(st, torch.from_numpy(np.ascontiguousarray(g["rays"][stable])), count=True)
+    torch.cuda.synchronize()
+    assert st.accel_stats.traversal_count == int(visits[stable].sum())
+    assert st.accel_stats.intersection_count == int(tests[stable].sum())
