@@ -32,7 +32,8 @@ EXPORTS = [
     "dipl_bvh_trace_closest_counted", "dipl_bvh_trace_any", "dipl_bvh_sah_cost", "dipl_bvh_get_info",
     "dipl_bvh_download_topology", "dipl_bvh_download_layout", "dipl_bvh_check_errors", "dipl_bvh_destroy", "dipl_compute_codes",
     "dipl_radix_sort_pairs", "dipl_radix_sort_pairs_noalloc", "dipl_reintersect_f64", "dipl_trace_adjoint",
-    "dipl_generate_pinhole_rays", "dipl_generate_bounce_rays", "dipl_selftest_bounded_waits",
+    "dipl_generate_pinhole_rays", "dipl_generate_bounce_rays", "dipl_generate_shadow_rays",
+    "dipl_selftest_bounded_waits",
     "dipl_obj_scene_load", "dipl_obj_scene_get_info", "dipl_obj_scene_get_triangles", "dipl_obj_scene_get_soa",
     "dipl_obj_scene_get_materials", "dipl_obj_scene_get_lights", "dipl_obj_scene_destroy",
     "dipl_set_limits", "dipl_get_limits", "dipl_status_string",
@@ -115,6 +116,7 @@ def load(path: str = LIB_PATH):
         "dipl_trace_adjoint": (i32, [vp, vp, vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]),
         "dipl_generate_pinhole_rays": (i32, [C.POINTER(Camera), i32, i32, vp, vp]),
         "dipl_generate_bounce_rays": (i32, [vp, vp, vp, vp, vp, i64, u32, vp, vp]),
+        "dipl_generate_shadow_rays": (i32, [vp, vp, vp, vp, vp, i64, i32, vp, i32, i32, vp, i32, u32, vp, vp]),
         "dipl_selftest_bounded_waits": (i32, [u32, vp, vp]),
         "dipl_obj_scene_load": (i32, [C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
         "dipl_obj_scene_get_info": (i32, [vp, C.POINTER(ObjSceneInfo)]),

@@ -383,12 +383,44 @@ def generate_bounce_rays(v, rays: torch.Tensor, hits: Hits, seed: int) -> torch.
     return out
 
 
-def trace_frame(bvh: "GpuPlocBvh", camera: dict, width: int, height: int, seed: int, stats: "Stats | None" = None):
+def generate_shadow_rays(v, rays: torch.Tensor, hits: Hits, width: int, area_light_triangles=(), samples: int = 1,
+                         point_lights=(), seed: int = 42) -> torch.Tensor:
+    """Shadow rays of every hit toward the lights (dipl_generate_shadow_rays): (R * per_hit, 8), per_hit = area
+    lights x samples + point lights, in the reference's light order; null rays where the reference casts none."""
+    lib = L.load()
+    n = rays.shape[0]
+    dev = rays.device
+    area = torch.as_tensor(np.asarray(area_light_triangles, np.int32).reshape(-1), device=dev)
+    points = torch.as_tensor(np.asarray(point_lights, np.float32).reshape(-1, 3), device=dev).contiguous()
+    per_hit = area.numel() * samples + points.shape[0]
+    out = torch.empty((n * per_hit, 8), dtype=torch.float32, device=dev)
+    L.check(lib.dipl_generate_shadow_rays(_ptr(v[0]), _ptr(v[1]), _ptr(v[2]), _ptr(rays), _ptr(hits.raw), n,
+                                          int(width), _ptr(area), int(area.numel()), int(samples), _ptr(points),
+                                          int(points.shape[0]), int(seed) & 0xFFFFFFFF, _ptr(out), _stream()),
+            "dipl_generate_shadow_rays")
+    return out
+
+
+@dataclass
+class Lights:
+    """The lights of a frame's shadow wave: area lights (triangle ids) sampled ``samples`` times each (the reference
+    RenderConfig's area_light_sample_cnt) and point lights (positions)."""
+    area_light_triangles: tuple = ()
+    samples: int = 1
+    point_lights: tuple = ()
+    seed: int = 42  # the reference's area-light sampling seed (cpu_raytracer.cc:181-182)
+
+
+def trace_frame(bvh: "GpuPlocBvh", camera: dict, width: int, height: int, seed: int, stats: "Stats | None" = None,
+                lights: "Lights | None" = None):
     """One wavefront frame of the renderer path: primary rays, their closest hits, one bounce ray per hit and
-    the bounce hits, all on the device. Returns (primary rays, primary hits, bounce rays, bounce hits).
+    the bounce hits, all on the device. Returns (primary rays, primary hits, bounce rays, bounce hits); with
+    ``lights``, also (shadow rays, occluded flags) of the primary hits' shadow wave (IsShadowed through
+    dipl_bvh_trace_any).
 
     With ``stats``, adds the frame to its RaytracingStats (time in seconds, synchronised; width * height primary
-    rays; one secondary ray per primary hit, the bounces that carry a ray) and its AccelerationStats queries."""
+    rays; one secondary ray per primary hit, the bounces that carry a ray; one shadow ray per cast shadow ray) and its
+    AccelerationStats queries."""
     st = stats if stats is not None else Stats()
     t0 = time.perf_counter()
     rays = generate_pinhole_rays(camera["cam_pos"], camera["cam_dir"], camera["cam_up"], camera["fov"],
@@ -396,11 +428,20 @@ def trace_frame(bvh: "GpuPlocBvh", camera: dict, width: int, height: int, seed: 
     hits = bvh.Intersect(st, rays)
     bounce = generate_bounce_rays(bvh._v, rays, hits, seed)
     bhits = bvh.Intersect(st, bounce)
+    shadow = occluded = None
+    if lights is not None:
+        shadow = generate_shadow_rays(bvh._v, rays, hits, width, lights.area_light_triangles, lights.samples,
+                                      lights.point_lights, lights.seed)
+        occluded = bvh.IntersectAny(st, shadow)
     if stats is not None:
         secondary = int((hits.prim >= 0).sum().item())  # synchronises the stream
         stats.rt_stats.raytracing_time += time.perf_counter() - t0
         stats.rt_stats.primary_ray_count += int(width) * int(height)
         stats.rt_stats.secondary_ray_count += secondary
+        if shadow is not None:
+            stats.rt_stats.shadow_ray_count += int((shadow[:, 7] > 0).sum().item())
+    if lights is not None:
+        return rays, hits, bounce, bhits, shadow, occluded
     return rays, hits, bounce, bhits
 
 

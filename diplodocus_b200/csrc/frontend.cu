@@ -129,6 +129,91 @@ __global__ void __launch_bounds__(kGenThreads) bounce_kernel(const float* __rest
     o4[1] = make_float4(d.x, d.y, d.z, kInfinity);
 }
 
+// Normalize with the reference's cut-off (src/util/vec3.h:111-117): a vector of length <= kEpsilon becomes 0.
+__device__ __forceinline__ V3 v_normalize_ref(V3 v) {
+    const float len = __fsqrt_rn(v_dot(v, v));
+    if (len <= kEpsilon) return {0.0f, 0.0f, 0.0f};
+    return {__fdiv_rn(v.x, len), __fdiv_rn(v.y, len), __fdiv_rn(v.z, len)};
+}
+
+// RandomAreaLightSample01 (src/renderer/cpu_raytracer.cc:28-40): a key of seed, pixel, light and sample, hashed.
+__device__ __forceinline__ float area_light_sample01(uint32_t seed, uint32_t px, uint32_t py, uint32_t light,
+                                                     uint32_t sample, uint32_t dim) {
+    uint32_t key = 0;
+    key ^= seed * 0x9e3779b1U;
+    key ^= px * 0x165667b1U;
+    key ^= py * 0xd3a2646cU;
+    key ^= light * 0x85ebca6bU;
+    key ^= sample * 0xc2b2ae35U;
+    key ^= dim * 0x27d4eb2fU;
+    return (float)(hash_u32(key) >> 8) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ V3 ld_v3(const float* p, int64_t i) { return {__ldg(p + 3 * i), __ldg(p + 3 * i + 1), __ldg(p + 3 * i + 2)}; }
+
+// One shadow ray per (hit, light sample): CpuRaytracer::IsShadowed (src/renderer/cpu_raytracer.cc:222-237) with the
+// hit record of the closest-hit trace (position Ray::At(t), RayEpsilon, the triangle's geometric normal) and the
+// light sample of LocalIlluminationAreaLights (:165-186; Triangle::SampleSurface, src/scene/triangle.cc:45-53) or
+// a point light (:202-218). Rays that cast nothing get tmax = 0 (never occluded).
+__global__ void __launch_bounds__(kGenThreads) shadow_kernel(const float* __restrict__ v0, const float* __restrict__ v1,
+                                                             const float* __restrict__ v2,
+                                                             const dipl_ray* __restrict__ rays,
+                                                             const dipl_hit* __restrict__ hits, int64_t n, int width,
+                                                             const int32_t* __restrict__ area, int num_area,
+                                                             int samples, const float* __restrict__ points,
+                                                             int num_point, uint32_t seed, dipl_ray* __restrict__ out) {
+    const int per_hit = num_area * samples + num_point;
+    const int64_t j = blockIdx.x * (int64_t)kGenThreads + threadIdx.x;
+    if (j >= n * per_hit) return;
+    const int64_t i = j / per_hit;
+    const int k = (int)(j - i * per_hit);
+    float4* o4 = reinterpret_cast<float4*>(out + j);
+    const float4 none0 = make_float4(0.0f, 0.0f, 0.0f, kEpsilon), none1 = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    const int4 h = __ldg(reinterpret_cast<const int4*>(hits) + i);
+    if (h.x < 0) {
+        o4[0] = none0, o4[1] = none1;
+        return;
+    }
+    V3 light;
+    if (k < num_area * samples) {
+        const int al = k / samples, smp = k - al * samples;
+        for (int q = 0; q <= al; ++q)  // the hit is an area light: the reference returns its colour, no more rays
+            if (__ldg(area + q) == h.x) {
+                o4[0] = none0, o4[1] = none1;
+                return;
+            }
+        const uint32_t px = (uint32_t)(i % width), py = (uint32_t)(i / width);
+        const float r1 = area_light_sample01(seed, px, py, (uint32_t)al, (uint32_t)smp, 0u);
+        const float r2 = area_light_sample01(seed, px, py, (uint32_t)al, (uint32_t)smp, 1u);
+        const bool flip = __fadd_rn(r1, r2) > 1.0f;
+        const float u = flip ? __fsub_rn(1.0f, r1) : r1, w = flip ? __fsub_rn(1.0f, r2) : r2;
+        const int64_t lt = __ldg(area + al);
+        const V3 a = ld_v3(v0, lt), b = ld_v3(v1, lt), c = ld_v3(v2, lt);
+        light = v_add(v_add(a, v_scale(v_sub(b, a), u)), v_scale(v_sub(c, a), w));
+    } else {
+        const int pl = k - num_area * samples;
+        light = {__ldg(points + 3 * pl), __ldg(points + 3 * pl + 1), __ldg(points + 3 * pl + 2)};
+    }
+    const float4 ra = __ldg(reinterpret_cast<const float4*>(rays + i)), rb = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
+    const float t = __int_as_float(h.y);
+    const V3 pos = v_add(V3{ra.x, ra.y, ra.z}, v_scale(V3{rb.x, rb.y, rb.z}, t));  // Ray::At
+    const float eps = ray_epsilon(pos, t);
+    const int64_t p = h.x;
+    const V3 ta = ld_v3(v0, p), tb = ld_v3(v1, p), tc = ld_v3(v2, p);
+    const V3 ng = v_normalize_ref(v_cross(v_sub(tb, ta), v_sub(tc, ta)));  // RecomputeTriangleGeometricNormal
+    const V3 to_light = v_sub(light, pos);
+    const float dist = __fsqrt_rn(v_dot(to_light, to_light));  // Length
+    if (dist < kEpsilon) {  // on the light's surface: not shadowed
+        o4[0] = none0, o4[1] = none1;
+        return;
+    }
+    const V3 dir = {__fdiv_rn(to_light.x, dist), __fdiv_rn(to_light.y, dist), __fdiv_rn(to_light.z, dist)};
+    const V3 off = v_dot(dir, ng) > 0.0f ? ng : V3{-ng.x, -ng.y, -ng.z};  // OffsetRayOrigin (:42-47)
+    const V3 org = v_add(pos, v_scale(off, eps));
+    o4[0] = make_float4(org.x, org.y, org.z, kEpsilon);
+    o4[1] = make_float4(dir.x, dir.y, dir.z, __fmul_rn(dist, __fsub_rn(1.0f, eps)));
+}
+
 // Camera basis on the host, the reference renderers' formula (cpu_raytracer.cc:64-70) in FP32; 2 tan(fov/2) is
 // evaluated once in double precision (tan of the FP32 half angle, rounded to FP32).
 CameraBasis camera_basis(const dipl_camera& c, int w, int h) {
@@ -185,6 +270,35 @@ extern "C" dipl_status dipl_generate_bounce_rays(const float* d_v0, const float*
     DIPL_CHECK_ARG(d_out != d_rays, "d_out may not alias d_rays");
     bounce_kernel<<<(unsigned)((n + kGenThreads - 1) / kGenThreads), kGenThreads, 0, static_cast<cudaStream_t>(stream)>>>(
         d_v0, d_v1, d_v2, d_rays, d_hits, n, seed, d_out);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return DIPL_OK;
+}
+
+extern "C" dipl_status dipl_generate_shadow_rays(const float* d_v0, const float* d_v1, const float* d_v2,
+                                                 const dipl_ray* d_rays, const dipl_hit* d_hits, int64_t n,
+                                                 int32_t width, const int32_t* d_area_light_triangles,
+                                                 int32_t num_area_lights, int32_t samples, const float* d_point_lights,
+                                                 int32_t num_point_lights, uint32_t seed, dipl_ray* d_out,
+                                                 void* stream) {
+    DIPL_CHECK_ARG(n >= 0 && width >= 1 && num_area_lights >= 0 && num_point_lights >= 0 && samples >= 0,
+                   "n, lights and samples must be >= 0 and width >= 1");
+    DIPL_CHECK_ARG(num_area_lights == 0 || samples >= 1, "area lights need samples >= 1");
+    const int64_t per_hit = (int64_t)num_area_lights * samples + num_point_lights;
+    DIPL_CHECK_ARG(per_hit <= (1 << 20), "at most 2^20 shadow rays per hit");
+    if (n == 0 || per_hit == 0) return DIPL_OK;
+    DIPL_CHECK_ARG(d_v0 && d_v1 && d_v2 && d_rays && d_hits && d_out, "arrays must be non-NULL");
+    DIPL_CHECK_ARG(num_area_lights == 0 || d_area_light_triangles, "d_area_light_triangles must be non-NULL");
+    DIPL_CHECK_ARG(num_point_lights == 0 || d_point_lights, "d_point_lights must be non-NULL");
+    DIPL_CHECK_ARG((reinterpret_cast<uintptr_t>(d_rays) & 15) == 0 && (reinterpret_cast<uintptr_t>(d_hits) & 15) == 0 &&
+                       (reinterpret_cast<uintptr_t>(d_out) & 15) == 0,
+                   "rays, hits and output must be 16-byte aligned");
+    DIPL_CHECK_ARG(d_out != d_rays, "d_out may not alias d_rays");
+    const int64_t total = n * per_hit;
+    shadow_kernel<<<(unsigned)((total + kGenThreads - 1) / kGenThreads), kGenThreads, 0,
+                    static_cast<cudaStream_t>(stream)>>>(d_v0, d_v1, d_v2, d_rays, d_hits, n, width,
+                                                         d_area_light_triangles, num_area_lights, samples,
+                                                         d_point_lights, num_point_lights, seed, d_out);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
     return DIPL_OK;

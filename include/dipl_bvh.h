@@ -289,6 +289,25 @@ DIPL_API dipl_status dipl_generate_bounce_rays(const float* d_v0, const float* d
                                                const dipl_ray* d_rays, const dipl_hit* d_hits, int64_t n,
                                                uint32_t seed, dipl_ray* d_out, void* stream);
 
+/* Shadow rays of the renderer's local illumination, one per (hit, light sample), for dipl_bvh_trace_any.
+ * Replaces the shadow-ray set-up of IsShadowed (src/renderer/cpu_raytracer.cc:222-237,
+ * src/gpu/renderer/gpu_renderer_util.h:96-108) around the hit record the reference makes (Ray::At(t), RayEpsilon,
+ * the triangle's geometric normal): dir = (light - pos) / |light - pos|, origin offset by RayEpsilon along the
+ * normal on dir's side (OffsetRayOrigin), tmax = |light - pos| (1 - RayEpsilon). Lights, in the reference's order:
+ * num_area_lights area lights (triangle ids of the vertex arrays) with `samples` samples each, drawn as
+ * LocalIlluminationAreaLights does (cpu_raytracer.cc:165-186: RandomAreaLightSample01(seed, x, y, light, sample, dim)
+ * over ray i's pixel x = i % width, y = i / width, then Triangle::SampleSurface; the reference's seed is 42), then
+ * num_point_lights point lights (d_point_lights: xyz per light). Output: d_out[i * per_hit + j] with
+ * per_hit = num_area_lights * samples + num_point_lights. A ray that casts no shadow ray for a light gets a null ray
+ * (tmax = 0, never occluded): a miss; a hit on an area light's own triangle (the reference returns the light's
+ * colour and casts no more area-light rays for that hit); a light within kEpsilon of the hit point.
+ * FP32 IEEE arithmetic in the reference's order, so the records are reproducible bit for bit on the host. */
+DIPL_API dipl_status dipl_generate_shadow_rays(const float* d_v0, const float* d_v1, const float* d_v2,
+                                               const dipl_ray* d_rays, const dipl_hit* d_hits, int64_t n, int32_t width,
+                                               const int32_t* d_area_light_triangles, int32_t num_area_lights,
+                                               int32_t samples, const float* d_point_lights, int32_t num_point_lights,
+                                               uint32_t seed, dipl_ray* d_out, void* stream);
+
 /* No counterpart in the reference. Failure-detection self-test: runs the library's bounded device waits (the
  * warp and block decoupled look-backs of the sort and the clustering, and the grid barrier between clustering
  * iterations) on a status word that no tile publishes and on a barrier with one participant that never

@@ -992,3 +992,79 @@ void orc_bounce_rays(const float* tris, const float* rays, const int32_t* prim, 
         q[4] = d.x, q[5] = d.y, q[6] = d.z, q[7] = ORC_INF;
     }
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* Shadow rays of the frontend (dipl_generate_shadow_rays): CpuRaytracer::IsShadowed          */
+/* (src/renderer/cpu_raytracer.cc:222-237) around the reference's hit record, with the light     */
+/* samples of LocalIlluminationAreaLights (:165-186: RandomAreaLightSample01 :28-40, then       */
+/* Triangle::SampleSurface, src/scene/triangle.cc:45-53) and the point lights (:202-218).       */
+/* ------------------------------------------------------------------------------------------ */
+static float orc_area_light_sample01(uint32_t seed, uint32_t px, uint32_t py, uint32_t light, uint32_t sample,
+                                     uint32_t dim) {
+    uint32_t key = 0;
+    key ^= seed * 0x9e3779b1U;
+    key ^= px * 0x165667b1U;
+    key ^= py * 0xd3a2646cU;
+    key ^= light * 0x85ebca6bU;
+    key ^= sample * 0xc2b2ae35U;
+    key ^= dim * 0x27d4eb2fU;
+    return (float)(orc_hash_u32(key) >> 8) * (1.0f / 16777216.0f);
+}
+
+/* Normalize with the reference's cut-off (src/util/vec3.h:111-117). */
+static orc_v3 v3_normalize_ref(orc_v3 v) {
+    float len = sqrtf(v3_dot(v, v));
+    orc_v3 z = {0.0f, 0.0f, 0.0f};
+    if (len <= ORC_EPS) return z;
+    orc_v3 r = {v.x / len, v.y / len, v.z / len};
+    return r;
+}
+
+/* out: n * per_hit rays, per_hit = num_area * samples + num_point; area: triangle ids; points: xyz per light. */
+void orc_shadow_rays(const float* tris, const float* rays, const int32_t* prim, const float* t, int64_t n, int width,
+                     const int32_t* area, int num_area, int samples, const float* points, int num_point, uint32_t seed,
+                     float* out) {
+    const int per_hit = num_area * samples + num_point;
+    for (int64_t i = 0; i < n; ++i) {
+        for (int k = 0; k < per_hit; ++k) {
+            float* q = out + 8 * (i * per_hit + k);
+            q[0] = 0.0f, q[1] = 0.0f, q[2] = 0.0f, q[3] = ORC_EPS, q[4] = 0.0f, q[5] = 0.0f, q[6] = 1.0f, q[7] = 0.0f;
+            if (prim[i] < 0) continue;
+            orc_v3 light;
+            if (k < num_area * samples) {
+                int al = k / samples, smp = k - al * samples, lit = 0;
+                for (int qq = 0; qq <= al; ++qq)
+                    if (area[qq] == prim[i]) lit = 1;
+                if (lit) continue;
+                uint32_t px = (uint32_t)(i % width), py = (uint32_t)(i / width);
+                float r1 = orc_area_light_sample01(seed, px, py, (uint32_t)al, (uint32_t)smp, 0u);
+                float r2 = orc_area_light_sample01(seed, px, py, (uint32_t)al, (uint32_t)smp, 1u);
+                float u = r1 + r2 > 1.0f ? 1.0f - r1 : r1;
+                float w = r1 + r2 > 1.0f ? 1.0f - r2 : r2;
+                const float* lt = tris + 9 * (int64_t)area[al];
+                orc_v3 a = {lt[0], lt[1], lt[2]}, b = {lt[3], lt[4], lt[5]}, c = {lt[6], lt[7], lt[8]};
+                light = v3_add(v3_add(a, v3_scale(v3_sub(b, a), u)), v3_scale(v3_sub(c, a), w));
+            } else {
+                const float* pl = points + 3 * (k - num_area * samples);
+                orc_v3 l = {pl[0], pl[1], pl[2]};
+                light = l;
+            }
+            const float* r = rays + 8 * i;
+            orc_v3 o = {r[0], r[1], r[2]}, din = {r[4], r[5], r[6]};
+            orc_v3 pos = v3_add(o, v3_scale(din, t[i]));
+            float eps = orc_ray_epsilon(pos, t[i]);
+            const float* tri = tris + 9 * (int64_t)prim[i];
+            orc_v3 a = {tri[0], tri[1], tri[2]}, b = {tri[3], tri[4], tri[5]}, c = {tri[6], tri[7], tri[8]};
+            orc_v3 ng = v3_normalize_ref(v3_cross(v3_sub(b, a), v3_sub(c, a)));
+            orc_v3 to_light = v3_sub(light, pos);
+            float dist = sqrtf(v3_dot(to_light, to_light));
+            if (dist < ORC_EPS) continue;
+            orc_v3 dir = {to_light.x / dist, to_light.y / dist, to_light.z / dist};
+            orc_v3 off = ng;
+            if (!(v3_dot(dir, ng) > 0.0f)) off.x = -ng.x, off.y = -ng.y, off.z = -ng.z;
+            orc_v3 org = v3_add(pos, v3_scale(off, eps));
+            q[0] = org.x, q[1] = org.y, q[2] = org.z, q[3] = ORC_EPS;
+            q[4] = dir.x, q[5] = dir.y, q[6] = dir.z, q[7] = dist * (1.0f - eps);
+        }
+    }
+}

@@ -20,6 +20,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libref_oracle.so")
+ADAPTER_CHECK = os.path.join(HERE, "_ref", "adapter_check")
 ORC_LIB = os.path.join(HERE, "libdipl_oracle.so")
 # where the reference tree is compiled from (the reference harness is built only where it exists)
 REFERENCE_TREE = os.environ.get("DIPL_REFERENCE_TREE", "/root/reference")
@@ -37,7 +38,7 @@ def build(force=False):
     """Compile the C restatement always, and the reference harness when the reference tree is here."""
     targets = ["libdipl_oracle.so"]
     if os.path.isdir(REFERENCE_TREE):
-        targets.append("ref")
+        targets += ["ref", "adapter"]
     cmd = ["make", "-C", HERE] + (["-B"] if force else []) + targets
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
 
@@ -231,6 +232,8 @@ class Oracle:
         L.orc_hploc.argtypes = [_f32p, C.c_int64, _i32p, _u64p, C.c_void_p, C.c_int, C.c_int, _i32p, _f32p, _i32p]
         L.orc_retrace_binary.argtypes = [_f32p, C.c_int64, _f32p, C.c_int32, _f32p, C.c_int64, C.c_int, _i64p, _i64p,
                                          _u8p, _i32p, _f32p]
+        L.orc_shadow_rays.argtypes = [_f32p, _f32p, _i32p, _f32p, C.c_int64, C.c_int, _i32p, C.c_int, C.c_int, _f32p,
+                                      C.c_int, C.c_uint32, _f32p]
         L.orc_pinhole_rays.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
         L.orc_bounce_rays.argtypes = [_f32p, _f32p, _i32p, _f32p, C.c_int64, C.c_uint32, _f32p]
 
@@ -248,6 +251,20 @@ class Oracle:
         t = np.ascontiguousarray(t, np.float32)
         out = np.empty((len(rays), 8), np.float32)
         self.lib.orc_bounce_rays(tris, rays, prim, t, len(rays), int(seed) & 0xFFFFFFFF, out)
+        return out
+
+    def shadow_rays(self, tris, rays, prim, t, width, area=(), samples=1, points=(), seed=42):
+        """Shadow rays of the frontend's generator, restated (per hit: area lights x samples, then point lights)."""
+        tris, rays = _tris(tris), _rays(rays)
+        prim = np.ascontiguousarray(prim, np.int32)
+        t = np.ascontiguousarray(t, np.float32)
+        area = np.ascontiguousarray(np.asarray(area, np.int32).reshape(-1))
+        points = np.ascontiguousarray(np.asarray(points, np.float32).reshape(-1))
+        per_hit = len(area) * samples + len(points) // 3
+        out = np.empty((len(rays) * per_hit, 8), np.float32)
+        self.lib.orc_shadow_rays(tris, rays, prim, t, len(rays), int(width), area if len(area) else np.zeros(1, np.int32),
+                                 len(area), int(samples), points if len(points) else np.zeros(3, np.float32),
+                                 len(points) // 3, int(seed) & 0xFFFFFFFF, out)
         return out
 
     def set_threads(self, n):

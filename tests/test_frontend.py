@@ -98,3 +98,62 @@ def test_generators_reject_bad_arguments():
     assert lib.dipl_generate_pinhole_rays(None, 4, 4, C.c_void_p(16), None) == 1  # DIPL_ERR_INVALID_ARGUMENT
     assert lib.dipl_generate_bounce_rays(None, None, None, None, None, 4, 0, None, None) == 1  # DIPL_ERR_INVALID_ARGUMENT
     assert lib.dipl_generate_bounce_rays(None, None, None, None, None, 0, 0, None, None) == L.DIPL_OK
+
+
+# ---- the shadow wave (IsShadowed through dipl_bvh_trace_any) ---------------------------------------------------
+def _lit_small_scene():
+    """The small scene with two area lights (triangles of the box's top wall) and two point lights."""
+    tris, _ = S.small_scene(seed=4, width=8, height=8)
+    top = [i for i in range(10) if np.allclose(tris[i, :, 1], tris[i, 0, 1]) and tris[i, 0, 1] > 0.4]
+    assert len(top) >= 2
+    points = np.array([[0.0, 0.45, -0.2], [0.3, 0.2, 0.4]], np.float32)
+    return tris, top[:2], points
+
+
+def test_oracle_shadow_rays_follow_is_shadowed(orc):
+    """Restated shadow rays: unit directions toward the light sample, origins offset by RayEpsilon on the light's
+    side, tmax short of the light by RayEpsilon; null rays for misses and for hits on an area light."""
+    tris, area, points = _lit_small_scene()
+    rays = S.pinhole_rays(48, 48, **S.SMALL_CAMERA)
+    h = orc.brute(tris, rays)
+    sr = orc.shadow_rays(tris, rays, h.prim, h.t, 48, area, 3, points)
+    per_hit = len(area) * 3 + len(points)
+    assert sr.shape == (len(rays) * per_hit, 8)
+    sr = sr.reshape(len(rays), per_hit, 8)
+    miss = h.prim < 0
+    assert (sr[miss, :, 7] == 0).all()
+    for j, tri in enumerate(area):  # a hit on area light j: the reference returns its colour at light j, so
+        on = h.prim == tri          # lights before j were sampled and j and later ones cast nothing
+        assert on.any()
+        assert (sr[on, j * 3: len(area) * 3, 7] == 0).all()
+    cast = sr[:, :, 7] > 0
+    assert cast.sum() > 1000
+    d = sr[cast][:, 4:7].astype(np.float64)
+    np.testing.assert_allclose(np.linalg.norm(d, axis=1), 1.0, atol=1e-6)
+    # point-light rays end just short of the light
+    pl = sr[~miss, len(area) * 3:, :]
+    cast_pl = pl[:, :, 7] > 0
+    end = pl[..., 0:3].astype(np.float64) + pl[..., 4:7] * pl[..., 7:8]
+    for j, p in enumerate(points):
+        gap = np.linalg.norm(end[:, j] - p, axis=1)[cast_pl[:, j]]
+        assert (gap < 2e-3).all()
+
+
+@pytest.mark.gpu
+def test_device_shadow_wave_bit_exact(orc):
+    """Device shadow rays equal the restatement bit for bit, and their occlusion (dipl_bvh_trace_any) equals the
+    oracle's any-hit brute force (IntersectAny semantics: tmin < t < tmax)."""
+    from diplodocus_b200 import accel as A
+    tris, area, points = _lit_small_scene()
+    bvh = A.GpuPlocBvh().Build(A.AccelerationStructureConfig(), A.Stats(), torch.from_numpy(tris))
+    lights = A.Lights(area_light_triangles=tuple(area), samples=3, point_lights=tuple(map(tuple, points)))
+    st = A.Stats()
+    rays, hits, bounce, bhits, shadow, occ = A.trace_frame(bvh, dict(S.SMALL_CAMERA), 64, 64, seed=5, stats=st,
+                                                           lights=lights)
+    want = orc.shadow_rays(tris, rays.cpu().numpy(), hits.prim.cpu().numpy(), hits.t.cpu().numpy(), 64, area, 3,
+                           points)
+    got = shadow.cpu().numpy()
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    np.testing.assert_array_equal(occ.cpu().numpy(), orc.brute_any(tris, want))
+    assert 0 < occ.cpu().numpy().sum() < (want[:, 7] > 0).sum()  # some shadowed, some lit
+    assert st.rt_stats.shadow_ray_count == int((want[:, 7] > 0).sum())
