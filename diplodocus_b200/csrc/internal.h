@@ -147,6 +147,19 @@ dipl_status trace_closest(const dipl_bvh* bvh, const dipl_ray* rays, int64_t n, 
 dipl_status trace_any(const dipl_bvh* bvh, const dipl_ray* rays, int64_t n, uint8_t* occluded, int leaf_test,
                       uint32_t flags, cudaStream_t stream);
 dipl_status sah_cost(const dipl_bvh* bvh, double* cost, cudaStream_t stream);
+// Coherent ray order of large traces (trace.cu): batches of kReorderMinRays rays or more are traced in the order
+// of a key of the origin cell and the direction octant, sorted on the device; records still go to each ray's index.
+constexpr int64_t kReorderMinRays = int64_t(1) << 20;
+inline bool reorder_rays(int64_t n, uint32_t flags) {
+    return n >= kReorderMinRays && (flags & DIPL_TRACE_KEEP_ORDER) == 0u;
+}
+// Device memory of one reordered trace: keys, the order and the sort's scratch (released in stream order).
+struct RayOrder {
+    void* mem = nullptr;
+    uint32_t* order = nullptr;  // the ray index to trace at each position of the work order
+};
+dipl_status make_ray_order(const dipl_ray* rays, int64_t n, uint32_t* d_err, cudaStream_t s, RayOrder& ro);
+
 // Traversal of the SOBB and 8-wide quantised layouts.
 dipl_status trace_closest_ext(const dipl_bvh* bvh, const dipl_ray* rays, int64_t n, dipl_hit* hits, int leaf_test,
                               uint32_t flags, unsigned long long* counters, cudaStream_t stream);

@@ -497,7 +497,6 @@ __global__ void __launch_bounds__(kTraceThreads) tail_kernel(const BNode* __rest
 // above a 9-bit-per-axis Morton code of the origin within the batch's origin bounds. A warp's chunk of rays then
 // starts in one small region and heads the same way, so its lanes fetch the same nodes and branch alike.
 // Records still go to each ray's own index; only the order of work changes, never a result.
-constexpr int64_t kReorderMinRays = int64_t(1) << 20;
 constexpr int kReorderBits = 30;
 
 __global__ void __launch_bounds__(256) ray_bounds_kernel(const dipl_ray* __restrict__ rays, int64_t n,
@@ -554,38 +553,6 @@ __global__ void __launch_bounds__(256) ray_keys_kernel(const dipl_ray* __restric
     keys[i] = (oct << 27) | (spread3_9(cell[0]) << 2) | (spread3_9(cell[1]) << 1) | spread3_9(cell[2]);
 }
 
-// Device memory of one reordered trace: keys, the order and the sort's scratch (released in stream order).
-struct RayOrder {
-    void* mem = nullptr;
-    uint32_t* order = nullptr;
-};
-
-dipl_status make_ray_order(const dipl_ray* rays, int64_t n, uint32_t* d_err, cudaStream_t s, RayOrder& ro) {
-    const size_t sort_bytes = radix_sort_scratch_bytes(n, 0, kReorderBits, 8);
-    const size_t key_bytes = sizeof(uint32_t) * (size_t)n;
-    const size_t bytes = 256 + 5 * key_bytes + sort_bytes;
-    dipl_status st = device_alloc(&ro.mem, bytes, s);
-    if (st != DIPL_OK) return st;
-    unsigned char* base = static_cast<unsigned char*>(ro.mem);
-    int* box = reinterpret_cast<int*>(base);
-    uint32_t* keys = reinterpret_cast<uint32_t*>(base + 256);
-    uint32_t* keys_sorted = keys + n;
-    uint32_t* keys_alt = keys_sorted + n;
-    ro.order = keys_alt + n;
-    uint32_t* order_alt = ro.order + n;
-    unsigned char* scratch = reinterpret_cast<unsigned char*>(order_alt + n);
-    ray_box_init_kernel<<<1, 32, 0, s>>>(box);
-    note_launches();
-    const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-    ray_bounds_kernel<<<grid, 256, 0, s>>>(rays, n, box);
-    note_launches();
-    ray_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rays, n, box, keys);
-    note_launches();
-    DIPL_CUDA(cudaGetLastError());
-    return radix_sort_pairs(keys, nullptr, keys_sorted, ro.order, keys_alt, order_alt, n, 4, 0, kReorderBits, 8,
-                            scratch, s, d_err);
-}
-
 // Blocks of a persistent trace launch: every resident block on every SM (per kernel instantiation and device).
 template <typename K>
 int persistent_grid(K kernel) {
@@ -634,7 +601,7 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
         }
     }
     RayOrder ro;
-    if (n >= kReorderMinRays && (flags & DIPL_TRACE_KEEP_ORDER) == 0u) {
+    if (reorder_rays(n, flags)) {
         dipl_status st = make_ray_order(rays, n, b->d_err, s, ro);
         if (st != DIPL_OK) {
             if (ro.mem) device_free(ro.mem, s);
@@ -673,6 +640,33 @@ dipl_status launch_trace_stack(const dipl_bvh* b, const dipl_ray* rays, int64_t 
 }
 
 }  // namespace
+
+dipl_status make_ray_order(const dipl_ray* rays, int64_t n, uint32_t* d_err, cudaStream_t s, RayOrder& ro) {
+    const size_t sort_bytes = radix_sort_scratch_bytes(n, 0, kReorderBits, 8);
+    const size_t key_bytes = sizeof(uint32_t) * (size_t)n;
+    const size_t bytes = 256 + 5 * key_bytes + sort_bytes;
+    dipl_status st = device_alloc(&ro.mem, bytes, s);
+    if (st != DIPL_OK) return st;
+    unsigned char* base = static_cast<unsigned char*>(ro.mem);
+    int* box = reinterpret_cast<int*>(base);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(base + 256);
+    uint32_t* keys_sorted = keys + n;
+    uint32_t* keys_alt = keys_sorted + n;
+    ro.order = keys_alt + n;
+    uint32_t* order_alt = ro.order + n;
+    unsigned char* scratch = reinterpret_cast<unsigned char*>(order_alt + n);
+    ray_box_init_kernel<<<1, 32, 0, s>>>(box);
+    note_launches();
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    ray_bounds_kernel<<<grid, 256, 0, s>>>(rays, n, box);
+    note_launches();
+    ray_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rays, n, box, keys);
+    note_launches();
+    DIPL_CUDA(cudaGetLastError());
+    return radix_sort_pairs(keys, nullptr, keys_sorted, ro.order, keys_alt, order_alt, n, 4, 0, kReorderBits, 8,
+                            scratch, s, d_err);
+}
+
 
 dipl_status trace_closest(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, int leaf_test,
                           uint32_t flags, unsigned long long* counters, cudaStream_t s) {

@@ -1,11 +1,12 @@
-// Autotuner of the build knobs: PLOC radius, PLOC block size and sort digit width.
+// Autotuner of the build knobs: PLOC radius, PLOC block size (global PLOC only: the hierarchical clustering's block
+// is fixed) and sort digit width.
 //
 // For a batch (its total triangle count gives a size bucket, floor(log2 N)), it times real builds of the
 // caller's meshes and keeps the fastest setting whose SAH cost stays within 2% of the default radius-16
 // tree (the radius trades build time for tree quality; hits are exact with any valid tree, so only time and
 // quality are compared). Coordinate search: digit width, then block size, then radius, each with the others
-// fixed at the best so far. Winners are cached per (code, bounding volume, layout, leaf size, bucket) as one
-// JSON object per line in a file, so a bucket is tuned once.
+// fixed at the best so far. Winners are cached per (code, bounding volume, layout, leaf size, clustering, bucket) as
+// one JSON object per line in a file, so a bucket is tuned once.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -28,8 +29,8 @@ std::string bucket_key(const dipl_build_desc& d, long long total) {
     while ((1ll << (bucket + 1)) <= total) ++bucket;
     std::ostringstream os;
     os << (d.code_type == DIPL_CODE_EMC60 ? "emc60" : "morton30") << "/" << (d.bv_type == DIPL_BV_SOBB ? "sobb" : "aabb")
-       << "/" << (d.layout == DIPL_LAYOUT_WIDE8_Q8 ? "wide8" : "binary") << "/L" << d.max_triangles_per_leaf << "/b"
-       << bucket;
+       << "/" << (d.layout == DIPL_LAYOUT_WIDE8_Q8 ? "wide8" : "binary") << "/L" << d.max_triangles_per_leaf << "/"
+       << (d.clustering == DIPL_CLUSTER_PLOC ? "ploc" : "hploc") << "/b" << bucket;
     return os.str();
 }
 
@@ -123,6 +124,7 @@ dipl_status autotune(const dipl_build_desc* descs, int count, const char* cache_
             if (ms < best.ms) best.digits = digits, best.ms = ms, best.sah = sah;
         }
         for (int block : {128, 512}) {
+            if (descs[0].clustering != DIPL_CLUSTER_PLOC) break;  // the hierarchical clustering has one block size
             apply(best.radius, block, best.digits);
             if ((st = time_builds(v, 2, s, &ms, &sah)) != DIPL_OK) return st;
             if (ms < best.ms) best.block = block, best.ms = ms, best.sah = sah;

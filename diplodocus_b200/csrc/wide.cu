@@ -295,10 +295,12 @@ template <int LEAF, bool ANY, bool COUNT, int STACK>
 __global__ void __launch_bounds__(kWTraceThreads) wide_trace_kernel(
     const WNode* __restrict__ nodes, const float4* __restrict__ tris, int root, int num_nodes,
     const dipl_ray* __restrict__ rays, int64_t n, dipl_hit* __restrict__ hits, uint8_t* __restrict__ occluded,
-    uint32_t flags, unsigned long long* __restrict__ counters, uint32_t* __restrict__ err, uint32_t step_limit) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    uint32_t flags, unsigned long long* __restrict__ counters, uint32_t* __restrict__ err, uint32_t step_limit,
+    const uint32_t* __restrict__ order) {
+    const int64_t work = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // position in the work order
     unsigned visits = 0, tests = 0;
-    if (i < n) {
+    if (work < n) {
+        const int64_t i = order ? (int64_t)__ldg(order + work) : work;  // the ray's own index
         const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * i;
         const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
         WRay r;
@@ -449,13 +451,24 @@ template <int LEAF, bool ANY, bool COUNT, int STACK>
 dipl_status launch_wide(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, uint32_t flags,
                         unsigned long long* counters, cudaStream_t s) {
     const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
+    RayOrder ro;
+    if (reorder_rays(n, flags)) {
+        const dipl_status st = make_ray_order(rays, n, b->d_err, s, ro);
+        if (st != DIPL_OK) {
+            if (ro.mem) device_free(ro.mem, s);
+            return st;
+        }
+    }
     wide_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kWTraceThreads - 1) / kWTraceThreads), kWTraceThreads,
                                                   0, s>>>(static_cast<const WNode*>(b->nodes), b->tris, b->root,
                                                           num_nodes, rays, n, hits, occ, flags, counters, b->d_err,
                                                           trace_step_limit() ? trace_step_limit()
-                                                                             : 2u * (uint32_t)std::max(num_nodes, 0) + 64u);
+                                                                             : 2u * (uint32_t)std::max(num_nodes, 0) + 64u,
+                                                          ro.order);
     note_launches();
-    DIPL_CUDA(cudaGetLastError());
+    const cudaError_t e = cudaGetLastError();
+    if (ro.mem) device_free(ro.mem, s);
+    DIPL_CUDA(e);
     return DIPL_OK;
 }
 

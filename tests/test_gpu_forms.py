@@ -196,4 +196,36 @@ def test_autotuner_picks_valid_knobs_and_caches(tmp_path):
     assert d.sort_digit_bits in (6, 8, 10)
     tuned2, from_cache2, _ = A.autotune(cfg, meshes, cache)
     assert from_cache2 and tuned2[0].nn_search_radius == d.nn_search_radius
-    assert '"key": "morton30/aabb/binary/L4/b' in open(cache).read()
+    assert '"key": "morton30/aabb/binary/L4/hploc/b' in open(cache).read()
+
+
+@pytest.mark.parametrize("clustering", ["hploc", "ploc"])
+def test_autotuned_build_keeps_the_sah_rule_and_is_not_slower(tmp_path, clustering):
+    """The tuned knobs build a tree whose SAH cost is within 2% of the radius-16 default's (the tuner's rule) and
+    the tuned build is not slower than the default beyond timing noise."""
+    import time
+    meshes = [torch.from_numpy(S.uv_sphere(nu, nu // 2, 1.0, (0, 0, 0), displacement=0.05, seed=nu))
+              for nu in (64, 200, 512)]
+    cfg = A.AccelerationStructureConfig(clustering=clustering)
+    tuned, _, _ = A.autotune(cfg, meshes, str(tmp_path / "tune.jsonl"))
+    default = A.AccelerationStructureConfig(clustering=clustering)
+
+    def run(desc_fix):
+        best, costs = 1e30, None
+        for _ in range(5):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            bvhs = A.build_batched(desc_fix, meshes)
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+            costs = [b.sah_cost() for b in bvhs]
+        return best, costs
+
+    t_def, c_def = run(default)
+    d0 = tuned[0]
+    tcfg = A.AccelerationStructureConfig(clustering=clustering, nn_search_radius=d0.nn_search_radius,
+                                         ploc_block_size=d0.ploc_block_size, sort_digit_bits=d0.sort_digit_bits)
+    t_tun, c_tun = run(tcfg)
+    w = np.array([len(m) for m in meshes], np.float64)
+    assert np.dot(c_tun, w) / w.sum() <= 1.02 * np.dot(c_def, w) / w.sum()
+    assert t_tun <= 1.25 * t_def, (t_tun, t_def)

@@ -323,15 +323,17 @@ def test_nan_and_inf_vertices(orc, kind, layout):
     bvh.check_errors()
 
 
+@pytest.mark.parametrize("form", ["binary", "sobb", "wide8_q8"])
 @pytest.mark.parametrize("workload", ["sphere", "soup"])
-def test_reordered_trace_equals_given_order(workload):
+def test_reordered_trace_equals_given_order(workload, form):
     """Batches of 2^20 rays or more are traced in a coherent order of their own; the records are bit-identical to
-    tracing in the given order (and, with counters, so are the visit and test totals)."""
+    tracing in the given order (and, with counters, so are the visit and test totals), in every layout."""
     if workload == "sphere":
         tris, rays = S.displaced_sphere(nu=256, nv=128, n_rays=1 << 20)
     else:
         tris, rays = S.soup(200_000, seed=5), S.random_rays((1 << 20) + 77, seed=5)
-    bvh = build(tris, A.AccelerationStructureType.kPlocEmc)
+    kind = A.AccelerationStructureType.kPlocEmcSobb if form == "sobb" else A.AccelerationStructureType.kPlocEmc
+    bvh = build(tris, kind, layout="wide8_q8" if form == "wide8_q8" else "binary")
     rd = torch.from_numpy(rays).cuda()
     st_a, st_b = A.Stats(), A.Stats()
     a = bvh.Intersect(st_a, rd, count=True)
