@@ -1314,6 +1314,7 @@ __global__ void __launch_bounds__(kHplocThreads) hploc_kernel(HplocParams P) {
             }
         }
         unsigned pending = __ballot_sync(full, todo);
+        const bool stored = pending != 0u;
         while (pending) {
             const int src = __ffs(pending) - 1;
             pending &= pending - 1u;
@@ -1322,6 +1323,7 @@ __global__ void __launch_bounds__(kHplocThreads) hploc_kernel(HplocParams P) {
             const bool whole = __shfl_sync(full, (int)(l == mstart && r == mend), src) != 0;
             iters += hploc_node(P, nl, nr, nm, nbase, whole);
         }
+        if (stored) __threadfence();  // every lane's part of the lists and nodes, before any lane's next arrival
         __syncwarp();
         if (!__any_sync(full, active)) break;
     }

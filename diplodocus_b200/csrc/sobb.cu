@@ -271,10 +271,9 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
                                                                unsigned long long* __restrict__ counters,
                                                                uint32_t* __restrict__ err, uint32_t step_limit,
                                                                const uint32_t* __restrict__ order) {
-    __shared__ float s_o[kDirs][kSThreads];
-    __shared__ float s_inv[kDirs][kSThreads];
-    __shared__ float s_tol[kDirs][kSThreads];
-    __shared__ float s_rel[kDirs][kSThreads];
+    // per table direction: the ray's projected origin, reciprocal projected direction, and the two widening terms,
+    // one 16-byte record per (direction, thread) so a slab costs one shared load
+    __shared__ float4 s_ray[kDirs][kSThreads];
     const int64_t work = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // position in the work order
     unsigned visits = 0, tests = 0;
     if (work < n) {
@@ -289,12 +288,10 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
         for (int k = 0; k < dirs; ++k) {
             const float dk = proj(k, d.x, d.y, d.z);
             const float inv = __frcp_rn(fabsf(dk) < 1e-20f ? copysignf(1e-20f, dk) : dk);
-            s_o[k][tid] = proj(k, o.x, o.y, o.z);
-            s_inv[k][tid] = inv;
             // rounding of the projected origin as a distance along the ray (absolute), and of the projected
             // direction as a relative error of every distance on this slab (large for grazing slabs)
-            s_tol[k][tid] = omag * 4.0e-7f * fabsf(inv);
-            s_rel[k][tid] = kSSlabWiden + dmag * 4.0e-7f * fabsf(inv);
+            s_ray[k][tid] = make_float4(proj(k, o.x, o.y, o.z), inv, omag * 4.0e-7f * fabsf(inv),
+                                        kSSlabWiden + dmag * 4.0e-7f * fabsf(inv));
         }
         const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
         WtRay w{};
@@ -313,7 +310,8 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 const int k = (axes >> (8 * j)) & 0xFF;
-                const float ok = s_o[k][tid], inv = s_inv[k][tid], tol = s_tol[k][tid], rel = s_rel[k][tid];
+                const float4 q = s_ray[k][tid];
+                const float ok = q.x, inv = q.y, tol = q.z, rel = q.w;
                 const float t0 = __fmul_rn(__fsub_rn(ls[j], ok), inv), t1 = __fmul_rn(__fsub_rn(hs[j], ok), inv);
                 const float a0 = fminf(t0, t1), a1 = fmaxf(t0, t1);
                 tn = fmaxf(tn, a0 - fabsf(a0) * rel - tol);
