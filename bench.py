@@ -143,6 +143,9 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------------------
 SOUP_TRIANGLES = 16 * 1024 * 1024
 DEFAULT_CODE = {"soup16m": "emc60", "displaced_sphere": "morton30"}
+# Pre-splitting of large triangles (percent more clustering leaves at most): the soup's log-normal tail of large
+# triangles overlaps everywhere; the sphere's triangles are all alike (nothing would split).
+DEFAULT_SPLIT = {"soup16m": 40, "displaced_sphere": 0}
 
 
 def workload(name, rays_override=None, soup_tris=SOUP_TRIANGLES):
@@ -308,14 +311,14 @@ def max_over_ranks(values, world, device=None):
     return t.tolist()
 
 
-def build_bytes_per_tri(code_type, digit_bits=8, node_bytes_per_tri=None):
+def build_bytes_per_tri(code_type, digit_bits=8, node_bytes_per_tri=None, leaves_per_tri=1.0):
     """Algorithmic bytes of one build per triangle (byte model, Morton30: 176 B, EMC60: 308 B with 64 B/tri of
     nodes): vertices once, code + index written, the sort's passes at 8-bit digits, the node array, the
-    permutation."""
+    permutation; with pre-splitting the per-leaf terms count once per clustering leaf."""
     k = 4 if code_type == 0 else 8
     passes = -(-(30 if code_type == 0 else 60) // 8)
     node = 64.0 if node_bytes_per_tri is None else node_bytes_per_tri
-    return 36 + (k + 4) + passes * 2 * (k + 4) + node + 4
+    return 36 + leaves_per_tri * ((k + 4) + passes * 2 * (k + 4) + 4) + node
 
 
 def trace_bytes_per_ray(visits, tests, node_bytes):
@@ -337,9 +340,10 @@ def _quantiles(x, qs):
 KIND_OF = {("morton30", "aabb"): "kPloc", ("emc60", "aabb"): "kPlocEmc", ("morton30", "sobb"): "kPlocSobb",
            ("emc60", "sobb"): "kPlocEmcSobb"}
 # The soup's variants beside the main arm (EMC60, AABB, binary): (code, bounding volume, layout).
-SOUP_VARIANTS = {"ploc_morton30": ("morton30", "aabb", "binary"),
-                 "ploc_emc_sobb": ("emc60", "sobb", "binary"),
-                 "ploc_emc_wide8_q8": ("emc60", "aabb", "wide8_q8")}
+SOUP_VARIANTS = {"ploc_emc_no_split": ("emc60", "aabb", "binary", 0),
+                 "ploc_morton30": ("morton30", "aabb", "binary", None),
+                 "ploc_emc_sobb": ("emc60", "sobb", "binary", None),
+                 "ploc_emc_wide8_q8": ("emc60", "aabb", "wide8_q8", None)}
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -359,9 +363,12 @@ def run_gpu(args, rank, world, local_rank):
     n, nr = len(tris), len(rays_np)
     AT = A.AccelerationStructureType
 
-    def config(code_, bv="aabb", layout="binary"):
+    split = args.split_budget if args.split_budget is not None else DEFAULT_SPLIT.get(args.workload, 0)
+
+    def config(code_, bv="aabb", layout="binary", split_budget=None):
         return A.AccelerationStructureConfig(getattr(AT, KIND_OF[(code_, bv)]), nn_search_radius=args.radius,
-                                             leaf_test=args.leaf_test, layout=layout)
+                                             leaf_test=args.leaf_test, layout=layout,
+                                             split_budget=split if split_budget is None else split_budget)
 
     cfg = config(code)
     v = A.soa_vertices(tris, dev)
@@ -456,7 +463,7 @@ def run_gpu(args, rank, world, local_rank):
     steps = args.steps
     build_s = t_build / 1e3 / steps
     trace_s = t_trace / 1e3 / steps
-    bpt = build_bytes_per_tri(desc.code_type, 8, info.node_bytes / max(n, 1))
+    bpt = build_bytes_per_tri(desc.code_type, 8, info.node_bytes / max(n, 1), info.num_leaves / max(n, 1))
     achieved_build = bpt * n / build_s / 1e9
     ray_bytes = trace_bytes_per_ray(visits / nr, tests / nr, node_bytes)
     achieved_trace = ray_bytes * nr / trace_s / 1e9
@@ -477,7 +484,8 @@ def run_gpu(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": round(t_step / steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": desc_txt, "triangles": n, "rays": nr,
-                   "code": code, "bounding_volume": "aabb", "nn_search_radius": args.radius,
+                   "code": code, "bounding_volume": "aabb", "split_budget": split,
+                   "clustering_leaves": int(info.num_leaves), "nn_search_radius": args.radius,
                    "leaf_test": args.leaf_test, "layout": "binary", "max_triangles_per_leaf": 4,
                    "l2": "inputs larger than L2, and L2 flushed between steps (256 MB write)",
                    "parallelism": f"replicas x{world}"},
@@ -653,8 +661,8 @@ def soup_forms(args, lib, L, A, torch, C, v, rays, hits, h_main, cfg, config, bu
     out["disagreements"][f"{args.leaf_test}_vs_{other}"] = disagreement(hits, h_wt)
     del h_wt
     vh = torch.empty_like(hits)
-    for name, (code_, bv, layout) in SOUP_VARIANTS.items():
-        c = config(code_, bv, layout)
+    for name, (code_, bv, layout, split_) in SOUP_VARIANTS.items():
+        c = config(code_, bv, layout, split_)
         d = A.make_desc(*v, c)
         b_ms = timed(lambda: build(d), args.variant_builds)
         hv = build(d)
@@ -673,7 +681,7 @@ def soup_forms(args, lib, L, A, torch, C, v, rays, hits, h_main, cfg, config, bu
         same = float((vh[:, 0] == main_prim).float().mean().item())
         bm = float(np.median(b_ms))
         out["variants"][name] = {
-            "code": code_, "bounding_volume": bv, "layout": layout,
+            "code": code_, "bounding_volume": bv, "layout": layout, "split_budget": c.split_budget,
             "build_ms": round(bm, 3), "build_ms_all": [round(x, 3) for x in b_ms],
             "build_mtri_s": round(n / bm / 1e3, 1), "trace_ms": round(tm, 3),
             "trace_mrays_s": round(nr / tm / 1e3, 2), "sah_cost": round(sah.value, 4),
@@ -1011,6 +1019,8 @@ def main():
     ap.add_argument("--code", default=None, choices=["morton30", "emc60"],
                     help="code of the main arm (default: emc60 on the soup, morton30 on the sphere)")
     ap.add_argument("--radius", type=int, default=16)
+    ap.add_argument("--split-budget", type=int, default=None,
+                    help="pre-splitting of large triangles, percent (default: 40 on the soup, 0 on the sphere)")
     ap.add_argument("--leaf-test", default="ref_mt", choices=["ref_mt", "watertight"])
     ap.add_argument("--rays", type=int, default=None)
     ap.add_argument("--ref-sample-rays", type=int, default=1 << 12)

@@ -46,7 +46,7 @@ class BuildDesc(C.Structure):
                 ("code_type", C.c_int32), ("bv_type", C.c_int32), ("layout", C.c_int32),
                 ("max_triangles_per_leaf", C.c_int32), ("nn_search_radius", C.c_int32), ("kdop_size", C.c_int32),
                 ("ploc_block_size", C.c_int32), ("sort_digit_bits", C.c_int32), ("clustering", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("split_budget", C.c_int32)]
 
 
 class BvhInfo(C.Structure):

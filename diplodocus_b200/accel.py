@@ -68,6 +68,7 @@ class AccelerationStructureConfig:
     ploc_block_size: int = 0
     sort_digit_bits: int = 0
     clustering: str = "hploc"           # "hploc" (hierarchical, default) | "ploc" (global iterations)
+    split_budget: int = 0               # pre-splitting of large triangles: at most this % more leaves (0 = none)
 
 
 @dataclass
@@ -163,6 +164,7 @@ def make_desc(v0, v1, v2, config: AccelerationStructureConfig) -> L.BuildDesc:
     d.ploc_block_size = config.ploc_block_size
     d.sort_digit_bits = config.sort_digit_bits
     d.clustering = {"hploc": L.CLUSTER_HPLOC, "ploc": L.CLUSTER_PLOC}[config.clustering]
+    d.split_budget = config.split_budget
     return d
 
 
@@ -255,8 +257,9 @@ class GpuPlocBvh:
         return c.value
 
     def download_topology(self):
-        """(perm (N,), children (N-1, 2), boxes (N-1, 6)) of the clustering, as numpy arrays."""
-        n = self.num_triangles
+        """(perm (n,), children (n-1, 2), boxes (n-1, 6)) of the clustering, as numpy arrays; n = the clustering's
+        leaves (the triangles, and their pieces with pre-splitting)."""
+        n = int(self.info().num_leaves)
         perm = np.empty(max(n, 1), np.int32)
         ch = np.empty(max(2 * (n - 1), 1), np.int32)
         bx = np.empty(max(6 * (n - 1), 1), np.float32)
@@ -269,11 +272,12 @@ class GpuPlocBvh:
         """(nodes bytes as uint8 array, triangles (N, 3, 4) float32, root reference)."""
         info = self.info()
         nodes = np.empty(max(int(info.node_bytes), 1), np.uint8)
-        tris = np.empty((max(self.num_triangles, 1), 3, 4), np.float32)
+        nl = int(info.num_leaves)
+        tris = np.empty((max(nl, 1), 3, 4), np.float32)
         root = C.c_int32(0)
         L.check(self._lib.dipl_bvh_download_layout(self._h, nodes.ctypes.data, tris.ctypes.data, C.byref(root),
                                                    _stream()), "dipl_bvh_download_layout")
-        return nodes[: int(info.node_bytes)], tris[: self.num_triangles], root.value
+        return nodes[: int(info.node_bytes)], tris[:nl], root.value
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

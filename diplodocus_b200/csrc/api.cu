@@ -189,7 +189,7 @@ void dipl_build_desc_init(dipl_build_desc* d) {
     d->ploc_block_size = 0;
     d->sort_digit_bits = 0;
     d->clustering = DIPL_CLUSTER_HPLOC;
-    d->reserved = 0;
+    d->split_budget = 0;
 }
 
 dipl_status dipl_bvh_build(const dipl_build_desc* desc, dipl_bvh** out, void* stream) {
@@ -258,9 +258,9 @@ dipl_status dipl_bvh_get_info(const dipl_bvh* b, dipl_bvh_info* info) {
     std::memset(info, 0, sizeof(*info));
     info->num_triangles = b->num_triangles;
     info->num_inner_nodes = b->num_nodes;
-    info->num_leaves = b->num_leaves;
+    info->num_leaves = b->num_refs;
     info->node_bytes = b->num_nodes * b->node_size;
-    info->triangle_bytes = b->num_triangles * 48;
+    info->triangle_bytes = b->num_refs * 48;
     info->depth = b->depth;
     info->ploc_iterations = b->ploc_iterations;
     info->code_type = b->code_type;
@@ -279,13 +279,20 @@ dipl_status dipl_bvh_download_topology(const dipl_bvh* b, int32_t* h_perm, int32
         set_last_error("dipl_bvh_download_topology: bvh must be non-NULL");
         return DIPL_ERR_INVALID_ARGUMENT;
     }
-    if (b->batch_leaves != b->num_triangles) {
+    if (b->batched) {
         set_last_error("dipl_bvh_download_topology: handles of a batched build share one topology");
         return DIPL_ERR_UNSUPPORTED;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int64_t n = b->num_triangles, k = n > 0 ? n - 1 : 0;
-    if (h_perm && n > 0) DIPL_CUDA(cudaMemcpyAsync(h_perm, b->perm, 4 * n, cudaMemcpyDeviceToHost, s));
+    const int64_t n = b->num_refs, k = n > 0 ? n - 1 : 0;
+    std::vector<int32_t> ref_tri;
+    if (h_perm && n > 0) {
+        DIPL_CUDA(cudaMemcpyAsync(h_perm, b->perm, 4 * n, cudaMemcpyDeviceToHost, s));
+        if (b->ref_tri) {  // positions hold references: report their triangles
+            ref_tri.resize(n);
+            DIPL_CUDA(cudaMemcpyAsync(ref_tri.data(), b->ref_tri, 4 * n, cudaMemcpyDeviceToHost, s));
+        }
+    }
     std::vector<int4> ch(k);
     std::vector<float4> lo(k), hi(k);
     if (k > 0) {
@@ -294,6 +301,8 @@ dipl_status dipl_bvh_download_topology(const dipl_bvh* b, int32_t* h_perm, int32
         DIPL_CUDA(cudaMemcpyAsync(hi.data(), b->node_hi, sizeof(float4) * k, cudaMemcpyDeviceToHost, s));
     }
     DIPL_CUDA(cudaStreamSynchronize(s));
+    if (!ref_tri.empty())
+        for (int64_t i = 0; i < n; ++i) h_perm[i] = ref_tri[h_perm[i]];
     for (int64_t i = 0; i < k; ++i) {
         if (h_children) {
             h_children[2 * i] = ch[i].x;
@@ -314,15 +323,15 @@ dipl_status dipl_bvh_download_layout(const dipl_bvh* b, void* h_nodes, void* h_t
         set_last_error("dipl_bvh_download_layout: bvh must be non-NULL");
         return DIPL_ERR_INVALID_ARGUMENT;
     }
-    if (b->batch_leaves != b->num_triangles) {
+    if (b->batched) {
         set_last_error("dipl_bvh_download_layout: handles of a batched build share one layout");
         return DIPL_ERR_UNSUPPORTED;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (h_nodes && b->num_nodes > 0)
         DIPL_CUDA(cudaMemcpyAsync(h_nodes, b->nodes, b->num_nodes * b->node_size, cudaMemcpyDeviceToHost, s));
-    if (h_triangles && b->num_triangles > 0)
-        DIPL_CUDA(cudaMemcpyAsync(h_triangles, b->tris, b->num_triangles * 48, cudaMemcpyDeviceToHost, s));
+    if (h_triangles && b->num_refs > 0)
+        DIPL_CUDA(cudaMemcpyAsync(h_triangles, b->tris, b->num_refs * 48, cudaMemcpyDeviceToHost, s));
     DIPL_CUDA(cudaStreamSynchronize(s));
     if (h_root) *h_root = b->root;
     return DIPL_OK;

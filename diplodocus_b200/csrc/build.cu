@@ -289,8 +289,9 @@ __global__ void __launch_bounds__(256) emc_tables_kernel(CodeParams* params) {
     }
 }
 
-__device__ __forceinline__ unsigned long long tri_code(const Tri& t, const CodeParams& p, int code_type) {
-    float3 c = centroid(t);
+// The code of a point c with a size given by box extents (dx, dy, dz): Morton30 uses c, EMC60 also the box diagonal.
+__device__ __forceinline__ unsigned long long point_code(float3 c, float dx, float dy, float dz, const CodeParams& p,
+                                                         int code_type) {
     if (code_type == DIPL_CODE_MORTON30) {
         float xs[3] = {c.x, c.y, c.z};
         uint32_t q[3];
@@ -302,9 +303,6 @@ __device__ __forceinline__ unsigned long long tri_code(const Tri& t, const CodeP
         }
         return (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
     }
-    float dx = __fsub_rn(fmaxf(fmaxf(t.a.x, t.b.x), t.c.x), fminf(fminf(t.a.x, t.b.x), t.c.x));
-    float dy = __fsub_rn(fmaxf(fmaxf(t.a.y, t.b.y), t.c.y), fminf(fminf(t.a.y, t.b.y), t.c.y));
-    float dz = __fsub_rn(fmaxf(fmaxf(t.a.z, t.b.z), t.c.z), fminf(fminf(t.a.z, t.b.z), t.c.z));
     float xs[4] = {c.x, c.y, c.z,
                    __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)))};
     unsigned long long code = 0;
@@ -318,6 +316,14 @@ __device__ __forceinline__ unsigned long long tri_code(const Tri& t, const CodeP
         for (int c = 0; c < chunks; ++c) code |= p.dep[a][c][(qi >> (4 * c)) & 15ull];
     }
     return code;
+}
+
+// A triangle's code: its centroid (the reference's, triangle.h:36) and, for EMC60, its box diagonal.
+__device__ __forceinline__ unsigned long long tri_code(const Tri& t, const CodeParams& p, int code_type) {
+    const float dx = __fsub_rn(fmaxf(fmaxf(t.a.x, t.b.x), t.c.x), fminf(fminf(t.a.x, t.b.x), t.c.x));
+    const float dy = __fsub_rn(fmaxf(fmaxf(t.a.y, t.b.y), t.c.y), fminf(fminf(t.a.y, t.b.y), t.c.y));
+    const float dz = __fsub_rn(fmaxf(fmaxf(t.a.z, t.b.z), t.c.z), fminf(fminf(t.a.z, t.b.z), t.c.z));
+    return point_code(centroid(t), dx, dy, dz, p, code_type);
 }
 
 template <typename K>
@@ -340,6 +346,215 @@ __global__ void __launch_bounds__(256) codes_kernel(const MeshDesc* __restrict__
         tbox[2 * g] = make_float4(lo.x, lo.y, lo.z, 0.0f);
         tbox[2 * g + 1] = make_float4(hi.x, hi.y, hi.z, 0.0f);
     }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Pre-splitting of large triangles (early split clipping, after Ernst & Greiner 2007 and the pre-splitting of
+// Karras & Aila 2013): a triangle whose box is large compared with its mesh's other triangles enters the
+// clustering as several references, each with the box of the part of the triangle inside one half of its box
+// (recursively halved at the longest axis' midpoint). Leaves still hold the whole triangle, so a ray tests the
+// same triangles with the same arithmetic and gets the same closest hit; it only meets far fewer boxes that
+// are mostly empty (a log-normal soup's large triangles cover every point of the cube many times over).
+//
+// Split counts are deterministic: w = (dx dy + dy dz) + dz dx of the triangle's box in FP32, quantised to an
+// integer q = floor(w 2^32 / D^2) (D = the mesh's vertex-box diagonal) so the per-mesh sum Q is exact; the
+// triangle gets s = floor(q budget N / (100 Q)) splits (FP64, one rounding per operation), at most
+// kMaxPieces - 1, and s + 1 references. Every reference of a split triangle codes by its box centre and box
+// diagonal; an unsplit triangle codes exactly as without splitting. oracle/dipl_oracle.c orc_presplit restates
+// this bit for bit.
+// ------------------------------------------------------------------------------------------------
+constexpr int kMaxPieces = 64;
+
+__device__ __forceinline__ unsigned long long split_weight(const Tri& t, float diag) {
+    if (!tri_finite(t) || !(diag > 0.0f)) return 0ull;
+    float3 lo, hi;
+    tri_box(t, lo, hi);
+    const float dx = __fsub_rn(hi.x, lo.x), dy = __fsub_rn(hi.y, lo.y), dz = __fsub_rn(hi.z, lo.z);
+    const float w = __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
+    const double scale = __ddiv_rn(4294967296.0, __dmul_rn((double)diag, (double)diag));
+    const double q = __dmul_rn((double)w, scale);
+    return q < 1.8e19 ? (unsigned long long)q : 18000000000000000000ull;
+}
+
+__device__ __forceinline__ float mesh_diag(const Bounds& b) {
+    float e[3];
+    for (int a = 0; a < 3; ++a) e[a] = __fsub_rn(ordered_to_float(b.v[9 + a]), ordered_to_float(b.v[6 + a]));
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(e[0], e[0]), __fmul_rn(e[1], e[1])), __fmul_rn(e[2], e[2])));
+}
+
+__global__ void __launch_bounds__(256) split_weight_kernel(const MeshDesc* __restrict__ meshes,
+                                                           const long long* __restrict__ offsets, int m, long long n,
+                                                           const Bounds* __restrict__ bounds,
+                                                           unsigned long long* __restrict__ mesh_sum) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    unsigned long long q = 0ull;
+    int k = 0;
+    if (g < n) {
+        k = find_mesh(offsets, m, g);
+        q = split_weight(load_tri(meshes[k], g - meshes[k].first), mesh_diag(bounds[k]));
+    }
+    // integer sums are exact in any order: one atomic per warp when the warp lies in one mesh, else one per thread
+    const int k0 = __shfl_sync(0xffffffffu, k, 0);
+    if (__all_sync(0xffffffffu, k == k0)) {
+        for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+        if ((threadIdx.x & 31) == 0 && q) atomicAdd(mesh_sum + k0, q);
+    } else if (q) {
+        atomicAdd(mesh_sum + k, q);
+    }
+}
+
+__device__ __forceinline__ uint32_t split_pieces(unsigned long long q, unsigned long long sum, long long mesh_tris,
+                                                 int budget) {
+    if (sum == 0ull || q == 0ull) return 1u;
+    const double num = __dmul_rn(__dmul_rn((double)q, (double)budget), (double)mesh_tris);
+    const double den = __dmul_rn(100.0, (double)sum);
+    const double s = floor(__ddiv_rn(num, den));
+    return 1u + (uint32_t)fmin(s, (double)(kMaxPieces - 1));
+}
+
+__global__ void __launch_bounds__(256) split_count_kernel(const MeshDesc* __restrict__ meshes,
+                                                          const long long* __restrict__ offsets, int m, long long n,
+                                                          const Bounds* __restrict__ bounds,
+                                                          const unsigned long long* __restrict__ mesh_sum, int budget,
+                                                          uint32_t* __restrict__ pieces) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const int k = find_mesh(offsets, m, g);
+    const unsigned long long q = split_weight(load_tri(meshes[k], g - meshes[k].first), mesh_diag(bounds[k]));
+    pieces[g] = split_pieces(q, mesh_sum[k], meshes[k].count, budget);
+}
+
+// First reference of every mesh (cluster positions of the meshes) from the exclusive scan of the piece counts.
+__global__ void mesh_ref_offsets_kernel(const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ first,
+                                        const uint32_t* __restrict__ total, long long* __restrict__ coffsets) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) coffsets[k] = first[offsets[k]];
+    if (k == m) coffsets[m] = *total;
+}
+
+// Box of the part of triangle t inside [lo, hi]: the triangle clipped against the six planes (Sutherland-Hodgman;
+// points on a plane are inside; a crossing point takes the plane's coordinate exactly), then clamped to the box.
+// An empty result (only rounding can make one) gives the box itself, which is conservative.
+__device__ void clipped_box(const Tri& t, const float* lo, const float* hi, float* olo, float* ohi) {
+    float P[9][3], Q[9][3];
+    int np = 3;
+    const float3 v[3] = {t.a, t.b, t.c};
+    for (int i = 0; i < 3; ++i) P[i][0] = v[i].x, P[i][1] = v[i].y, P[i][2] = v[i].z;
+    for (int plane = 0; plane < 6 && np > 0; ++plane) {
+        const int a = plane >> 1;
+        const bool low = (plane & 1) == 0;
+        const float b = low ? lo[a] : hi[a];
+        int nq = 0;
+        for (int i = 0; i < np; ++i) {
+            const float* p = P[i];
+            const float* q = P[i + 1 < np ? i + 1 : 0];
+            const bool ip = low ? p[a] >= b : p[a] <= b, iq = low ? q[a] >= b : q[a] <= b;
+            if (ip && nq < 9) Q[nq][0] = p[0], Q[nq][1] = p[1], Q[nq][2] = p[2], ++nq;
+            if (ip != iq && nq < 9) {
+                const float s = __fdiv_rn(__fsub_rn(b, p[a]), __fsub_rn(q[a], p[a]));
+                for (int c = 0; c < 3; ++c) Q[nq][c] = c == a ? b : __fadd_rn(p[c], __fmul_rn(s, __fsub_rn(q[c], p[c])));
+                ++nq;
+            }
+        }
+        np = nq;
+        for (int i = 0; i < np; ++i) P[i][0] = Q[i][0], P[i][1] = Q[i][1], P[i][2] = Q[i][2];
+    }
+    if (np == 0) {
+        for (int c = 0; c < 3; ++c) olo[c] = lo[c], ohi[c] = hi[c];
+        return;
+    }
+    for (int c = 0; c < 3; ++c) {
+        float mn = P[0][c], mx = P[0][c];
+        for (int i = 1; i < np; ++i) mn = fminf(mn, P[i][c]), mx = fmaxf(mx, P[i][c]);
+        olo[c] = fmaxf(mn, lo[c]);
+        ohi[c] = fminf(mx, hi[c]);
+    }
+}
+
+// The references of every triangle at its scanned position: an unsplit triangle's box, or its pieces in depth-first
+// order (the lower half first; a box of c pieces gives ceil(c/2) to the lower half and floor(c/2) to the upper).
+__global__ void __launch_bounds__(128) split_kernel(const MeshDesc* __restrict__ meshes,
+                                                    const long long* __restrict__ offsets, int m, long long n,
+                                                    const uint32_t* __restrict__ pieces,
+                                                    const uint32_t* __restrict__ first, int* __restrict__ ref_tri,
+                                                    float4* __restrict__ rbox) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const int k = find_mesh(offsets, m, g);
+    const Tri t = load_tri(meshes[k], g - meshes[k].first);
+    const uint32_t c = pieces[g];
+    long long r = first[g];
+    float3 blo, bhi;
+    tri_box(t, blo, bhi);
+    if (c == 1u) {
+        ref_tri[r] = (int)g;
+        rbox[2 * r] = make_float4(blo.x, blo.y, blo.z, 0.0f);
+        rbox[2 * r + 1] = make_float4(bhi.x, bhi.y, bhi.z, 0.0f);
+        return;
+    }
+    struct Item {
+        float lo[3], hi[3];
+        int c;
+    };
+    Item st[8];  // depth <= log2(kMaxPieces) + 1
+    int sp = 0;
+    st[sp++] = Item{{blo.x, blo.y, blo.z}, {bhi.x, bhi.y, bhi.z}, (int)c};
+    while (sp > 0) {
+        const Item it = st[--sp];
+        if (it.c == 1) {
+            ref_tri[r] = (int)g;
+            rbox[2 * r] = make_float4(it.lo[0], it.lo[1], it.lo[2], 0.0f);
+            rbox[2 * r + 1] = make_float4(it.hi[0], it.hi[1], it.hi[2], 0.0f);
+            ++r;
+            continue;
+        }
+        const float e0 = __fsub_rn(it.hi[0], it.lo[0]), e1 = __fsub_rn(it.hi[1], it.lo[1]),
+                    e2 = __fsub_rn(it.hi[2], it.lo[2]);
+        const int a = (e0 >= e1 && e0 >= e2) ? 0 : (e1 >= e2 ? 1 : 2);
+        const float mid = __fadd_rn(it.lo[a], __fmul_rn(__fsub_rn(it.hi[a], it.lo[a]), 0.5f));
+        Item lower = it, upper = it;
+        lower.hi[a] = mid;
+        upper.lo[a] = mid;
+        float l[3], h[3];
+        clipped_box(t, lower.lo, lower.hi, l, h);
+        for (int q = 0; q < 3; ++q) lower.lo[q] = l[q], lower.hi[q] = h[q];
+        clipped_box(t, upper.lo, upper.hi, l, h);
+        for (int q = 0; q < 3; ++q) upper.lo[q] = l[q], upper.hi[q] = h[q];
+        lower.c = (it.c + 1) / 2;
+        upper.c = it.c / 2;
+        if (sp + 2 > 8) break;  // cannot happen for kMaxPieces = 64 (depth 7)
+        st[sp++] = upper;
+        st[sp++] = lower;
+    }
+}
+
+// Codes of the references: an unsplit triangle's exactly as codes_kernel computes it, a piece's from the centre
+// and the diagonal of its box.
+template <typename K>
+__global__ void __launch_bounds__(256) ref_codes_kernel(const MeshDesc* __restrict__ meshes,
+                                                        const long long* __restrict__ offsets, int m, long long n_refs,
+                                                        const int* __restrict__ ref_tri,
+                                                        const uint32_t* __restrict__ pieces,
+                                                        const float4* __restrict__ rbox,
+                                                        const CodeParams* __restrict__ params, int code_type,
+                                                        int code_shift, int mesh_shift, K* __restrict__ keys) {
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= n_refs) return;
+    const long long g = ref_tri[r];
+    const int k = find_mesh(offsets, m, g);
+    unsigned long long code;
+    if (pieces[g] == 1u) {
+        code = tri_code(load_tri(meshes[k], g - meshes[k].first), params[k], code_type);
+    } else {
+        const float4 lo = rbox[2 * r], hi = rbox[2 * r + 1];
+        const float3 c = make_float3(__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f), __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
+                                     __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f));
+        code = point_code(c, __fsub_rn(hi.x, lo.x), __fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z), params[k],
+                          code_type);
+    }
+    code >>= code_shift;
+    if (mesh_shift > 0) code |= (unsigned long long)k << mesh_shift;
+    keys[r] = static_cast<K>(code);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1408,8 +1623,9 @@ __global__ void leaf_owner_kernel(LayoutParams P, uint32_t* __restrict__ contrib
 }
 
 __device__ __forceinline__ void write_tri(const MeshDesc* meshes, const long long* offsets, int m,
-                                          const uint32_t* perm, int pos, float4* tris, int slot) {
+                                          const uint32_t* perm, const int* ref_tri, int pos, float4* tris, int slot) {
     long long g = perm[pos];
+    if (ref_tri) g = ref_tri[g];  // a reference: its triangle
     int k = find_mesh(offsets, m, g);
     long long local = g - meshes[k].first;
     Tri t = load_tri(meshes[k], local);
@@ -1423,7 +1639,7 @@ __device__ __forceinline__ void write_tri(const MeshDesc* meshes, const long lon
 // its slot directly, so every thread gathers and writes one triangle (no per-leaf loop).
 __global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
                                   const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
-                                  const uint32_t* __restrict__ starts, int* __restrict__ leaf_start_of,
+                                  const int* __restrict__ ref_tri, const uint32_t* __restrict__ starts, int* __restrict__ leaf_start_of,
                                   float4* __restrict__ tris, const uint32_t* err) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.num_leaves || *err != 0u) return;
@@ -1438,7 +1654,7 @@ __global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ m
     const int first = node_pmin(P, x);
     const int start = (int)starts[first];
     if (p == first) leaf_start_of[x] = start;
-    write_tri(meshes, offsets, m, perm, p, tris, start + rank);
+    write_tri(meshes, offsets, m, perm, ref_tri, p, tris, start + rank);
 }
 
 __device__ __forceinline__ float pad_down(float lo, float hi) {
@@ -1717,7 +1933,7 @@ static dipl_status validate_desc(const dipl_build_desc& d) {
                    "sort_digit_bits must be 0, 6, 7, 8 or 10");
     DIPL_CHECK_ARG(d.clustering == DIPL_CLUSTER_HPLOC || d.clustering == DIPL_CLUSTER_PLOC,
                    "clustering must be DIPL_CLUSTER_HPLOC or DIPL_CLUSTER_PLOC");
-    DIPL_CHECK_ARG(d.reserved == 0, "reserved must be 0");
+    DIPL_CHECK_ARG(d.split_budget >= 0 && d.split_budget <= 100, "split_budget must be 0..100");
     return DIPL_OK;
 }
 
@@ -1730,10 +1946,13 @@ struct BuildPlan {
     std::vector<dipl_build_desc> descs;
     std::vector<int> mesh_of_desc;
     std::vector<MeshDesc> meshes;
-    std::vector<long long> offsets;
+    std::vector<long long> offsets;   // first triangle of every mesh (+ the total): vertex access
+    std::vector<long long> coffsets;  // first cluster leaf (reference) of every mesh (+ the total)
     dipl_build_desc d0{};
     int count = 0, m = 0, L = 4;
-    long long N = 0, K = 0, Kalloc = 1;
+    long long T = 0;                  // triangles of the batch
+    long long N = 0, K = 0, Kalloc = 1;  // cluster leaves (references; = T without pre-splitting), internal nodes
+    bool split = false;               // pre-splitting of large triangles
     int code_bits = 30, mesh_bits = 0, key_bits = 30, code_shift = 0, mesh_shift = 0, key_bytes = 4;
     int digit_bits = 8, B = 256, tiles0 = 1, tiles_max = 1;
     cudaStream_t stream = nullptr;
@@ -1742,6 +1961,10 @@ struct BuildPlan {
     uint32_t* d_err = nullptr;
     MeshDesc* d_meshes = nullptr;
     long long* d_offsets = nullptr;
+    long long* d_coffsets = nullptr;  // = d_offsets without pre-splitting
+    uint32_t *pieces = nullptr, *piece_first = nullptr;  // per triangle: references, first reference
+    unsigned long long* mesh_wsum = nullptr;
+    int* ref_tri = nullptr;           // per reference: its triangle (global index); NULL without pre-splitting
     Bounds* d_bounds = nullptr;
     CodeParams* d_params = nullptr;
     void *keys = nullptr, *keys_sorted = nullptr, *keys_alt = nullptr;
@@ -1778,6 +2001,8 @@ struct BuildPlan {
     }
 };
 
+static dipl_status enqueue_bounds_and_params(BuildPlan& P, cudaStream_t stream);
+
 static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int count, cudaStream_t stream,
                                 bool own_summary) {
     DIPL_CHECK_ARG(descs && count >= 1, "descs must be non-NULL and count >= 1");
@@ -1791,7 +2016,8 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
                            descs[i].layout == d0.layout && descs[i].max_triangles_per_leaf == d0.max_triangles_per_leaf &&
                            descs[i].nn_search_radius == d0.nn_search_radius && descs[i].kdop_size == d0.kdop_size &&
                            descs[i].ploc_block_size == d0.ploc_block_size &&
-                           descs[i].sort_digit_bits == d0.sort_digit_bits && descs[i].clustering == d0.clustering,
+                           descs[i].sort_digit_bits == d0.sort_digit_bits && descs[i].clustering == d0.clustering &&
+                           descs[i].split_budget == d0.split_budget,
                        "batched builds need one set of build options");
     }
     P.descs.assign(descs, descs + count);
@@ -1810,9 +2036,10 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
     DIPL_CHECK_ARG(total < (1ll << 27), "total triangles of a build must be < 2^27");
     P.m = (int)P.meshes.size();
     P.offsets.push_back(total);
+    P.T = total;
     P.N = total;
-    P.K = total - P.m;
-    P.Kalloc = std::max<long long>(P.K, 1);
+    P.coffsets = P.offsets;
+    P.split = d0.split_budget > 0;
     P.L = d0.max_triangles_per_leaf;
     P.out = std::make_shared<Storage>();
     P.out->stream = stream;
@@ -1820,9 +2047,10 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
     P.work->stream = stream;
     dipl_status st;
     if ((st = P.out->alloc(&P.d_err, 4)) != DIPL_OK) return st;
+    P.K = P.N - P.m;
+    P.Kalloc = std::max<long long>(P.K, 1);
     if (P.m == 0) return DIPL_OK;
     const int m = P.m;
-    const long long N = P.N, K = P.K, Kalloc = P.Kalloc;
     Storage& W = *P.work;
     Storage& O = *P.out;
     if ((st = W.alloc(&P.d_meshes, m)) != DIPL_OK || (st = W.alloc(&P.d_offsets, m + 1)) != DIPL_OK ||
@@ -1831,6 +2059,50 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
     DIPL_CUDA(cudaMemcpyAsync(P.d_meshes, P.meshes.data(), sizeof(MeshDesc) * m, cudaMemcpyHostToDevice, stream));
     DIPL_CUDA(cudaMemcpyAsync(P.d_offsets, P.offsets.data(), sizeof(long long) * (m + 1), cudaMemcpyHostToDevice,
                               stream));
+    P.d_coffsets = P.d_offsets;
+    if (P.split) {
+        // bounds and code parameters first (they are the triangles'), then the piece counts, their scan and every
+        // mesh's first reference; the reference count sizes everything after, so it is read back here
+        const long long T = P.T;
+        uint32_t* d_total = nullptr;
+        if ((st = W.alloc(&P.pieces, T)) != DIPL_OK || (st = W.alloc(&P.piece_first, T)) != DIPL_OK ||
+            (st = W.alloc(&P.mesh_wsum, m)) != DIPL_OK || (st = W.alloc(&P.d_coffsets, m + 1)) != DIPL_OK ||
+            (st = W.alloc(&d_total, 4)) != DIPL_OK)
+            return st;
+        unsigned char* scan_tmp = nullptr;
+        if ((st = W.alloc(&scan_tmp, scan_scratch_bytes(T))) != DIPL_OK) return st;
+        if ((st = enqueue_bounds_and_params(P, stream)) != DIPL_OK) return st;
+        DIPL_CUDA(cudaMemsetAsync(P.mesh_wsum, 0, sizeof(unsigned long long) * m, stream));
+        split_weight_kernel<<<blocks_for(T, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, T, P.d_bounds,
+                                                                    P.mesh_wsum);
+        note_launches();
+        split_count_kernel<<<blocks_for(T, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, T, P.d_bounds,
+                                                                   P.mesh_wsum, d0.split_budget, P.pieces);
+        note_launches();
+        DIPL_CUDA(cudaGetLastError());
+        if ((st = exclusive_scan_u32(P.pieces, P.piece_first, T, d_total, scan_tmp, stream, P.d_err)) != DIPL_OK)
+            return st;
+        mesh_ref_offsets_kernel<<<blocks_for(m + 1, 64), 64, 0, stream>>>(P.d_offsets, m, P.piece_first, d_total,
+                                                                          P.d_coffsets);
+        note_launches();
+        DIPL_CUDA(cudaGetLastError());
+        P.coffsets.assign(m + 1, 0);
+        DIPL_CUDA(cudaMemcpyAsync(P.coffsets.data(), P.d_coffsets, sizeof(long long) * (m + 1), cudaMemcpyDeviceToHost,
+                                  stream));
+        uint32_t err = 0;
+        DIPL_CUDA(cudaMemcpyAsync(&err, P.d_err, 4, cudaMemcpyDeviceToHost, stream));
+        DIPL_CUDA(cudaStreamSynchronize(stream));
+        if (err != 0u) {
+            set_last_error("build: a bounded device wait timed out while counting the pieces of large triangles");
+            return DIPL_ERR_TIMEOUT;
+        }
+        P.N = P.coffsets[m];
+        DIPL_CHECK_ARG(P.N < (1ll << 27), "references of a build (triangles and their pieces) must be < 2^27");
+        P.K = P.N - m;
+        P.Kalloc = std::max<long long>(P.K, 1);
+        if ((st = O.alloc(&P.ref_tri, P.N)) != DIPL_OK) return st;
+    }
+    const long long N = P.N, K = P.K, Kalloc = P.Kalloc;
     P.code_bits = d0.code_type == DIPL_CODE_MORTON30 ? 30 : 60;
     while ((1ll << P.mesh_bits) < m) ++P.mesh_bits;
     P.key_bits = P.code_bits + P.mesh_bits;
@@ -1897,36 +2169,66 @@ static dipl_status launch_ploc_any(const PlocParams& p, int tiles0, cudaStream_t
 }
 
 // Everything on the stream, nothing else: no allocation, no host copy from pageable memory, no synchronisation.
-static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
+// Scene bounds and code parameters of every mesh (from its triangles).
+static dipl_status enqueue_bounds_and_params(BuildPlan& P, cudaStream_t stream) {
+    const int m = P.m;
+    const long long T = P.T;
     DIPL_CUDA(cudaMemsetAsync(P.d_err, 0, 4, stream));
-    if (P.m == 0) return DIPL_OK;
+    bounds_init_kernel<<<blocks_for(m, 128), 128, 0, stream>>>(P.d_bounds, m);
+    note_launches();
+    {
+        long long grid = std::max<long long>(1, std::min<long long>((T + 1023) / 1024, 148 * 16));
+        long long chunk = (T + grid - 1) / grid;
+        bounds_kernel<<<(unsigned)grid, 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, T, chunk, P.d_bounds);
+        note_launches();
+    }
+    code_params_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(P.d_bounds, m, P.d0.code_type, P.d_params);
+    note_launches();
+    if (P.d0.code_type == DIPL_CODE_EMC60) {
+        emc_tables_kernel<<<(unsigned)m, 256, 0, stream>>>(P.d_params);
+        note_launches();
+    }
+    DIPL_CUDA(cudaGetLastError());
+    return DIPL_OK;
+}
+
+static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
+    if (P.m == 0) {
+        DIPL_CUDA(cudaMemsetAsync(P.d_err, 0, 4, stream));
+        return DIPL_OK;
+    }
     const int m = P.m;
     const long long N = P.N, K = P.K;
     const dipl_build_desc& d0 = P.d0;
     dipl_status st;
-    bounds_init_kernel<<<blocks_for(m, 128), 128, 0, stream>>>(P.d_bounds, m);
-    note_launches();
-    {
-        long long grid = std::max<long long>(1, std::min<long long>((N + 1023) / 1024, 148 * 16));
-        long long chunk = (N + grid - 1) / grid;
-        bounds_kernel<<<(unsigned)grid, 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, chunk, P.d_bounds);
+    if (P.split) {
+        // bounds and parameters were enqueued with the piece counts (plan_prepare): the references and their codes
+        split_kernel<<<blocks_for(P.T, 128), 128, 0, stream>>>(P.d_meshes, P.d_offsets, m, P.T, P.pieces,
+                                                               P.piece_first, P.ref_tri, P.tbox);
+        note_launches();
+        if (P.key_bytes == 4)
+            ref_codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(
+                P.d_meshes, P.d_offsets, m, N, P.ref_tri, P.pieces, P.tbox, P.d_params, d0.code_type, P.code_shift,
+                P.mesh_shift, (uint32_t*)P.keys);
+        else
+            ref_codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
+                P.d_meshes, P.d_offsets, m, N, P.ref_tri, P.pieces, P.tbox, P.d_params, d0.code_type, P.code_shift,
+                P.mesh_shift, (unsigned long long*)P.keys);
+        note_launches();
+    } else if ((st = enqueue_bounds_and_params(P, stream)) != DIPL_OK) {
+        return st;
+    }
+    if (!P.split) {  // (the references' codes are written above)
+        if (P.key_bytes == 4)
+            codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.d_params,
+                                                                           d0.code_type, P.code_shift, P.mesh_shift,
+                                                                           (uint32_t*)P.keys, P.tbox);
+        else
+            codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
+                P.d_meshes, P.d_offsets, m, N, P.d_params, d0.code_type, P.code_shift, P.mesh_shift,
+                (unsigned long long*)P.keys, P.tbox);
         note_launches();
     }
-    code_params_kernel<<<blocks_for(m, 64), 64, 0, stream>>>(P.d_bounds, m, d0.code_type, P.d_params);
-    note_launches();
-    if (d0.code_type == DIPL_CODE_EMC60) {
-        emc_tables_kernel<<<(unsigned)m, 256, 0, stream>>>(P.d_params);
-        note_launches();
-    }
-    if (P.key_bytes == 4)
-        codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.d_params,
-                                                                       d0.code_type, P.code_shift, P.mesh_shift,
-                                                                       (uint32_t*)P.keys, P.tbox);
-    else
-        codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
-            P.d_meshes, P.d_offsets, m, N, P.d_params, d0.code_type, P.code_shift, P.mesh_shift,
-            (unsigned long long*)P.keys, P.tbox);
-    note_launches();
     DIPL_CUDA(cudaGetLastError());
     st = radix_sort_pairs(P.keys, nullptr, P.keys_sorted, P.perm, P.keys_alt, P.perm_alt, N, P.key_bytes, 0,
                           P.key_bits, P.digit_bits, P.sort_scratch, stream, P.d_err);
@@ -1942,14 +2244,14 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
         DIPL_CUDA(cudaMemsetAsync(P.status, 0, sizeof(unsigned long long) * (2 * P.tiles_max + 2), stream));
     fill_int_kernel<<<blocks_for(N + K, 256), 256, 0, stream>>>(P.parent, N + K, -1);
     note_launches();
-    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_offsets, m, N, P.perm, P.tbox,
+    ploc_init_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(P.d_meshes, P.d_coffsets, m, N, P.perm, P.tbox,
                                                              P.c_lo[0], P.c_hi[0], P.c_in[0], P.parent);
     note_launches();
     DIPL_CUDA(cudaGetLastError());
     if (hier) {
         DIPL_CUDA(cudaMemsetAsync(P.hp_other, 0xFF, sizeof(int) * N, stream));
         HplocParams hp{};
-        hp.keys = P.keys_sorted, hp.offsets = P.d_offsets;
+        hp.keys = P.keys_sorted, hp.offsets = P.d_coffsets;
         hp.lo = P.c_lo[0], hp.hi = P.c_hi[0], hp.info = P.c_in[0];
         hp.child = P.child, hp.node_lo = P.nlo, hp.node_hi = P.nhi, hp.parent = P.parent;
         hp.other = P.hp_other, hp.cnt = P.hp_cnt, hp.fid = P.hp_fid;
@@ -1999,11 +2301,11 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     note_launches();
     if ((st = exclusive_scan_u32(P.contrib, P.contrib, N, nullptr, P.scan_scratch, stream, P.d_err)) != DIPL_OK)
         return st;
-    leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.contrib,
-                                                               P.leaf_start_of, P.tris, P.d_err);
+    leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.ref_tri,
+                                                               P.contrib, P.leaf_start_of, P.tris, P.d_err);
     note_launches();
     if (K > 0) {
-        node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.tbox, P.d_offsets, m, P.perm, P.rev_flags,
+        node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.tbox, P.d_coffsets, m, P.perm, P.rev_flags,
                                                                    P.leaf_start_of, P.nodes, P.d_sah, P.d_err);
         note_launches();
     }
@@ -2087,6 +2389,8 @@ static dipl_status plan_finish(BuildPlan& P, dipl_bvh** out, bool allow_wide) {
         h->node_lo = P.nlo;
         h->node_hi = P.nhi;
         h->batch_leaves = P.N;
+        h->batched = P.m > 1;
+        h->ref_tri = P.ref_tri;
         h->node_capacity = inner_total;
         h->ploc_iterations = iterations;
         const int k = P.mesh_of_desc[i];
@@ -2094,7 +2398,8 @@ static dipl_status plan_finish(BuildPlan& P, dipl_bvh** out, bool allow_wide) {
             const RootInfo& ri = h_roots[k];
             h->root = ri.root_ref;
             h->depth = ri.depth;
-            h->leaf_base = P.offsets[k];
+            h->leaf_base = P.coffsets[k];
+            h->num_refs = P.coffsets[k + 1] - P.coffsets[k];
             h->num_nodes = (int64_t)h_sah[2 * k + 1];
             h->sah_area = ri.root_area;
             h->sah_sum = h_sah[2 * k] + ri.leaf_cost;
@@ -2140,6 +2445,12 @@ dipl_status plan_create(const dipl_build_desc* descs, int count, dipl_build_plan
     *out = nullptr;
     auto holder = std::make_unique<dipl_build_plan>();
     BuildPlan& P = holder->plan;
+    for (int i = 0; i < count && descs; ++i)
+        if (descs[i].split_budget != 0) {
+            // the pieces depend on the vertex positions, which a plan's replays may change
+            set_last_error("pre-splitting (split_budget > 0) cannot be captured in a build plan");
+            return DIPL_ERR_UNSUPPORTED;
+        }
     dipl_status st = plan_prepare(P, descs, count, stream, true);
     if (st != DIPL_OK) return st;
     if (P.d0.layout == DIPL_LAYOUT_WIDE8_Q8) {

@@ -127,6 +127,9 @@ struct dipl_bvh {
     int64_t leaf_base = 0;      // first leaf id of this mesh in the batch numbering
     int64_t inner_base = 0;     // first internal node index of this mesh
     int64_t batch_leaves = 0;   // leaves of the whole batch (internal node id = batch_leaves + k)
+    int64_t num_refs = 0;       // clustering leaves of this mesh: its triangles, or triangles and pieces
+    bool batched = false;       // one of several meshes built together (they share the arrays)
+    const int* ref_tri = nullptr;  // per leaf of the batch: its triangle (global index); NULL without pre-splitting
     double sah_area = 0.0;      // surface area of the root box
     double sah_sum = 0.0;       // sum over inner SA + leaf SA * count (FP64, device-summed)
     // device error word shared by the build and later traces

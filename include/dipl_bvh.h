@@ -99,7 +99,12 @@ typedef struct dipl_build_desc {
     int32_t ploc_block_size;        /* clustering threads per block: 0 = auto, else 128, 256 or 512 */
     int32_t sort_digit_bits;        /* radix sort digit width: 0 = auto (8), else 6, 7, 8 or 10 */
     int32_t clustering;             /* dipl_clustering (ABI version 2) */
-    int32_t reserved;               /* 0 */
+    int32_t split_budget;           /* pre-splitting of large triangles (ABI version 2): at most this percentage
+                                       more clustering leaves than triangles, 0..100; 0 = none (the default). A
+                                       triangle whose box is large against its mesh's others enters the clustering
+                                       as pieces (the boxes of its parts in halves of its box); leaves still hold
+                                       the whole triangle, so hits are the same and rays meet fewer empty boxes.
+                                       One-shot builds only (not in build plans). */
 } dipl_build_desc;
 
 /* A ray: origin, hit interval lower bound, direction, upper bound (32 bytes). A hit needs
@@ -122,16 +127,17 @@ typedef struct dipl_bvh dipl_bvh; /* opaque, owns its device memory */
 typedef struct dipl_bvh_info {
     int64_t num_triangles;
     int64_t num_inner_nodes;     /* nodes of the traced layout */
-    int64_t num_leaves;
+    int64_t num_leaves;          /* clustering leaves: the triangles, and their pieces with pre-splitting */
     int64_t node_bytes;          /* bytes of the traced node array */
-    int64_t triangle_bytes;      /* bytes of the leaf triangle array */
+    int64_t triangle_bytes;      /* bytes of the leaf triangle array (one record per clustering leaf) */
     int32_t depth;               /* levels of the clustering tree (bounds the traversal stack) */
     int32_t ploc_iterations;     /* PLOC: global iterations; HPLOC: iterations of all tree nodes, summed */
     int32_t code_type, bv_type, layout, max_triangles_per_leaf, nn_search_radius, kdop_size;
     int32_t clustering, reserved; /* dipl_clustering (ABI version 2) */
 } dipl_bvh_info;
 
-/* Fills a description with the defaults (Morton30, AABB, binary, leaves < 4, r = 16, 32-DOP, auto, HPLOC). */
+/* Fills a description with the defaults (Morton30, AABB, binary, leaves < 4, r = 16, 32-DOP, auto, HPLOC, no
+ * pre-splitting). */
 DIPL_API void dipl_build_desc_init(dipl_build_desc* desc);
 
 /* Builds a BVH over desc->num_triangles triangles (0 is allowed: every ray misses).
@@ -194,10 +200,11 @@ DIPL_API dipl_status dipl_bvh_sah_cost(const dipl_bvh* bvh, double* cost, void* 
 
 DIPL_API dipl_status dipl_bvh_get_info(const dipl_bvh* bvh, dipl_bvh_info* info);
 
-/* Copies the clustering result to HOST buffers (any may be NULL): h_perm[num_triangles] = triangle id at
- * each sorted-code position (leaf node id = position); h_children[2*(num_triangles-1)] = left/right node
+/* Copies the clustering result to HOST buffers (any may be NULL); n = num_leaves of dipl_bvh_get_info (the
+ * triangle count without pre-splitting): h_perm[n] = triangle id at each sorted-code position (leaf node id =
+ * position; a split triangle appears once per piece); h_children[2*(n-1)] = left/right node
  * ids of internal node k (id num_triangles + k; PLOC numbers nodes in creation order, HPLOC gives node k the
- * id of radix-tree split k or of a split below it); h_boxes[6*(num_triangles-1)] = its box
+ * id of radix-tree split k or of a split below it); h_boxes[6*(n-1)] = its box
  * (lo xyz, hi xyz). Synchronises `stream`. For checking and debugging. */
 DIPL_API dipl_status dipl_bvh_download_topology(const dipl_bvh* bvh, int32_t* h_perm, int32_t* h_children, float* h_boxes,
                                        void* stream);

@@ -642,8 +642,29 @@ static int hploc_merge(orc_cluster* L, int c, int target, int radius, const int3
 /* codes: sorted codes (one per sorted position); perm, seg as in orc_ploc. threshold in [1, 32].
  * children/boxes are indexed by id - n for ids n .. 2n - 2 (minus one per extra segment).
  * Returns the number of internal nodes, or -1 on bad input. */
+int64_t orc_hploc_boxes(const float* leaf_boxes, int64_t n, const uint64_t* codes, const int32_t* seg, int radius,
+                        int threshold, int32_t* children, float* boxes, int32_t* iterations);
+
 int64_t orc_hploc(const float* tris, int64_t n, const int32_t* perm, const uint64_t* codes, const int32_t* seg,
                   int radius, int threshold, int32_t* children, float* boxes, int32_t* iterations) {
+    if (n <= 0) return 0;
+    float* lb = (float*)malloc(sizeof(float) * 6 * (size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = tris + 9 * (int64_t)perm[i];
+        const int fin = tri_finite(p);
+        for (int a = 0; a < 3; ++a) {
+            lb[6 * i + a] = fin ? fminf(fminf(p[a], p[3 + a]), p[6 + a]) : INFINITY;
+            lb[6 * i + 3 + a] = fin ? fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]) : -INFINITY;
+        }
+    }
+    int64_t r = orc_hploc_boxes(lb, n, codes, seg, radius, threshold, children, boxes, iterations);
+    free(lb);
+    return r;
+}
+
+/* The same over given leaf boxes (6 floats per sorted position: lo xyz, hi xyz), e.g. pre-split references. */
+int64_t orc_hploc_boxes(const float* leaf_boxes, int64_t n, const uint64_t* codes, const int32_t* seg, int radius,
+                        int threshold, int32_t* children, float* boxes, int32_t* iterations) {
     if (n <= 0) return 0;
     if (radius < 1 || threshold < 1 || threshold > 32) return -1;
     orc_cluster* clus = (orc_cluster*)malloc(sizeof(orc_cluster) * (size_t)n);
@@ -651,11 +672,9 @@ int64_t orc_hploc(const float* tris, int64_t n, const int32_t* perm, const uint6
     int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)n); /* list length of the node starting at l */
     int64_t* other = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 1 ? n - 1 : 1));
     for (int64_t i = 0; i < n; ++i) {
-        const float* p = tris + 9 * (int64_t)perm[i];
-        const int fin = tri_finite(p);
         for (int a = 0; a < 3; ++a) {
-            clus[i].lo[a] = fin ? fminf(fminf(p[a], p[3 + a]), p[6 + a]) : INFINITY;
-            clus[i].hi[a] = fin ? fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]) : -INFINITY;
+            clus[i].lo[a] = leaf_boxes[6 * i + a];
+            clus[i].hi[a] = leaf_boxes[6 * i + 3 + a];
         }
         clus[i].node = (int32_t)i;
         clus[i].seg = seg ? seg[i] : 0;
@@ -1066,5 +1085,203 @@ void orc_shadow_rays(const float* tris, const float* rays, const int32_t* prim, 
             q[0] = org.x, q[1] = org.y, q[2] = org.z, q[3] = ORC_EPS;
             q[4] = dir.x, q[5] = dir.y, q[6] = dir.z, q[7] = dist * (1.0f - eps);
         }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Pre-splitting of large triangles (the build's split_budget), restated: per mesh, the weights  */
+/* q = floor(w 2^32 / D^2) of the triangle boxes (w = (dx dy + dy dz) + dz dx in FP32, D = the     */
+/* mesh's vertex-box diagonal), their exact sum Q, the piece counts                                */
+/* 1 + min(63, floor(q budget N / (100 Q))), and the pieces: a box of c pieces is split at its    */
+/* longest axis' midpoint, each half's box is the box of the triangle clipped to that half          */
+/* (Sutherland-Hodgman, crossing points on the plane exactly, clamped to the half; empty: the half */
+/* itself), ceil(c/2) pieces to the lower half first. One mesh (seg = NULL) or meshes of the given  */
+/* sizes in input order.                                                                            */
+/* ------------------------------------------------------------------------------------------ */
+static uint64_t orc_split_weight(const float* p, float diag) {
+    if (!tri_finite(p) || !(diag > 0.0f)) return 0;
+    float lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = fminf(fminf(p[a], p[3 + a]), p[6 + a]);
+        hi[a] = fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]);
+    }
+    float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    float w = (dx * dy + dy * dz) + dz * dx;
+    double scale = 4294967296.0 / ((double)diag * (double)diag);
+    double q = (double)w * scale;
+    return q < 1.8e19 ? (uint64_t)q : (uint64_t)18000000000000000000ull;
+}
+
+static void orc_clipped_box(const float* t, const float* lo, const float* hi, float* olo, float* ohi) {
+    float P[9][3], Q[9][3];
+    int np = 3;
+    for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) P[i][c] = t[3 * i + c];
+    for (int plane = 0; plane < 6 && np > 0; ++plane) {
+        int a = plane >> 1, low = (plane & 1) == 0, nq = 0;
+        float b = low ? lo[a] : hi[a];
+        for (int i = 0; i < np; ++i) {
+            const float* p = P[i];
+            const float* q = P[i + 1 < np ? i + 1 : 0];
+            int ip = low ? p[a] >= b : p[a] <= b, iq = low ? q[a] >= b : q[a] <= b;
+            if (ip && nq < 9) Q[nq][0] = p[0], Q[nq][1] = p[1], Q[nq][2] = p[2], ++nq;
+            if (ip != iq && nq < 9) {
+                float s = (b - p[a]) / (q[a] - p[a]);
+                for (int c = 0; c < 3; ++c) Q[nq][c] = c == a ? b : p[c] + s * (q[c] - p[c]);
+                ++nq;
+            }
+        }
+        np = nq;
+        for (int i = 0; i < np; ++i) P[i][0] = Q[i][0], P[i][1] = Q[i][1], P[i][2] = Q[i][2];
+    }
+    if (np == 0) {
+        for (int c = 0; c < 3; ++c) olo[c] = lo[c], ohi[c] = hi[c];
+        return;
+    }
+    for (int c = 0; c < 3; ++c) {
+        float mn = P[0][c], mx = P[0][c];
+        for (int i = 1; i < np; ++i) mn = fminf(mn, P[i][c]), mx = fmaxf(mx, P[i][c]);
+        olo[c] = fmaxf(mn, lo[c]);
+        ohi[c] = fminf(mx, hi[c]);
+    }
+}
+
+/* tris: all meshes' triangles in input order; mesh_sizes[nm]. Writes pieces[n] and, when ref_tri != NULL, the
+ * references (ref_tri[R], rbox[R][6] = lo xyz, hi xyz). Returns R. */
+int64_t orc_presplit(const float* tris, int64_t n, const int64_t* mesh_sizes, int nm, int budget, uint32_t* pieces,
+                     int32_t* ref_tri, float* rbox) {
+    int64_t first = 0, r = 0;
+    for (int k = 0; k < nm; ++k) {
+        const float* mt = tris + 9 * first;
+        const int64_t nk = mesh_sizes[k];
+        float cmin[3], cmax[3], bmin[3], bmax[3];
+        orc_scene_bounds(mt, nk, cmin, cmax, bmin, bmax);
+        float diag = orc_scene_diag(bmin, bmax);
+        uint64_t sum = 0;
+        for (int64_t i = 0; i < nk; ++i) sum += orc_split_weight(mt + 9 * i, diag);
+        for (int64_t i = 0; i < nk; ++i) {
+            uint64_t q = orc_split_weight(mt + 9 * i, diag);
+            uint32_t c = 1;
+            if (sum != 0 && q != 0) {
+                double num = ((double)q * (double)budget) * (double)nk;
+                double den = 100.0 * (double)sum;
+                double s = floor(num / den);
+                c = 1u + (uint32_t)(s < 63.0 ? s : 63.0);
+            }
+            pieces[first + i] = c;
+            const float* p = mt + 9 * i;
+            float blo[3], bhi[3];
+            for (int a = 0; a < 3; ++a) {
+                int fin = tri_finite(p);
+                blo[a] = fin ? fminf(fminf(p[a], p[3 + a]), p[6 + a]) : INFINITY;
+                bhi[a] = fin ? fmaxf(fmaxf(p[a], p[3 + a]), p[6 + a]) : -INFINITY;
+            }
+            if (!ref_tri) {
+                r += c;
+                continue;
+            }
+            struct {
+                float lo[3], hi[3];
+                int c;
+            } st[8];
+            int sp = 0;
+            for (int a = 0; a < 3; ++a) st[0].lo[a] = blo[a], st[0].hi[a] = bhi[a];
+            st[0].c = (int)c;
+            sp = 1;
+            while (sp > 0) {
+                --sp;
+                float lo[3], hi[3];
+                int cc = st[sp].c;
+                for (int a = 0; a < 3; ++a) lo[a] = st[sp].lo[a], hi[a] = st[sp].hi[a];
+                if (cc == 1) {
+                    ref_tri[r] = (int32_t)(first + i);
+                    for (int a = 0; a < 3; ++a) rbox[6 * r + a] = lo[a], rbox[6 * r + 3 + a] = hi[a];
+                    ++r;
+                    continue;
+                }
+                float e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = hi[2] - lo[2];
+                int ax = (e0 >= e1 && e0 >= e2) ? 0 : (e1 >= e2 ? 1 : 2);
+                float mid = lo[ax] + (hi[ax] - lo[ax]) * 0.5f;
+                float llo[3], lhi[3], ulo[3], uhi[3], tl[3], th[3];
+                for (int a = 0; a < 3; ++a) llo[a] = ulo[a] = lo[a], lhi[a] = uhi[a] = hi[a];
+                lhi[ax] = mid;
+                ulo[ax] = mid;
+                orc_clipped_box(p, llo, lhi, tl, th);
+                for (int a = 0; a < 3; ++a) llo[a] = tl[a], lhi[a] = th[a];
+                orc_clipped_box(p, ulo, uhi, tl, th);
+                for (int a = 0; a < 3; ++a) ulo[a] = tl[a], uhi[a] = th[a];
+                if (sp + 2 > 8) break;
+                for (int a = 0; a < 3; ++a) st[sp].lo[a] = ulo[a], st[sp].hi[a] = uhi[a];
+                st[sp].c = cc / 2;
+                ++sp;
+                for (int a = 0; a < 3; ++a) st[sp].lo[a] = llo[a], st[sp].hi[a] = lhi[a];
+                st[sp].c = (cc + 1) / 2;
+                ++sp;
+            }
+        }
+        first += nk;
+    }
+    return r;
+}
+
+/* Codes of the references of one mesh (the build's ref_codes_kernel): an unsplit triangle's code as orc_morton30 /
+ * orc_emc60 compute it; a piece's from its box centre ((lo + hi) * 0.5) and box diagonal. Bounds are the mesh's
+ * triangles' (orc_scene_bounds). code_type 0: Morton30, 1: EMC60. */
+void orc_ref_codes(const float* tris, int64_t n, const uint32_t* pieces, const int32_t* ref_tri, const float* rbox,
+                   int64_t nr, int code_type, uint64_t* codes) {
+    float cmin[3], cmax[3], bmin[3], bmax[3];
+    orc_scene_bounds(tris, n, cmin, cmax, bmin, bmax);
+    float diag = orc_scene_diag(bmin, bmax);
+    int bits[4] = {10, 10, 10, 0};
+    uint64_t masks[4] = {0, 0, 0, 0};
+    float lo4[4] = {cmin[0], cmin[1], cmin[2], 0.0f};
+    float ext[4] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2], diag};
+    float s[4];
+    uint64_t top[4];
+    if (code_type == 1) orc_emc60_plan(cmin, cmax, diag, bits, masks);
+    for (int a = 0; a < 4; ++a) {
+        if (code_type == 0) {
+            s[a] = a < 3 && ext[a] > 0.0f ? 1024.0f / ext[a] : 0.0f;
+            top[a] = 1023;
+        } else {
+            float cells = ldexpf(1.0f, bits[a]);
+            s[a] = (ext[a] > 0.0f && bits[a] > 0) ? cells / ext[a] : 0.0f;
+            top[a] = bits[a] >= 64 ? ~(uint64_t)0 : (((uint64_t)1 << bits[a]) - 1);
+        }
+    }
+    for (int64_t r = 0; r < nr; ++r) {
+        const int32_t g = ref_tri[r];
+        const float* p = tris + 9 * (int64_t)g;
+        float x[4], dx, dy, dz;
+        if (pieces[g] == 1) {
+            centroid(p, x);
+            dx = fmaxf(fmaxf(p[0], p[3]), p[6]) - fminf(fminf(p[0], p[3]), p[6]);
+            dy = fmaxf(fmaxf(p[1], p[4]), p[7]) - fminf(fminf(p[1], p[4]), p[7]);
+            dz = fmaxf(fmaxf(p[2], p[5]), p[8]) - fminf(fminf(p[2], p[5]), p[8]);
+        } else {
+            const float* b = rbox + 6 * r;
+            for (int a = 0; a < 3; ++a) x[a] = (b[a] + b[3 + a]) * 0.5f;
+            dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+        }
+        if (code_type == 0) {
+            uint32_t q[3];
+            for (int a = 0; a < 3; ++a) {
+                float v = (x[a] - cmin[a]) * s[a];
+                v = fminf(fmaxf(v, 0.0f), 1023.0f);
+                q[a] = (uint32_t)v;
+            }
+            codes[r] = (uint64_t)((expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]));
+            continue;
+        }
+        x[3] = sqrtf((dx * dx + dy * dy) + dz * dz);
+        uint64_t code = 0;
+        for (int a = 0; a < 4; ++a) {
+            if (bits[a] == 0) continue;
+            float q = fmaxf((x[a] - lo4[a]) * s[a], 0.0f);
+            uint64_t qi = q < 1.8e19f ? (uint64_t)q : top[a];
+            if (qi > top[a]) qi = top[a];
+            code |= deposit(qi, masks[a]);
+        }
+        codes[r] = code;
     }
 }

@@ -234,6 +234,11 @@ class Oracle:
                                          _u8p, _i32p, _f32p]
         L.orc_shadow_rays.argtypes = [_f32p, _f32p, _i32p, _f32p, C.c_int64, C.c_int, _i32p, C.c_int, C.c_int, _f32p,
                                       C.c_int, C.c_uint32, _f32p]
+        L.orc_hploc_boxes.restype = C.c_int64
+        L.orc_hploc_boxes.argtypes = [_f32p, C.c_int64, _u64p, C.c_void_p, C.c_int, C.c_int, _i32p, _f32p, _i32p]
+        L.orc_presplit.restype = C.c_int64
+        L.orc_presplit.argtypes = [_f32p, C.c_int64, _i64p, C.c_int, C.c_int, _u32p, C.c_void_p, C.c_void_p]
+        L.orc_ref_codes.argtypes = [_f32p, C.c_int64, _u32p, _i32p, _f32p, C.c_int64, C.c_int, _u64p]
         L.orc_pinhole_rays.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
         L.orc_bounce_rays.argtypes = [_f32p, _f32p, _i32p, _f32p, C.c_int64, C.c_uint32, _f32p]
 
@@ -367,6 +372,41 @@ class Oracle:
         self.lib.orc_retrace_binary(nodes, len(nodes) // 16, tris, int(root), rays, n, int(backface), visits, tests,
                                     stable, prim, t)
         return visits, tests, stable.astype(bool), prim, t
+
+    def presplit(self, tris, budget, mesh_sizes=None):
+        """Pre-splitting of large triangles (orc_presplit): (pieces per triangle, ref_tri (R,), ref boxes (R, 6))."""
+        tris = _tris(tris)
+        sizes = np.ascontiguousarray([len(tris)] if mesh_sizes is None else mesh_sizes, np.int64)
+        pieces = np.zeros(len(tris), np.uint32)
+        total = self.lib.orc_presplit(tris, len(tris), sizes, len(sizes), int(budget), pieces, None, None)
+        ref_tri = np.zeros(max(total, 1), np.int32)
+        rbox = np.zeros((max(total, 1), 6), np.float32)
+        self.lib.orc_presplit(tris, len(tris), sizes, len(sizes), int(budget), pieces,
+                              ref_tri.ctypes.data_as(C.c_void_p), rbox.ctypes.data_as(C.c_void_p))
+        return pieces, ref_tri[:total], rbox[:total]
+
+    def ref_codes(self, tris, pieces, ref_tri, rbox, code_type):
+        """Codes of one mesh's references (orc_ref_codes): 0 Morton30 (in uint64), 1 EMC60."""
+        tris = _tris(tris)
+        codes = np.zeros(len(ref_tri), np.uint64)
+        self.lib.orc_ref_codes(tris, len(tris), np.ascontiguousarray(pieces, np.uint32),
+                               np.ascontiguousarray(ref_tri, np.int32), np.ascontiguousarray(rbox, np.float32),
+                               len(ref_tri), int(code_type), codes)
+        return codes
+
+    def hploc_boxes(self, leaf_boxes, sorted_keys, radius=16, threshold=16):
+        """orc_hploc over given leaf boxes in sorted order (e.g. pre-split references)."""
+        lb = np.ascontiguousarray(leaf_boxes, np.float32)
+        n = len(lb)
+        rows = max(n - 1, 1)
+        children = np.full(2 * rows, -1, np.int32)
+        boxes = np.zeros(6 * rows, np.float32)
+        it = np.zeros(1, np.int32)
+        k = self.lib.orc_hploc_boxes(lb, n, np.ascontiguousarray(sorted_keys).astype(np.uint64), None, int(radius),
+                                     int(threshold), children, boxes, it)
+        if k < 0:
+            raise ValueError("orc_hploc_boxes: bad input")
+        return children[: 2 * (n - 1)].reshape(-1, 2), boxes[: 6 * (n - 1)].reshape(-1, 6), int(it[0])
 
     def ploc(self, tris, perm, radius=16, seg=None, nseg=1):
         """Returns (children (K,2) int32, boxes (K,6) float32, iterations)."""

@@ -176,3 +176,37 @@ def test_empty_and_tiny_builds():
         bvh = build(tris)
         info = bvh.info()
         assert info.num_triangles == n
+
+
+@pytest.mark.parametrize("kind", [A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmc])
+@pytest.mark.parametrize("budget", [20, 100])
+def test_presplit_topology_matches_oracle(orc, kind, budget):
+    """Pre-splitting: the device's pieces, their codes, sort and hierarchical clustering equal the restatement bit
+    for bit (leaf order by triangle, every internal node's children and box)."""
+    tris = np.concatenate([S.soup(30000, seed=41), S.soup(5, seed=42) * 40.0])  # a few very large triangles too
+    bvh = build(tris, kind, split_budget=budget)
+    perm, ch, bx = bvh.download_topology()
+    pieces, ref_tri, rbox = orc.presplit(tris, budget)
+    code = 0 if kind is A.AccelerationStructureType.kPloc else 1
+    codes = orc.ref_codes(tris, pieces, ref_tri, rbox, code)
+    order = np.argsort(codes, kind="stable")
+    assert bvh.info().num_leaves == len(ref_tri) > len(tris)
+    np.testing.assert_array_equal(perm, ref_tri[order])
+    ech, ebx, it = orc.hploc_boxes(rbox[order], codes[order])
+    np.testing.assert_array_equal(ch, ech)
+    np.testing.assert_array_equal(bx.view(np.uint32), ebx.view(np.uint32))
+    assert bvh.info().ploc_iterations == it
+
+
+def test_presplit_changes_nothing_on_an_even_mesh():
+    """No triangle of a displaced sphere is split: the build equals the one without pre-splitting."""
+    tris = S.uv_sphere(256, 128, 1.0, (0, 0, 0), displacement=0.05, seed=2)
+    a, b = build(tris), build(tris, split_budget=40)
+    for x, y in zip(a.download_topology(), b.download_topology()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_presplit_rejected_in_build_plans():
+    with pytest.raises(L.DiplError) as e:
+        A.BuildPlan(A.AccelerationStructureConfig(split_budget=20), [torch.from_numpy(S.soup(100, seed=1))])
+    assert e.value.status == 6  # DIPL_ERR_UNSUPPORTED

@@ -17,6 +17,7 @@ pytestmark = pytest.mark.gpu
 N = 16 * 1024 * 1024
 SAMPLE = 4096
 FORMS = [("ploc_emc", A.AccelerationStructureType.kPlocEmc, "binary"),
+         ("ploc_emc_split40", A.AccelerationStructureType.kPlocEmc, "binary"),
          ("ploc", A.AccelerationStructureType.kPloc, "binary"),
          ("ploc_emc_sobb", A.AccelerationStructureType.kPlocEmcSobb, "binary"),
          ("ploc_emc_wide8_q8", A.AccelerationStructureType.kPlocEmc, "wide8_q8")]
@@ -47,7 +48,7 @@ def test_soup16m_forms_bit_exact_on_a_ray_sample_and_every_hit_retests(orc, soup
     rays_dev = torch.from_numpy(rays).cuda()
     first = None
     for name, kind, layout in FORMS:
-        bvh = build(tris, kind, layout=layout)
+        bvh = build(tris, kind, layout=layout, split_budget=40 if name.endswith("split40") else 0)
         prim, t, u, v = _hits(bvh, rays_dev)
         cls = O.classify_hits(prim[idx], t[idx], u[idx], v[idx], brute, sbvh)
         assert cls["E"] == SAMPLE and cls["F"] == 0 and cls["T"] == 0, (name, cls)

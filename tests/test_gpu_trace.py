@@ -13,13 +13,15 @@ pytestmark = pytest.mark.gpu
 KINDS = [A.AccelerationStructureType.kPloc, A.AccelerationStructureType.kPlocEmc]
 
 
+@pytest.mark.parametrize("split", [0, 60])
 @pytest.mark.parametrize("layout", ["binary", "wide8_q8"])
 @pytest.mark.parametrize("kind", KINDS)
 @pytest.mark.parametrize("name", GOLDEN_NAMES)
-def test_ref_mt_hits_bit_exact_with_reference_brute_force(name, kind, layout):
-    """Class E/T of the parity protocol: id, t, u, v bit-equal to DummyAccelerationStucture::Intersect."""
+def test_ref_mt_hits_bit_exact_with_reference_brute_force(name, kind, layout, split):
+    """Class E/T of the parity protocol: id, t, u, v bit-equal to DummyAccelerationStucture::Intersect (also with
+    large triangles pre-split: leaves hold whole triangles, so the records cannot change)."""
     g = load_golden(name)
-    bvh = build(g["tris"], kind, layout=layout)
+    bvh = build(g["tris"], kind, layout=layout, split_budget=split)
     prim, t, u, v = trace(bvh, g["rays"], leaf_test="ref_mt")
     np.testing.assert_array_equal(prim, g["brute_prim"])
     np.testing.assert_array_equal(fbits(t), fbits(g["brute_t"]))
@@ -362,3 +364,28 @@ def test_counted_trace_totals_equal_a_host_retraversal(orc, name, clustering):
     torch.cuda.synchronize()
     assert st.accel_stats.traversal_count == int(visits[stable].sum())
     assert st.accel_stats.intersection_count == int(tests[stable].sum())
+
+
+@pytest.mark.parametrize("form", ["binary", "sobb", "wide8_q8"])
+def test_presplit_hits_equal_brute_force_on_a_dense_soup(orc, form):
+    """A soup at the 16M soup's density (200k triangles in a 0.31 cube: large triangles overlap everywhere), split
+    at budget 40: every form's hits equal the brute force's bit for bit, and the rays visit fewer nodes and test
+    fewer triangles than without splitting."""
+    tris = S.soup(200_000, seed=44)
+    c = tris.mean(axis=1, keepdims=True)
+    tris = ((tris - c) + c * 0.31).astype(np.float32)
+    rays = S.random_rays(8192, seed=44)
+    rays[:, 0:3] *= 0.31
+    kind = A.AccelerationStructureType.kPlocEmcSobb if form == "sobb" else A.AccelerationStructureType.kPlocEmc
+    layout = "wide8_q8" if form == "wide8_q8" else "binary"
+    h = orc.brute(tris, rays)
+    counts = []
+    for split in (0, 40):
+        bvh = build(tris, kind, layout=layout, split_budget=split)
+        prim, t, u, v = trace(bvh, rays)
+        np.testing.assert_array_equal(prim, h.prim)
+        np.testing.assert_array_equal(fbits(t), fbits(h.t))
+        st = A.Stats()
+        bvh.Intersect(st, torch.from_numpy(rays), count=True)
+        counts.append((st.accel_stats.traversal_count, st.accel_stats.intersection_count))
+    assert counts[1][0] < 0.8 * counts[0][0] and counts[1][1] < 0.6 * counts[0][1], counts

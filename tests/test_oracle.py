@@ -180,3 +180,38 @@ def test_hierarchical_clustering_makes_one_binary_tree_per_segment(orc, n, nseg)
         a, b = ch[k]
         np.testing.assert_array_equal(bx[k, :3], np.minimum(lo(a), lo(b)))
         np.testing.assert_array_equal(bx[k, 3:], np.maximum(hi(a), hi(b)))
+
+
+@pytest.mark.parametrize("budget", [10, 40, 100])
+def test_presplit_pieces_cover_their_triangles(orc, budget):
+    """Pre-splitting (restated): the split triangles are the large ones, at most budget% more leaves, every piece box
+    lies in its triangle's box, and the pieces' boxes together cover the triangle (points sampled on it)."""
+    tris = S.soup(20000, seed=31)
+    pieces, ref_tri, rbox = orc.presplit(tris, budget)
+    n = len(tris)
+    assert len(ref_tri) == int(pieces.sum()) and len(ref_tri) <= n + (budget * n) // 100
+    assert (pieces > 1).any() and pieces.max() <= 64
+    lo, hi = tris.min(axis=1), tris.max(axis=1)
+    d = hi - lo
+    w = (d[:, 0] * d[:, 1] + d[:, 1] * d[:, 2]) + d[:, 2] * d[:, 0]
+    assert w[pieces > 1].min() >= np.median(w)          # only large triangles split
+    assert (np.diff(ref_tri) >= 0).all()                 # references in triangle order
+    assert (rbox[:, :3] >= lo[ref_tri]).all() and (rbox[:, 3:] <= hi[ref_tri]).all()
+    rng = np.random.default_rng(budget)
+    for g in np.nonzero(pieces > 1)[0][:200]:
+        boxes = rbox[ref_tri == g].astype(np.float64)
+        a, b = rng.random(64), rng.random(64)
+        flip = a + b > 1
+        a[flip], b[flip] = 1 - a[flip], 1 - b[flip]
+        t = tris[g].astype(np.float64)
+        pts = t[0] + a[:, None] * (t[1] - t[0]) + b[:, None] * (t[2] - t[0])
+        slack = 1e-6 * np.abs(t).max()
+        inside = ((pts[:, None, :] >= boxes[None, :, :3] - slack) & (pts[:, None, :] <= boxes[None, :, 3:] + slack))
+        assert inside.all(axis=2).any(axis=1).all(), g
+
+
+def test_presplit_leaves_even_meshes_alone(orc):
+    """A mesh of triangles of about equal size (a displaced sphere) gets no pieces at a moderate budget."""
+    tris = S.uv_sphere(128, 64, 1.0, (0, 0, 0), displacement=0.05, seed=2)
+    pieces, ref_tri, _ = orc.presplit(tris, 40)
+    assert (pieces == 1).all() and len(ref_tri) == len(tris)
