@@ -1601,6 +1601,23 @@ __global__ void inner_flags_kernel(LayoutParams P, uint32_t* __restrict__ rev_fl
     rev_flags[P.num_inner - 1 - k] = f;
 }
 
+// Inner-node numbering by height (hierarchical clustering): sort keys, then each inner node's traced index is its
+// rank, stored where the reverse-order consumers read it (rev_index[num_inner - 1 - k]).
+__global__ void height_keys_kernel(LayoutParams P, uint32_t* __restrict__ keys, const uint32_t* err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.num_inner) return;
+    const bool inner = (*err == 0u) && __float_as_int(P.node_lo[k].w) >= P.L;
+    keys[k] = inner ? 254u - (uint32_t)min(max(P.child[k].z, 0), 254) : 255u;
+}
+
+__global__ void height_index_kernel(LayoutParams P, const uint32_t* __restrict__ order, uint32_t* __restrict__ rev_index,
+                                    const uint32_t* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.num_inner || *err != 0u) return;
+    const int k = (int)order[i];
+    if (__float_as_int(P.node_lo[k].w) >= P.L) rev_index[P.num_inner - 1 - k] = (uint32_t)i;  // inner nodes sort first
+}
+
 __global__ void leaf_owner_kernel(LayoutParams P, uint32_t* __restrict__ contrib, int* __restrict__ owner_leaf,
                                   const uint32_t* err) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2296,6 +2313,22 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
         if ((st = exclusive_scan_u32(P.rev_flags, P.rev_flags, K, P.d_counts, P.scan_scratch, stream, P.d_err)) !=
             DIPL_OK)
             return st;
+        if (hier) {
+            // Hierarchical ids follow split positions, so reverse id order would scatter the tree's top levels over
+            // the whole node array. Number the inner nodes by height instead, the tallest (the roots) first, ties
+            // by id: the top levels every ray visits sit together at the front, as with the global loop's reverse
+            // creation order. A one-pass stable sort of 8-bit keys (255 - height; 255 for nodes inside leaves).
+            uint32_t* hkeys = reinterpret_cast<uint32_t*>(P.keys);
+            uint32_t* hsorted = reinterpret_cast<uint32_t*>(P.keys_sorted);
+            height_keys_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, hkeys, P.d_err);
+            note_launches();
+            DIPL_CUDA(cudaGetLastError());
+            if ((st = radix_sort_pairs(hkeys, nullptr, hsorted, P.perm_alt, P.keys_alt, P.contrib, K, 4, 0, 8, 8,
+                                       P.sort_scratch, stream, P.d_err)) != DIPL_OK)
+                return st;
+            height_index_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.perm_alt, P.rev_flags, P.d_err);
+            note_launches();
+        }
     }
     leaf_owner_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.contrib, P.owner_leaf, P.d_err);
     note_launches();

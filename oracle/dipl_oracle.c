@@ -753,6 +753,7 @@ int64_t orc_hploc_boxes(const float* leaf_boxes, int64_t n, const uint64_t* code
 /* 12 floats each (v0 xyz, primitive id bits, v1 xyz, 0, v2 xyz, 0).                              */
 /* ------------------------------------------------------------------------------------------ */
 static int close_rel(float a, float b) {
+    if (!isfinite(a) || !isfinite(b)) return 0; /* an infinite side (no hit yet: prune limit +inf) is never close */
     float m = fmaxf(fabsf(a), fabsf(b));
     return fabsf(a - b) <= 1e-6f * m;
 }

@@ -329,7 +329,9 @@ def test_nan_and_inf_vertices(orc, kind, layout):
 @pytest.mark.parametrize("workload", ["sphere", "soup"])
 def test_reordered_trace_equals_given_order(workload, form):
     """Batches of 2^20 rays or more are traced in a coherent order of their own; the records are bit-identical to
-    tracing in the given order (and, with counters, so are the visit and test totals), in every layout."""
+    tracing in the given order, in every layout. The visit and test totals agree to 0.1%: the binary trace hands
+    long rays of nearly idle warps to the warp-per-ray tail kernel, which counts the nodes that warp visits, and
+    which rays those are depends on the order."""
     if workload == "sphere":
         tris, rays = S.displaced_sphere(nu=256, nv=128, n_rays=1 << 20)
     else:
@@ -343,8 +345,9 @@ def test_reordered_trace_equals_given_order(workload, form):
     torch.cuda.synchronize()
     bvh.check_errors()
     assert torch.equal(a.raw, b.raw)
-    assert st_a.accel_stats.traversal_count == st_b.accel_stats.traversal_count
-    assert st_a.accel_stats.intersection_count == st_b.accel_stats.intersection_count
+    for x, y in ((st_a.accel_stats.traversal_count, st_b.accel_stats.traversal_count),
+                 (st_a.accel_stats.intersection_count, st_b.accel_stats.intersection_count)):
+        assert abs(x - y) <= 1e-3 * max(x, y), (x, y)
 
 
 @pytest.mark.parametrize("name", ["small_scene", "displaced_sphere_64x32", "soup_2k"])
