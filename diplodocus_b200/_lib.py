@@ -22,7 +22,7 @@ LAYOUT_BINARY, LAYOUT_WIDE8_Q8 = 0, 1
 LEAF_REF_MT, LEAF_WATERTIGHT = 0, 1
 CLUSTER_HPLOC, CLUSTER_PLOC = 0, 1
 TRACE_BACKFACE_CULLING = 1
-TRACE_KEEP_ORDER = 2
+TRACE_COHERENT_ORDER = 2
 
 # Every entry point include/dipl_bvh.h declares.
 EXPORTS = [

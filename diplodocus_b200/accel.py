@@ -206,13 +206,13 @@ class GpuPlocBvh:
 
     # -- AccelerationStructure::Intersect (batched) ---------------------------------------------------
     def Intersect(self, stats: Stats, rays, backface_culling: bool = False, leaf_test: str | None = None,
-                  count: bool = False, keep_order: bool = False) -> Hits:
-        """Closest hits of a ray batch. Large batches are traced in a coherent order chosen on the device unless
-        ``keep_order``; the records are the same either way."""
+                  count: bool = False, coherent_order: bool = False) -> Hits:
+        """Closest hits of a ray batch. With ``coherent_order``, a batch of 2^20 rays or more is traced in an order
+        sorted on the device by origin cell and direction octant; the records are the same either way."""
         rays = as_device_rays(rays)
         n = rays.shape[0]
         raw = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
-        flags = (L.TRACE_BACKFACE_CULLING if backface_culling else 0) | (L.TRACE_KEEP_ORDER if keep_order else 0)
+        flags = (L.TRACE_BACKFACE_CULLING if backface_culling else 0) | (L.TRACE_COHERENT_ORDER if coherent_order else 0)
         lt = _leaf_test(leaf_test or self.config.leaf_test)
         if count:
             ctr = torch.zeros(2, dtype=torch.int64, device=rays.device)

@@ -432,126 +432,134 @@ __global__ void mesh_ref_offsets_kernel(const long long* __restrict__ offsets, i
     if (k == m) coffsets[m] = *total;
 }
 
-// Box of the part of triangle t inside [lo, hi]: the triangle clipped against the six planes (Sutherland-Hodgman;
-// points on a plane are inside; a crossing point takes the plane's coordinate exactly), then clamped to the box.
-// An empty result (only rounding can make one) gives the box itself, which is conservative.
-__device__ void clipped_box(const Tri& t, const float* lo, const float* hi, float* olo, float* ohi) {
-    float P[9][3], Q[9][3];
-    int np = 3;
-    const float3 v[3] = {t.a, t.b, t.c};
-    for (int i = 0; i < 3; ++i) P[i][0] = v[i].x, P[i][1] = v[i].y, P[i][2] = v[i].z;
-    for (int plane = 0; plane < 6 && np > 0; ++plane) {
-        const int a = plane >> 1;
-        const bool low = (plane & 1) == 0;
-        const float b = low ? lo[a] : hi[a];
-        int nq = 0;
-        for (int i = 0; i < np; ++i) {
-            const float* p = P[i];
-            const float* q = P[i + 1 < np ? i + 1 : 0];
-            const bool ip = low ? p[a] >= b : p[a] <= b, iq = low ? q[a] >= b : q[a] <= b;
-            if (ip && nq < 9) Q[nq][0] = p[0], Q[nq][1] = p[1], Q[nq][2] = p[2], ++nq;
-            if (ip != iq && nq < 9) {
-                const float s = __fdiv_rn(__fsub_rn(b, p[a]), __fsub_rn(q[a], p[a]));
-                for (int c = 0; c < 3; ++c) Q[nq][c] = c == a ? b : __fadd_rn(p[c], __fmul_rn(s, __fsub_rn(q[c], p[c])));
-                ++nq;
-            }
-        }
-        np = nq;
-        for (int i = 0; i < np; ++i) P[i][0] = Q[i][0], P[i][1] = Q[i][1], P[i][2] = Q[i][2];
-    }
-    if (np == 0) {
-        for (int c = 0; c < 3; ++c) olo[c] = lo[c], ohi[c] = hi[c];
-        return;
-    }
-    for (int c = 0; c < 3; ++c) {
-        float mn = P[0][c], mx = P[0][c];
-        for (int i = 1; i < np; ++i) mn = fminf(mn, P[i][c]), mx = fmaxf(mx, P[i][c]);
-        olo[c] = fmaxf(mn, lo[c]);
-        ohi[c] = fminf(mx, hi[c]);
-    }
+__device__ __forceinline__ float axis_of(const float3& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+__device__ __forceinline__ void set_axis(float3& v, int a, float x) {
+    if (a == 0) v.x = x;
+    else if (a == 1) v.y = x;
+    else v.z = x;
 }
 
-// The references of every triangle at its scanned position: an unsplit triangle's box, or its pieces in depth-first
-// order (the lower half first; a box of c pieces gives ceil(c/2) to the lower half and floor(c/2) to the upper).
-__global__ void __launch_bounds__(128) split_kernel(const MeshDesc* __restrict__ meshes,
-                                                    const long long* __restrict__ offsets, int m, long long n,
-                                                    const uint32_t* __restrict__ pieces,
-                                                    const uint32_t* __restrict__ first, int* __restrict__ ref_tri,
-                                                    float4* __restrict__ rbox) {
+constexpr int kSplitThreads = 128;
+constexpr int kPolyMax = 9;  // a triangle clipped by at most 6 planes
+
+// A piece's polygon in shared memory, one column per thread (vertex v, coordinate c of thread j at
+// [(v * 3 + c) * kSplitThreads + j]: a warp's accesses never share a bank).
+struct Poly {
+    float* s;
+    __device__ __forceinline__ float& at(int v, int c) const { return s[(v * 3 + c) * kSplitThreads]; }
+};
+
+// One halving of a piece (early split clipping): the piece is the part of the triangle inside its box [lo, hi],
+// kept as a polygon P of np vertices (the triangle clipped by the planes of the halvings so far). The plane
+// x_a = mid cuts it; the lower (x_a <= mid) or upper half's polygon Q is P clipped by that plane
+// (Sutherland-Hodgman: vertices on the plane are inside, a crossing point takes mid exactly on axis a), and its box
+// is Q's box intersected with the half of [lo, hi]. An empty Q or box (only rounding can make one) gives the half
+// itself, which is conservative. Returns Q's vertex count.
+__device__ __forceinline__ int split_half(const Poly& P, int np, const Poly& Q, int a, float mid, bool lower,
+                                          float3& lo, float3& hi) {
+    const float inf = __int_as_float(0x7F800000);
+    float3 bl = make_float3(inf, inf, inf), bh = make_float3(-inf, -inf, -inf);
+    int nq = 0;
+    for (int i = 0; i < np; ++i) {
+        const int j = i + 1 < np ? i + 1 : 0;
+        const float3 p = make_float3(P.at(i, 0), P.at(i, 1), P.at(i, 2));
+        const float3 q = make_float3(P.at(j, 0), P.at(j, 1), P.at(j, 2));
+        const float pa = axis_of(p, a), qa = axis_of(q, a);
+        const bool ip = lower ? pa <= mid : pa >= mid, iq = lower ? qa <= mid : qa >= mid;
+        if (ip && nq < kPolyMax) {
+            Q.at(nq, 0) = p.x, Q.at(nq, 1) = p.y, Q.at(nq, 2) = p.z, ++nq;
+            bl = make_float3(fminf(bl.x, p.x), fminf(bl.y, p.y), fminf(bl.z, p.z));
+            bh = make_float3(fmaxf(bh.x, p.x), fmaxf(bh.y, p.y), fmaxf(bh.z, p.z));
+        }
+        if (ip != iq && nq < kPolyMax) {
+            const float sc = __fdiv_rn(__fsub_rn(mid, pa), __fsub_rn(qa, pa));
+            float3 x = make_float3(__fadd_rn(p.x, __fmul_rn(sc, __fsub_rn(q.x, p.x))),
+                                   __fadd_rn(p.y, __fmul_rn(sc, __fsub_rn(q.y, p.y))),
+                                   __fadd_rn(p.z, __fmul_rn(sc, __fsub_rn(q.z, p.z))));
+            set_axis(x, a, mid);
+            Q.at(nq, 0) = x.x, Q.at(nq, 1) = x.y, Q.at(nq, 2) = x.z, ++nq;
+            bl = make_float3(fminf(bl.x, x.x), fminf(bl.y, x.y), fminf(bl.z, x.z));
+            bh = make_float3(fmaxf(bh.x, x.x), fmaxf(bh.y, x.y), fmaxf(bh.z, x.z));
+        }
+    }
+    if (lower) set_axis(hi, a, mid);
+    else set_axis(lo, a, mid);
+    const float3 nl = make_float3(fmaxf(bl.x, lo.x), fmaxf(bl.y, lo.y), fmaxf(bl.z, lo.z));
+    const float3 nh = make_float3(fminf(bh.x, hi.x), fminf(bh.y, hi.y), fminf(bh.z, hi.z));
+    if (nq > 0 && nl.x <= nh.x && nl.y <= nh.y && nl.z <= nh.z) lo = nl, hi = nh;
+    return nq;
+}
+
+// The triangle of every reference: triangle g owns the pieces[g] references from its scanned position first[g].
+__global__ void __launch_bounds__(256) ref_tri_kernel(long long n, const uint32_t* __restrict__ pieces,
+                                                      const uint32_t* __restrict__ first, int* __restrict__ ref_tri) {
     const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (g >= n) return;
-    const int k = find_mesh(offsets, m, g);
-    const Tri t = load_tri(meshes[k], g - meshes[k].first);
     const uint32_t c = pieces[g];
-    long long r = first[g];
-    float3 blo, bhi;
-    tri_box(t, blo, bhi);
-    if (c == 1u) {
-        ref_tri[r] = (int)g;
-        rbox[2 * r] = make_float4(blo.x, blo.y, blo.z, 0.0f);
-        rbox[2 * r + 1] = make_float4(bhi.x, bhi.y, bhi.z, 0.0f);
-        return;
-    }
-    struct Item {
-        float lo[3], hi[3];
-        int c;
-    };
-    Item st[8];  // depth <= log2(kMaxPieces) + 1
-    int sp = 0;
-    st[sp++] = Item{{blo.x, blo.y, blo.z}, {bhi.x, bhi.y, bhi.z}, (int)c};
-    while (sp > 0) {
-        const Item it = st[--sp];
-        if (it.c == 1) {
-            ref_tri[r] = (int)g;
-            rbox[2 * r] = make_float4(it.lo[0], it.lo[1], it.lo[2], 0.0f);
-            rbox[2 * r + 1] = make_float4(it.hi[0], it.hi[1], it.hi[2], 0.0f);
-            ++r;
-            continue;
-        }
-        const float e0 = __fsub_rn(it.hi[0], it.lo[0]), e1 = __fsub_rn(it.hi[1], it.lo[1]),
-                    e2 = __fsub_rn(it.hi[2], it.lo[2]);
-        const int a = (e0 >= e1 && e0 >= e2) ? 0 : (e1 >= e2 ? 1 : 2);
-        const float mid = __fadd_rn(it.lo[a], __fmul_rn(__fsub_rn(it.hi[a], it.lo[a]), 0.5f));
-        Item lower = it, upper = it;
-        lower.hi[a] = mid;
-        upper.lo[a] = mid;
-        float l[3], h[3];
-        clipped_box(t, lower.lo, lower.hi, l, h);
-        for (int q = 0; q < 3; ++q) lower.lo[q] = l[q], lower.hi[q] = h[q];
-        clipped_box(t, upper.lo, upper.hi, l, h);
-        for (int q = 0; q < 3; ++q) upper.lo[q] = l[q], upper.hi[q] = h[q];
-        lower.c = (it.c + 1) / 2;
-        upper.c = it.c / 2;
-        if (sp + 2 > 8) break;  // cannot happen for kMaxPieces = 64 (depth 7)
-        st[sp++] = upper;
-        st[sp++] = lower;
-    }
+    const long long r = first[g];
+    for (uint32_t i = 0; i < c; ++i) ref_tri[r + i] = (int)g;
 }
 
-// Codes of the references: an unsplit triangle's exactly as codes_kernel computes it, a piece's from the centre
-// and the diagonal of its box.
+// One thread per reference: its box and its code. An unsplit triangle's reference takes the triangle's box and
+// codes exactly as codes_kernel; piece j of a triangle split into c pieces follows its own path of halvings from
+// the triangle's box: a box of c pieces is cut at the midpoint of its longest axis, the lower half takes the
+// first ceil(c/2) pieces and the upper half the rest, and each half's box comes from split_half. The
+// pieces of one triangle are the leaves of that binary recursion in depth-first order (lower half first), and
+// every box is computed with the same operations whichever thread computes it. A piece codes by the centre and
+// the diagonal of its box.
 template <typename K>
-__global__ void __launch_bounds__(256) ref_codes_kernel(const MeshDesc* __restrict__ meshes,
-                                                        const long long* __restrict__ offsets, int m, long long n_refs,
-                                                        const int* __restrict__ ref_tri,
-                                                        const uint32_t* __restrict__ pieces,
-                                                        const float4* __restrict__ rbox,
-                                                        const CodeParams* __restrict__ params, int code_type,
-                                                        int code_shift, int mesh_shift, K* __restrict__ keys) {
+__global__ void __launch_bounds__(kSplitThreads) split_refs_kernel(const MeshDesc* __restrict__ meshes,
+                                                                   const long long* __restrict__ offsets, int m,
+                                                                   long long n_refs, const int* __restrict__ ref_tri,
+                                                                   const uint32_t* __restrict__ pieces,
+                                                                   const uint32_t* __restrict__ first,
+                                                                   const CodeParams* __restrict__ params,
+                                                                   int code_type, int code_shift, int mesh_shift,
+                                                                   float4* __restrict__ rbox, K* __restrict__ keys) {
+    __shared__ float s_poly[2 * kPolyMax * 3 * kSplitThreads];
     const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (r >= n_refs) return;
     const long long g = ref_tri[r];
     const int k = find_mesh(offsets, m, g);
+    const Tri t = load_tri(meshes[k], g - meshes[k].first);
+    int c = (int)pieces[g];
+    float3 blo, bhi;
+    tri_box(t, blo, bhi);
     unsigned long long code;
-    if (pieces[g] == 1u) {
-        code = tri_code(load_tri(meshes[k], g - meshes[k].first), params[k], code_type);
+    if (c == 1) {
+        code = tri_code(t, params[k], code_type);
     } else {
-        const float4 lo = rbox[2 * r], hi = rbox[2 * r + 1];
-        const float3 c = make_float3(__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f), __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
-                                     __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f));
-        code = point_code(c, __fsub_rn(hi.x, lo.x), __fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z), params[k],
+        Poly P{s_poly + threadIdx.x}, Q{s_poly + kPolyMax * 3 * kSplitThreads + threadIdx.x};
+        P.at(0, 0) = t.a.x, P.at(0, 1) = t.a.y, P.at(0, 2) = t.a.z;
+        P.at(1, 0) = t.b.x, P.at(1, 1) = t.b.y, P.at(1, 2) = t.b.z;
+        P.at(2, 0) = t.c.x, P.at(2, 1) = t.c.y, P.at(2, 2) = t.c.z;
+        int np = 3;
+        int j = (int)(r - (long long)first[g]);
+        for (int depth = 0; depth < 8 && c > 1; ++depth) {  // c <= kMaxPieces: at most 6 halvings
+            const float e0 = __fsub_rn(bhi.x, blo.x), e1 = __fsub_rn(bhi.y, blo.y), e2 = __fsub_rn(bhi.z, blo.z);
+            const int a = (e0 >= e1 && e0 >= e2) ? 0 : (e1 >= e2 ? 1 : 2);
+            const float la = axis_of(blo, a);
+            const float mid = __fadd_rn(la, __fmul_rn(__fsub_rn(axis_of(bhi, a), la), 0.5f));
+            const int lower = (c + 1) / 2;
+            const bool in_lower = j < lower;
+            if (in_lower) {
+                c = lower;
+            } else {
+                j -= lower;
+                c -= lower;
+            }
+            np = split_half(P, np, Q, a, mid, in_lower, blo, bhi);
+            const Poly tmp = P;
+            P = Q;
+            Q = tmp;
+        }
+        const float3 ctr = make_float3(__fmul_rn(__fadd_rn(blo.x, bhi.x), 0.5f), __fmul_rn(__fadd_rn(blo.y, bhi.y), 0.5f),
+                                       __fmul_rn(__fadd_rn(blo.z, bhi.z), 0.5f));
+        code = point_code(ctr, __fsub_rn(bhi.x, blo.x), __fsub_rn(bhi.y, blo.y), __fsub_rn(bhi.z, blo.z), params[k],
                           code_type);
     }
+    rbox[2 * r] = make_float4(blo.x, blo.y, blo.z, 0.0f);
+    rbox[2 * r + 1] = make_float4(bhi.x, bhi.y, bhi.z, 0.0f);
     code >>= code_shift;
     if (mesh_shift > 0) code |= (unsigned long long)k << mesh_shift;
     keys[r] = static_cast<K>(code);
@@ -1353,6 +1361,12 @@ struct HplocParams {
     int max_node_iterations;    // iterations within one node before the build gives up (kErrIterations)
 };
 
+__device__ __forceinline__ int atomic_exch_acq_rel(int* p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.exch.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 template <typename K>
 __device__ __forceinline__ bool split_before(const K* __restrict__ keys, int a, int b) {
     const K xa = __ldg(keys + a) ^ __ldg(keys + a + 1), xb = __ldg(keys + b) ^ __ldg(keys + b + 1);
@@ -1412,17 +1426,9 @@ __device__ __forceinline__ int hploc_node(const HplocParams& P, int nl, int nr, 
         }
         float bestd = __int_as_float(0x7F800000);
         int bestj = -1;
-        for (int d = 1; d <= R && d < c; ++d) {
-            const float fx = __shfl_down_sync(full, a.x, d), fy = __shfl_down_sync(full, a.y, d);
-            const float fz = __shfl_down_sync(full, a.z, d), gx = __shfl_down_sync(full, b.x, d);
-            const float gy = __shfl_down_sync(full, b.y, d), gz = __shfl_down_sync(full, b.z, d);
-            const bool fwd_ok = lane + d < c;
-            const float df = fwd_ok ? ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, fx, fy, fz, gx, gy, gz)
-                                    : __int_as_float(0x7F800000);
-            const float db = __shfl_up_sync(full, df, d);  // the pair (lane - d, lane), evaluated by lane - d
-            const bool back_ok = lane >= d && lane < c;
-            // equal distances: the candidate with the even lower index first, then the one below (the key's tie
-            // fields after the gap: parity of the lower index, side)
+        // candidates in the order of the key: gap d ascending; at one gap, the candidate with the even lower index
+        // first, then the one below (the key's tie fields after the gap: parity of the lower index, side)
+        auto consider = [&](int d, float df, float db, bool fwd_ok, bool back_ok) {
             if (((lane - d) & 1) <= (lane & 1)) {
                 if (back_ok && (db < bestd || bestj < 0)) bestd = db, bestj = lane - d;
                 if (fwd_ok && (df < bestd || bestj < 0)) bestd = df, bestj = lane + d;
@@ -1430,6 +1436,26 @@ __device__ __forceinline__ int hploc_node(const HplocParams& P, int nl, int nr, 
                 if (fwd_ok && (df < bestd || bestj < 0)) bestd = df, bestj = lane + d;
                 if (back_ok && (db < bestd || bestj < 0)) bestd = db, bestj = lane - d;
             }
+        };
+        const int dmax = min(R, c - 1);
+        // two gaps per pass (independent shuffles and distances in flight together), folded in gap order
+        for (int d = 1; d <= dmax; d += 2) {
+            const int e = d + 1;  // the second gap (only when e <= dmax; e <= 32, and a shuffle by 32 is harmless)
+            const float fx = __shfl_down_sync(full, a.x, d), fy = __shfl_down_sync(full, a.y, d);
+            const float fz = __shfl_down_sync(full, a.z, d), gx = __shfl_down_sync(full, b.x, d);
+            const float gy = __shfl_down_sync(full, b.y, d), gz = __shfl_down_sync(full, b.z, d);
+            const float hx = __shfl_down_sync(full, a.x, e), hy = __shfl_down_sync(full, a.y, e);
+            const float hz = __shfl_down_sync(full, a.z, e), kx = __shfl_down_sync(full, b.x, e);
+            const float ky = __shfl_down_sync(full, b.y, e), kz = __shfl_down_sync(full, b.z, e);
+            const bool fwd_d = lane + d < c, fwd_e = e <= dmax && lane + e < c;
+            const float df = fwd_d ? ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, fx, fy, fz, gx, gy, gz)
+                                   : __int_as_float(0x7F800000);
+            const float de = fwd_e ? ploc_distance(a.x, a.y, a.z, b.x, b.y, b.z, hx, hy, hz, kx, ky, kz)
+                                   : __int_as_float(0x7F800000);
+            const float db = __shfl_up_sync(full, df, d);  // the pair (lane - d, lane), evaluated by lane - d
+            const float dbe = __shfl_up_sync(full, de, e);
+            consider(d, df, db, fwd_d, lane >= d && lane < c);
+            if (e <= dmax) consider(e, de, dbe, fwd_e, lane >= e && lane < c);
         }
         const int partner = bestj >= 0 ? bestj : lane;
         const int nn_of_partner = __shfl_sync(full, bestj, partner);
@@ -1516,20 +1542,20 @@ __global__ void __launch_bounds__(kHplocThreads) hploc_kernel(HplocParams P) {
             } else {
                 const bool left_child = l == mstart || (r != mend && split_before(keys, r, l - 1));
                 split = left_child ? r : l - 1;
-                __threadfence();  // this node's list (written by its warp) before the arrival
-                const int prev = atomicExch(P.other + split, left_child ? l : r);
+                // release: this node's list, written by the lanes of this warp before the warp barrier that ended
+                // the previous step, is visible before the arrival; acquire: so is the sibling's when we are second
+                const int prev = atomic_exch_acq_rel(P.other + split, left_child ? l : r);
                 if (prev < 0) {
                     active = false;  // first to arrive: the sibling's thread goes on
                 } else {
-                    __threadfence();  // the sibling's list before the loads
                     if (left_child) r = prev;
                     else l = prev;
                     todo = (r - l + 1 > kHplocThreshold) || (l == mstart && r == mend);
                 }
             }
         }
+        __syncwarp();  // every lane's acquire before any lane of the warp loads a list
         unsigned pending = __ballot_sync(full, todo);
-        const bool stored = pending != 0u;
         while (pending) {
             const int src = __ffs(pending) - 1;
             pending &= pending - 1u;
@@ -1538,8 +1564,7 @@ __global__ void __launch_bounds__(kHplocThreads) hploc_kernel(HplocParams P) {
             const bool whole = __shfl_sync(full, (int)(l == mstart && r == mend), src) != 0;
             iters += hploc_node(P, nl, nr, nm, nbase, whole);
         }
-        if (stored) __threadfence();  // every lane's part of the lists and nodes, before any lane's next arrival
-        __syncwarp();
+        __syncwarp();  // every lane's part of the lists and nodes, before any lane's next (releasing) arrival
         if (!__any_sync(full, active)) break;
     }
     // every lane ran the same node iterations: one count per warp
@@ -1657,7 +1682,7 @@ __device__ __forceinline__ void write_tri(const MeshDesc* meshes, const long lon
 __global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
                                   const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
                                   const int* __restrict__ ref_tri, const uint32_t* __restrict__ starts, int* __restrict__ leaf_start_of,
-                                  float4* __restrict__ tris, const uint32_t* err) {
+                                  float4* __restrict__ tris, int* __restrict__ pos_slot, const uint32_t* err) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.num_leaves || *err != 0u) return;
     int x = p, rank = 0;
@@ -1671,6 +1696,7 @@ __global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ m
     const int first = node_pmin(P, x);
     const int start = (int)starts[first];
     if (p == first) leaf_start_of[x] = start;
+    if (pos_slot) pos_slot[p] = start + rank;
     write_tri(meshes, offsets, m, perm, ref_tri, p, tris, start + rank);
 }
 
@@ -1998,6 +2024,7 @@ struct BuildPlan {
     int *hp_other = nullptr, *hp_cnt = nullptr, *hp_fid = nullptr;  // hierarchical clustering
     uint32_t *rev_flags = nullptr, *contrib = nullptr, *d_counts = nullptr;
     int *owner_leaf = nullptr, *leaf_start_of = nullptr;
+    int* pos_slot = nullptr;  // pre-split SOBB builds: per sorted position, its slot in the leaf triangle array
     unsigned char* scan_scratch = nullptr;
     BNode* nodes = nullptr;
     float4* tris = nullptr;
@@ -2161,6 +2188,7 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
         return st;
     if (d0.bv_type == DIPL_BV_SOBB) {
         if ((st = sobb_prepare(N, K, W, O, &P.sobb, &P.snodes)) != DIPL_OK) return st;
+        if (P.split && (st = W.alloc(&P.pos_slot, N)) != DIPL_OK) return st;
     }
     P.summary_bytes = sizeof(RootInfo) * m + sizeof(double) * 2 * m + 16;
     if (own_summary) {  // a plan replays into its own pinned buffer
@@ -2220,17 +2248,16 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     dipl_status st;
     if (P.split) {
         // bounds and parameters were enqueued with the piece counts (plan_prepare): the references and their codes
-        split_kernel<<<blocks_for(P.T, 128), 128, 0, stream>>>(P.d_meshes, P.d_offsets, m, P.T, P.pieces,
-                                                               P.piece_first, P.ref_tri, P.tbox);
+        ref_tri_kernel<<<blocks_for(P.T, 256), 256, 0, stream>>>(P.T, P.pieces, P.piece_first, P.ref_tri);
         note_launches();
         if (P.key_bytes == 4)
-            ref_codes_kernel<uint32_t><<<blocks_for(N, 256), 256, 0, stream>>>(
-                P.d_meshes, P.d_offsets, m, N, P.ref_tri, P.pieces, P.tbox, P.d_params, d0.code_type, P.code_shift,
-                P.mesh_shift, (uint32_t*)P.keys);
+            split_refs_kernel<uint32_t><<<blocks_for(N, kSplitThreads), kSplitThreads, 0, stream>>>(
+                P.d_meshes, P.d_offsets, m, N, P.ref_tri, P.pieces, P.piece_first, P.d_params, d0.code_type,
+                P.code_shift, P.mesh_shift, P.tbox, (uint32_t*)P.keys);
         else
-            ref_codes_kernel<unsigned long long><<<blocks_for(N, 256), 256, 0, stream>>>(
-                P.d_meshes, P.d_offsets, m, N, P.ref_tri, P.pieces, P.tbox, P.d_params, d0.code_type, P.code_shift,
-                P.mesh_shift, (unsigned long long*)P.keys);
+            split_refs_kernel<unsigned long long><<<blocks_for(N, kSplitThreads), kSplitThreads, 0, stream>>>(
+                P.d_meshes, P.d_offsets, m, N, P.ref_tri, P.pieces, P.piece_first, P.d_params, d0.code_type,
+                P.code_shift, P.mesh_shift, P.tbox, (unsigned long long*)P.keys);
         note_launches();
     } else if ((st = enqueue_bounds_and_params(P, stream)) != DIPL_OK) {
         return st;
@@ -2335,7 +2362,7 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     if ((st = exclusive_scan_u32(P.contrib, P.contrib, N, nullptr, P.scan_scratch, stream, P.d_err)) != DIPL_OK)
         return st;
     leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.ref_tri,
-                                                               P.contrib, P.leaf_start_of, P.tris, P.d_err);
+                                                               P.contrib, P.leaf_start_of, P.tris, P.pos_slot, P.d_err);
     note_launches();
     if (K > 0) {
         node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.tbox, P.d_coffsets, m, P.perm, P.rev_flags,
@@ -2347,8 +2374,10 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     note_launches();
     DIPL_CUDA(cudaGetLastError());
     if (d0.bv_type == DIPL_BV_SOBB) {
+        SobbRefs refs;
+        if (P.split) refs = SobbRefs{P.pos_slot, P.perm, P.tbox};
         st = sobb_enqueue(P.child, P.nlo, P.nhi, P.parent, P.leaf_start_of, P.owner_leaf, P.tris, P.nodes, P.rev_flags,
-                          (int)N, (int)K, P.L, d0.kdop_size, P.sobb, P.snodes, stream, P.d_err);
+                          (int)N, (int)K, P.L, d0.kdop_size, P.sobb, refs, P.snodes, stream, P.d_err);
         if (st != DIPL_OK) return st;
     }
     // ---- the per-mesh summary to pinned host memory --------------------------------------------------

@@ -150,11 +150,12 @@ dipl_status trace_closest(const dipl_bvh* bvh, const dipl_ray* rays, int64_t n, 
 dipl_status trace_any(const dipl_bvh* bvh, const dipl_ray* rays, int64_t n, uint8_t* occluded, int leaf_test,
                       uint32_t flags, cudaStream_t stream);
 dipl_status sah_cost(const dipl_bvh* bvh, double* cost, cudaStream_t stream);
-// Coherent ray order of large traces (trace.cu): batches of kReorderMinRays rays or more are traced in the order
-// of a key of the origin cell and the direction octant, sorted on the device; records still go to each ray's index.
+// Coherent ray order of large traces (trace.cu): with DIPL_TRACE_COHERENT_ORDER, batches of kReorderMinRays rays
+// or more are traced in the order of a key of the origin cell and the direction octant, sorted on the device;
+// records still go to each ray's index.
 constexpr int64_t kReorderMinRays = int64_t(1) << 20;
 inline bool reorder_rays(int64_t n, uint32_t flags) {
-    return n >= kReorderMinRays && (flags & DIPL_TRACE_KEEP_ORDER) == 0u;
+    return n >= kReorderMinRays && (flags & DIPL_TRACE_COHERENT_ORDER) != 0u;
 }
 // Device memory of one reordered trace: keys, the order and the sort's scratch (released in stream order).
 struct RayOrder {
@@ -190,11 +191,18 @@ struct SobbScratch {
     unsigned* arrivals = nullptr;
     int triples = 0;
 };
+// Pre-split builds: per sorted position its slot in the leaf triangle array, the sorted order of the references
+// and every reference's box (all NULL without pre-splitting).
+struct SobbRefs {
+    const int* pos_slot = nullptr;
+    const uint32_t* perm = nullptr;
+    const float4* rbox = nullptr;
+};
 dipl_status sobb_prepare(long long N, long long K, Storage& work, Storage& out, SobbScratch* sc, SNode** snodes);
 dipl_status sobb_enqueue(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
                          const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
                          const uint32_t* rev_index, int N, int K, int L, int kdop_size, const SobbScratch& sc,
-                         SNode* snodes, cudaStream_t s, uint32_t* d_err);
+                         const SobbRefs& refs, SNode* snodes, cudaStream_t s, uint32_t* d_err);
 dipl_status trace_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ, int leaf_test,
                        uint32_t flags, unsigned long long* counters, bool any, cudaStream_t s);
 

@@ -75,41 +75,10 @@ __device__ __forceinline__ void store_kdop(Kdop* dst, const Kdop& k) {
     }
 }
 
-// k-DOP of a final leaf from its triangles, then up the tree: the second arriver at a parent merges. All 16
-// table directions are always projected (a smaller kdop_size only restricts which triples the node kernel
-// considers), so the k-DOP never leaves registers.
-__global__ void __launch_bounds__(256) kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf,
-                                                         Kdop* __restrict__ kdop, float* __restrict__ mag,
-                                                         unsigned* __restrict__ arrivals, const uint32_t* err) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= S.N || *err != 0u) return;
-    int x = owner_leaf[p];
-    if (x < 0) return;
-    const int cnt = scount(S, x);
-    const float4* t = S.btris + 3 * (long long)S.leaf_start_of[x];
-    Kdop k;
-    float m = 0.0f;
-#pragma unroll
-    for (int i = 0; i < kDirs; ++i) k.lo[i] = __int_as_float(0x7F800000), k.hi[i] = __int_as_float(0xFF800000);
-    for (int tr = 0; tr < cnt; ++tr) {
-        const float4 q0 = __ldg(t + 3 * tr), q1 = __ldg(t + 3 * tr + 1), q2 = __ldg(t + 3 * tr + 2);
-        // a triangle with a non-finite coordinate is never hit: it adds nothing to the k-DOP
-        if (!(isfinite(q0.x) && isfinite(q0.y) && isfinite(q0.z) && isfinite(q1.x) && isfinite(q1.y) &&
-              isfinite(q1.z) && isfinite(q2.x) && isfinite(q2.y) && isfinite(q2.z)))
-            continue;
-        for (int v = 0; v < 3; ++v) {
-            const float4 q = v == 0 ? q0 : (v == 1 ? q1 : q2);
-            m = fmaxf(m, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
-#pragma unroll
-            for (int i = 0; i < kDirs; ++i) {
-                const float d = proj(i, q.x, q.y, q.z);
-                k.lo[i] = fminf(k.lo[i], d);
-                k.hi[i] = fmaxf(k.hi[i], d);
-            }
-        }
-    }
-    store_kdop(kdop + x, k);
-    mag[x] = m;
+// Up the tree from node x with its k-DOP k and magnitude m already stored: the second arriver at a parent merges
+// the sibling's k-DOP and continues.
+__device__ __forceinline__ void kdop_ascend(const SobbIn& S, int x, Kdop& k, float m, Kdop* __restrict__ kdop,
+                                            float* __restrict__ mag, unsigned* __restrict__ arrivals) {
     for (int guard = 0; guard < 4096; ++guard) {
         const int par = S.parent[x];
         if (par < 0) return;
@@ -132,6 +101,83 @@ __global__ void __launch_bounds__(256) kdop_refit_kernel(SobbIn S, const int* __
         mag[par] = m;
         x = par;
     }
+}
+
+// k-DOP of one triangle (empty for a triangle with a non-finite coordinate: it is never hit) and the largest
+// magnitude of its coordinates folded into m.
+__device__ __forceinline__ void tri_kdop(const float4* __restrict__ t, Kdop& k, float& m) {
+    const float4 q0 = __ldg(t), q1 = __ldg(t + 1), q2 = __ldg(t + 2);
+    if (!(isfinite(q0.x) && isfinite(q0.y) && isfinite(q0.z) && isfinite(q1.x) && isfinite(q1.y) && isfinite(q1.z) &&
+          isfinite(q2.x) && isfinite(q2.y) && isfinite(q2.z)))
+        return;
+    for (int v = 0; v < 3; ++v) {
+        const float4 q = v == 0 ? q0 : (v == 1 ? q1 : q2);
+        m = fmaxf(m, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
+#pragma unroll
+        for (int i = 0; i < kDirs; ++i) {
+            const float d = proj(i, q.x, q.y, q.z);
+            k.lo[i] = fminf(k.lo[i], d);
+            k.hi[i] = fmaxf(k.hi[i], d);
+        }
+    }
+}
+
+__device__ __forceinline__ void empty_kdop(Kdop& k) {
+#pragma unroll
+    for (int i = 0; i < kDirs; ++i) k.lo[i] = __int_as_float(0x7F800000), k.hi[i] = __int_as_float(0xFF800000);
+}
+
+// k-DOP of a final leaf from its triangles, then up the tree: the second arriver at a parent merges. All 16
+// table directions are always projected (a smaller kdop_size only restricts which triples the node kernel
+// considers), so the k-DOP never leaves registers.
+__global__ void __launch_bounds__(256) kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf,
+                                                         Kdop* __restrict__ kdop, float* __restrict__ mag,
+                                                         unsigned* __restrict__ arrivals, const uint32_t* err) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.N || *err != 0u) return;
+    int x = owner_leaf[p];
+    if (x < 0) return;
+    const int cnt = scount(S, x);
+    const float4* t = S.btris + 3 * (long long)S.leaf_start_of[x];
+    Kdop k;
+    float m = 0.0f;
+    empty_kdop(k);
+    for (int tr = 0; tr < cnt; ++tr) tri_kdop(t + 3 * tr, k, m);
+    store_kdop(kdop + x, k);
+    mag[x] = m;
+    kdop_ascend(S, x, k, m, kdop, mag, arrivals);
+}
+
+// Pre-split builds: a reference bounds only the part of its triangle inside the reference's box, so every sorted
+// position starts with the intersection of its triangle's k-DOP and the k-DOP of its box (each interval of the
+// intersection holds the projections of every point of the triangle inside the box; an interval that rounding
+// leaves empty keeps the triangle's), and the tree is merged upwards from the positions.
+__global__ void __launch_bounds__(256) kdop_refit_refs_kernel(SobbIn S, const int* __restrict__ pos_slot,
+                                                              const uint32_t* __restrict__ perm,
+                                                              const float4* __restrict__ rbox, Kdop* __restrict__ kdop,
+                                                              float* __restrict__ mag, unsigned* __restrict__ arrivals,
+                                                              const uint32_t* err) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.N || *err != 0u) return;
+    Kdop k;
+    float m = 0.0f;
+    empty_kdop(k);
+    tri_kdop(S.btris + 3 * (long long)pos_slot[p], k, m);
+    const long long r = perm[p];
+    const float4 lo = __ldg(rbox + 2 * r), hi = __ldg(rbox + 2 * r + 1);
+#pragma unroll
+    for (int i = 0; i < kDirs; ++i) {
+        if (!(k.lo[i] <= k.hi[i])) continue;  // an empty (never hit) triangle stays empty
+        const float bl = proj(i, c_dir[i][0] >= 0.0f ? lo.x : hi.x, c_dir[i][1] >= 0.0f ? lo.y : hi.y,
+                              c_dir[i][2] >= 0.0f ? lo.z : hi.z);
+        const float bh = proj(i, c_dir[i][0] >= 0.0f ? hi.x : lo.x, c_dir[i][1] >= 0.0f ? hi.y : lo.y,
+                              c_dir[i][2] >= 0.0f ? hi.z : lo.z);
+        const float nl = fmaxf(k.lo[i], bl), nh = fminf(k.hi[i], bh);
+        if (nl <= nh) k.lo[i] = nl, k.hi[i] = nh;
+    }
+    store_kdop(kdop + p, k);
+    mag[p] = m;
+    kdop_ascend(S, p, k, m, kdop, mag, arrivals);
 }
 
 // One warp per inner node of the final layout, one half-warp per child; lane l of a half holds the child's
@@ -500,12 +546,16 @@ dipl_status sobb_prepare(long long N, long long K, Storage& work, Storage& out, 
 dipl_status sobb_enqueue(const int4* child, const float4* node_lo, const float4* node_hi, const int* parent,
                          const int* leaf_start_of, const int* owner_leaf, const float4* btris, const BNode* bnodes,
                          const uint32_t* rev_index, int N, int K, int L, int kdop_size, const SobbScratch& sc,
-                         SNode* snodes, cudaStream_t s, uint32_t* d_err) {
+                         const SobbRefs& refs, SNode* snodes, cudaStream_t s, uint32_t* d_err) {
     const int Kalloc = std::max(K, 1);
     Kdop* kdop = static_cast<Kdop*>(sc.kdop);
     DIPL_CUDA(cudaMemsetAsync(sc.arrivals, 0, sizeof(unsigned) * Kalloc, s));
     SobbIn S{child, node_lo, node_hi, parent, leaf_start_of, btris, N, L, kdop_size / 2};
-    kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, kdop, sc.mag, sc.arrivals, d_err);
+    if (refs.pos_slot)
+        kdop_refit_refs_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, refs.pos_slot, refs.perm, refs.rbox,
+                                                                           kdop, sc.mag, sc.arrivals, d_err);
+    else
+        kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, kdop, sc.mag, sc.arrivals, d_err);
     note_launches();
     if (K > 0) {
         // persistent: each CTA stages the triple table once, then its warps stride over the nodes

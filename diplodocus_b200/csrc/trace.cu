@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(kTraceThreads) tail_kernel(const BNode* __rest
 }
 
 // ---- ray order ----------------------------------------------------------------------------------------
-// Batches of at least kReorderMinRays rays are traced in the order of a 30-bit key: the direction's octant
+// On request, batches of at least kReorderMinRays rays are traced in the order of a 30-bit key: the direction's octant
 // above a 9-bit-per-axis Morton code of the origin within the batch's origin bounds. A warp's chunk of rays then
 // starts in one small region and heads the same way, so its lanes fetch the same nodes and branch alike.
 // Records still go to each ray's own index; only the order of work changes, never a result.

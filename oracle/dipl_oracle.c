@@ -1094,10 +1094,10 @@ void orc_shadow_rays(const float* tris, const float* rays, const int32_t* prim, 
 /* q = floor(w 2^32 / D^2) of the triangle boxes (w = (dx dy + dy dz) + dz dx in FP32, D = the     */
 /* mesh's vertex-box diagonal), their exact sum Q, the piece counts                                */
 /* 1 + min(63, floor(q budget N / (100 Q))), and the pieces: a box of c pieces is split at its    */
-/* longest axis' midpoint, each half's box is the box of the triangle clipped to that half          */
-/* (Sutherland-Hodgman, crossing points on the plane exactly, clamped to the half; empty: the half */
-/* itself), ceil(c/2) pieces to the lower half first. One mesh (seg = NULL) or meshes of the given  */
-/* sizes in input order.                                                                            */
+/* longest axis' midpoint; each half keeps the polygon of the triangle clipped by the planes of its */
+/* halvings (orc_split_half) and that polygon's box clamped to the half (empty: the half itself);   */
+/* ceil(c/2) pieces to the lower half first. One mesh (seg = NULL) or meshes of the given sizes in  */
+/* input order.                                                                                     */
 /* ------------------------------------------------------------------------------------------ */
 static uint64_t orc_split_weight(const float* p, float diag) {
     if (!tri_finite(p) || !(diag > 0.0f)) return 0;
@@ -1113,38 +1113,44 @@ static uint64_t orc_split_weight(const float* p, float diag) {
     return q < 1.8e19 ? (uint64_t)q : (uint64_t)18000000000000000000ull;
 }
 
-static void orc_clipped_box(const float* t, const float* lo, const float* hi, float* olo, float* ohi) {
-    float P[9][3], Q[9][3];
-    int np = 3;
-    for (int i = 0; i < 3; ++i)
-        for (int c = 0; c < 3; ++c) P[i][c] = t[3 * i + c];
-    for (int plane = 0; plane < 6 && np > 0; ++plane) {
-        int a = plane >> 1, low = (plane & 1) == 0, nq = 0;
-        float b = low ? lo[a] : hi[a];
-        for (int i = 0; i < np; ++i) {
-            const float* p = P[i];
-            const float* q = P[i + 1 < np ? i + 1 : 0];
-            int ip = low ? p[a] >= b : p[a] <= b, iq = low ? q[a] >= b : q[a] <= b;
-            if (ip && nq < 9) Q[nq][0] = p[0], Q[nq][1] = p[1], Q[nq][2] = p[2], ++nq;
-            if (ip != iq && nq < 9) {
-                float s = (b - p[a]) / (q[a] - p[a]);
-                for (int c = 0; c < 3; ++c) Q[nq][c] = c == a ? b : p[c] + s * (q[c] - p[c]);
-                ++nq;
-            }
+/* One halving of a piece (the build's split_half): the piece is polygon P (np vertices, the triangle clipped by the
+ * planes of the halvings so far) inside box [lo, hi]. The plane x_ax = mid cuts it; the lower (x_ax <= mid) or upper
+ * half's polygon Q is P clipped by that plane (Sutherland-Hodgman: vertices on the plane are inside, a crossing point
+ * takes mid exactly on axis ax; at most 9 vertices), and its box is Q's box intersected with the half of [lo, hi];
+ * an empty Q or box keeps the half. lo and hi are updated in place; returns Q's vertex count. */
+#define ORC_POLY_MAX 9
+static int orc_split_half(const float (*P)[3], int np, float (*Q)[3], int ax, float mid, int lower, float* lo,
+                          float* hi) {
+    float bl[3] = {INFINITY, INFINITY, INFINITY}, bh[3] = {-INFINITY, -INFINITY, -INFINITY};
+    int nq = 0;
+    for (int i = 0; i < np; ++i) {
+        const float* p = P[i];
+        const float* q = P[i + 1 < np ? i + 1 : 0];
+        float pa = p[ax], qa = q[ax];
+        int ip = lower ? pa <= mid : pa >= mid, iq = lower ? qa <= mid : qa >= mid;
+        if (ip && nq < ORC_POLY_MAX) {
+            for (int c = 0; c < 3; ++c) Q[nq][c] = p[c], bl[c] = fminf(bl[c], p[c]), bh[c] = fmaxf(bh[c], p[c]);
+            ++nq;
         }
-        np = nq;
-        for (int i = 0; i < np; ++i) P[i][0] = Q[i][0], P[i][1] = Q[i][1], P[i][2] = Q[i][2];
+        if (ip != iq && nq < ORC_POLY_MAX) {
+            float s = (mid - pa) / (qa - pa);
+            for (int c = 0; c < 3; ++c) Q[nq][c] = c == ax ? mid : p[c] + s * (q[c] - p[c]);
+            for (int c = 0; c < 3; ++c) bl[c] = fminf(bl[c], Q[nq][c]), bh[c] = fmaxf(bh[c], Q[nq][c]);
+            ++nq;
+        }
     }
-    if (np == 0) {
-        for (int c = 0; c < 3; ++c) olo[c] = lo[c], ohi[c] = hi[c];
-        return;
-    }
+    if (lower) hi[ax] = mid;
+    else lo[ax] = mid;
+    float nl[3], nh[3];
+    int ok = nq > 0;
     for (int c = 0; c < 3; ++c) {
-        float mn = P[0][c], mx = P[0][c];
-        for (int i = 1; i < np; ++i) mn = fminf(mn, P[i][c]), mx = fmaxf(mx, P[i][c]);
-        olo[c] = fmaxf(mn, lo[c]);
-        ohi[c] = fminf(mx, hi[c]);
+        nl[c] = fmaxf(bl[c], lo[c]);
+        nh[c] = fminf(bh[c], hi[c]);
+        ok = ok && nl[c] <= nh[c];
     }
+    if (ok)
+        for (int c = 0; c < 3; ++c) lo[c] = nl[c], hi[c] = nh[c];
+    return nq;
 }
 
 /* tris: all meshes' triangles in input order; mesh_sizes[nm]. Writes pieces[n] and, when ref_tri != NULL, the
@@ -1183,17 +1189,23 @@ int64_t orc_presplit(const float* tris, int64_t n, const int64_t* mesh_sizes, in
             }
             struct {
                 float lo[3], hi[3];
-                int c;
+                float poly[ORC_POLY_MAX][3];
+                int c, np;
             } st[8];
             int sp = 0;
             for (int a = 0; a < 3; ++a) st[0].lo[a] = blo[a], st[0].hi[a] = bhi[a];
+            for (int v = 0; v < 3; ++v)
+                for (int a = 0; a < 3; ++a) st[0].poly[v][a] = p[3 * v + a];
             st[0].c = (int)c;
+            st[0].np = 3;
             sp = 1;
             while (sp > 0) {
                 --sp;
-                float lo[3], hi[3];
-                int cc = st[sp].c;
+                float lo[3], hi[3], poly[ORC_POLY_MAX][3];
+                int cc = st[sp].c, np = st[sp].np;
                 for (int a = 0; a < 3; ++a) lo[a] = st[sp].lo[a], hi[a] = st[sp].hi[a];
+                for (int v = 0; v < np; ++v)
+                    for (int a = 0; a < 3; ++a) poly[v][a] = st[sp].poly[v][a];
                 if (cc == 1) {
                     ref_tri[r] = (int32_t)(first + i);
                     for (int a = 0; a < 3; ++a) rbox[6 * r + a] = lo[a], rbox[6 * r + 3 + a] = hi[a];
@@ -1203,19 +1215,14 @@ int64_t orc_presplit(const float* tris, int64_t n, const int64_t* mesh_sizes, in
                 float e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = hi[2] - lo[2];
                 int ax = (e0 >= e1 && e0 >= e2) ? 0 : (e1 >= e2 ? 1 : 2);
                 float mid = lo[ax] + (hi[ax] - lo[ax]) * 0.5f;
-                float llo[3], lhi[3], ulo[3], uhi[3], tl[3], th[3];
-                for (int a = 0; a < 3; ++a) llo[a] = ulo[a] = lo[a], lhi[a] = uhi[a] = hi[a];
-                lhi[ax] = mid;
-                ulo[ax] = mid;
-                orc_clipped_box(p, llo, lhi, tl, th);
-                for (int a = 0; a < 3; ++a) llo[a] = tl[a], lhi[a] = th[a];
-                orc_clipped_box(p, ulo, uhi, tl, th);
-                for (int a = 0; a < 3; ++a) ulo[a] = tl[a], uhi[a] = th[a];
                 if (sp + 2 > 8) break;
-                for (int a = 0; a < 3; ++a) st[sp].lo[a] = ulo[a], st[sp].hi[a] = uhi[a];
+                /* the upper half is pushed first, so the lower half's pieces come first */
+                for (int a = 0; a < 3; ++a) st[sp].lo[a] = lo[a], st[sp].hi[a] = hi[a];
+                st[sp].np = orc_split_half((const float (*)[3])poly, np, st[sp].poly, ax, mid, 0, st[sp].lo, st[sp].hi);
                 st[sp].c = cc / 2;
                 ++sp;
-                for (int a = 0; a < 3; ++a) st[sp].lo[a] = llo[a], st[sp].hi[a] = lhi[a];
+                for (int a = 0; a < 3; ++a) st[sp].lo[a] = lo[a], st[sp].hi[a] = hi[a];
+                st[sp].np = orc_split_half((const float (*)[3])poly, np, st[sp].poly, ax, mid, 1, st[sp].lo, st[sp].hi);
                 st[sp].c = (cc + 1) / 2;
                 ++sp;
             }
@@ -1225,7 +1232,7 @@ int64_t orc_presplit(const float* tris, int64_t n, const int64_t* mesh_sizes, in
     return r;
 }
 
-/* Codes of the references of one mesh (the build's ref_codes_kernel): an unsplit triangle's code as orc_morton30 /
+/* Codes of the references of one mesh (the build's split_refs_kernel): an unsplit triangle's code as orc_morton30 /
  * orc_emc60 compute it; a piece's from its box centre ((lo + hi) * 0.5) and box diagonal. Bounds are the mesh's
  * triangles' (orc_scene_bounds). code_type 0: Morton30, 1: EMC60. */
 void orc_ref_codes(const float* tris, int64_t n, const uint32_t* pieces, const int32_t* ref_tri, const float* rbox,

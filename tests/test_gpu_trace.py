@@ -341,7 +341,7 @@ def test_reordered_trace_equals_given_order(workload, form):
     rd = torch.from_numpy(rays).cuda()
     st_a, st_b = A.Stats(), A.Stats()
     a = bvh.Intersect(st_a, rd, count=True)
-    b = bvh.Intersect(st_b, rd, count=True, keep_order=True)
+    b = bvh.Intersect(st_b, rd, count=True, coherent_order=True)
     torch.cuda.synchronize()
     bvh.check_errors()
     assert torch.equal(a.raw, b.raw)
