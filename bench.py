@@ -146,6 +146,14 @@ DEFAULT_CODE = {"soup16m": "emc60", "displaced_sphere": "morton30"}
 # Pre-splitting of large triangles (percent more clustering leaves at most): the soup's log-normal tail of large
 # triangles overlaps everywhere; the sphere's triangles are all alike (nothing would split).
 DEFAULT_SPLIT = {"soup16m": 40, "displaced_sphere": 0}
+# Ray order of the traces: the pre-split soup's random rays trace faster sorted by origin cell and direction octant
+# (DIPL_TRACE_COHERENT_ORDER); the sphere's camera-like rays are faster as given (the sort costs more than it saves).
+DEFAULT_ORDER = {"soup16m": "coherent", "displaced_sphere": "given"}
+
+
+def trace_flags(args):
+    order = args.trace_order or DEFAULT_ORDER.get(args.workload, "given")
+    return 2 if order == "coherent" else 0  # DIPL_TRACE_COHERENT_ORDER
 
 
 def workload(name, rays_override=None, soup_tris=SOUP_TRIANGLES):
@@ -364,6 +372,7 @@ def run_gpu(args, rank, world, local_rank):
     AT = A.AccelerationStructureType
 
     split = args.split_budget if args.split_budget is not None else DEFAULT_SPLIT.get(args.workload, 0)
+    tflags = trace_flags(args)
 
     def config(code_, bv="aabb", layout="binary", split_budget=None):
         return A.AccelerationStructureConfig(getattr(AT, KIND_OF[(code_, bv)]), nn_search_radius=args.radius,
@@ -388,10 +397,10 @@ def run_gpu(args, rank, world, local_rank):
     def trace(h, out, leaf=lt, counters=None):
         if counters is None:
             L.check(lib.dipl_bvh_trace_closest(h, C.c_void_p(rays.data_ptr()), nr, C.c_void_p(out.data_ptr()), leaf,
-                                               0, sp), "dipl_bvh_trace_closest")
+                                               tflags, sp), "dipl_bvh_trace_closest")
         else:
             L.check(lib.dipl_bvh_trace_closest_counted(h, C.c_void_p(rays.data_ptr()), nr, C.c_void_p(out.data_ptr()),
-                                                       leaf, 0, C.c_void_p(counters.data_ptr()), sp),
+                                                       leaf, tflags, C.c_void_p(counters.data_ptr()), sp),
                     "dipl_bvh_trace_closest_counted")
             L.check(lib.dipl_bvh_check_errors(h, sp), "dipl_bvh_check_errors")  # synchronises; not in timed loops
 
@@ -485,6 +494,7 @@ def run_gpu(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": desc_txt, "triangles": n, "rays": nr,
                    "code": code, "bounding_volume": "aabb", "split_budget": split,
+                   "ray_order": "coherent (sorted on the device)" if tflags else "given",
                    "clustering_leaves": int(info.num_leaves), "nn_search_radius": args.radius,
                    "leaf_test": args.leaf_test, "layout": "binary", "max_triangles_per_leaf": 4,
                    "l2": "inputs larger than L2, and L2 flushed between steps (256 MB write)",
@@ -553,7 +563,7 @@ def e2e_run(args, lib, L, A, torch, C, v, rays, hits, cfg, stream, sp, world, de
         L.check(lib.dipl_bvh_build(C.byref(edescs[b]), C.byref(hh), sp), "dipl_bvh_build")
         stream.wait_event(ev_r[b])
         L.check(lib.dipl_bvh_trace_closest(hh, C.c_void_p(sets[b]["rays"].data_ptr()), nr,
-                                           C.c_void_p(sets[b]["hits"].data_ptr()), lt, 0, sp),
+                                           C.c_void_p(sets[b]["hits"].data_ptr()), lt, trace_flags(args), sp),
                 "dipl_bvh_trace_closest")
         ev_done[b].record(stream)
         d2h_s.wait_event(ev_done[b])
@@ -1022,6 +1032,8 @@ def main():
     ap.add_argument("--split-budget", type=int, default=None,
                     help="pre-splitting of large triangles, percent (default: 40 on the soup, 0 on the sphere)")
     ap.add_argument("--leaf-test", default="ref_mt", choices=["ref_mt", "watertight"])
+    ap.add_argument("--trace-order", default=None, choices=["given", "coherent"],
+                    help="ray order of the traces (default per workload: coherent for the soup, given otherwise)")
     ap.add_argument("--rays", type=int, default=None)
     ap.add_argument("--ref-sample-rays", type=int, default=1 << 12)
     ap.add_argument("--ref-sample-tris", type=int, default=1 << 21,

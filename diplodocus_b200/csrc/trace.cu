@@ -235,31 +235,28 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
                 cur = -0x7FFFFFFF - 1;  // pop below
             }
         } else if (cur != -0x7FFFFFFF - 1) {
+            // one triangle per step: a lane at a leaf never holds the warp for the leaf's other triangles (the
+            // rest of the leaf stays in cur as the reference of its remaining triangles)
             const int first = leaf_first(cur), cnt = leaf_count(cur);
-            for (int k = 0; k < cnt; ++k) {
-                const float4* tp = tris + 3 * (int64_t)(first + k);
-                const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
-                const int prim = __float_as_int(p0.w);
-                float b1 = 0.0f, b2 = 0.0f;
-                const float t = leaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
-                                                make_float3(p2.x, p2.y, p2.z), r, w, backface, b1, b2);
-                if (COUNT) ++tests;
-                // t == kInfinity is the tests' miss value (also when tmax is +inf)
-                if (ANY) {
-                    if (t > r.tmin && t < r.tmax && t < kInfinity) {
-                        found = true;
-                        break;
-                    }
-                } else if (t > r.tmin && t < kInfinity &&
-                           (t < best_t || (t == best_t && found && prim < best_prim))) {
-                    best_t = t;
-                    best_prim = prim;
-                    best_u = b1;
-                    best_v = b2;
-                    found = true;
-                }
+            const float4* tp = tris + 3 * (int64_t)first;
+            const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+            const int prim = __float_as_int(p0.w);
+            float b1 = 0.0f, b2 = 0.0f;
+            const float t = leaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
+                                            make_float3(p2.x, p2.y, p2.z), r, w, backface, b1, b2);
+            if (COUNT) ++tests;
+            // t == kInfinity is the tests' miss value (also when tmax is +inf)
+            if (ANY) {
+                if (t > r.tmin && t < r.tmax && t < kInfinity) found = true;
+            } else if (t > r.tmin && t < kInfinity && (t < best_t || (t == best_t && found && prim < best_prim))) {
+                best_t = t;
+                best_prim = prim;
+                best_u = b1;
+                best_v = b2;
+                found = true;
             }
             if (ANY && found) finished = true;
+            else if (cnt > 1) cur = make_leaf_ref(first + 1, cnt - 1);
             else cur = -0x7FFFFFFF - 1;  // pop below
         }
         if (!finished && cur == -0x7FFFFFFF - 1) {
@@ -582,7 +579,10 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
         set_last_error("trace: node array is not 64-byte aligned");
         return DIPL_ERR_INTERNAL;
     }
-    const uint32_t steps_cap = trace_step_limit() ? trace_step_limit() : 2u * (uint32_t)std::max(num_nodes, 0) + 64u;
+    // a ray takes at most one step per inner node and one per leaf triangle
+    const uint32_t steps_cap = trace_step_limit() ? trace_step_limit()
+                                                  : (uint32_t)std::min<int64_t>(0xFFFFFFFFll, 2ll * std::max(num_nodes, 0) +
+                                                                                                b->num_refs + 64);
     TailQueue tq{nullptr, nullptr, 0, kTailHeaderInts + 2 * STACK, n >= kTailMinRays ? kTailSteps : 0, kTailLanes,
                  steps_cap};
     void* tail_mem = nullptr;
