@@ -404,25 +404,26 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
                     continue;
                 }
             } else {
+                // one triangle per step (the rest of the leaf stays in cur), so a lane at a leaf does not hold
+                // its warp for the leaf's other triangles
                 const int first = leaf_first(cur), cnt = leaf_count(cur);
-                for (int k = 0; k < cnt; ++k) {
-                    const float4* tp = tris + 3 * (int64_t)(first + k);
-                    const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
-                    const int prim = __float_as_int(p0.w);
-                    float b1 = 0.0f, b2 = 0.0f;
-                    const float t = sleaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
-                                                     make_float3(p2.x, p2.y, p2.z), o, d, w, backface, b1, b2);
-                    if (COUNT) ++tests;
-                    if (ANY) {
-                        if (t > tmin && t < tmax && t < kInfinity) {
-                            found = true;
-                            break;
-                        }
-                    } else if (t > tmin && t < kInfinity && (t < best_t || (t == best_t && found && prim < best_prim))) {
-                        best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
-                    }
+                const float4* tp = tris + 3 * (int64_t)first;
+                const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+                const int prim = __float_as_int(p0.w);
+                float b1 = 0.0f, b2 = 0.0f;
+                const float t = sleaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
+                                                 make_float3(p2.x, p2.y, p2.z), o, d, w, backface, b1, b2);
+                if (COUNT) ++tests;
+                if (ANY) {
+                    if (t > tmin && t < tmax && t < kInfinity) found = true;
+                } else if (t > tmin && t < kInfinity && (t < best_t || (t == best_t && found && prim < best_prim))) {
+                    best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
                 }
                 if (ANY && found) break;
+                if (cnt > 1) {
+                    cur = make_leaf_ref(first + 1, cnt - 1);
+                    continue;
+                }
             }
             cur = 0x7FFFFFFF;
             const float lim = best_t + fabsf(best_t) * kSPruneSlack;
@@ -471,7 +472,9 @@ dipl_status launch_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl
     sobb_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kSThreads - 1) / kSThreads), kSThreads, 0, s>>>(
         static_cast<const SNode*>(b->nodes), b->tris, b->root, num_nodes, b->kdop / 2, rays, n, hits, occ, flags,
         counters, b->d_err,
-        trace_step_limit() ? trace_step_limit() : 2u * (uint32_t)std::max(num_nodes, 0) + 64u, ro.order);
+        trace_step_limit() ? trace_step_limit()
+                           : (uint32_t)std::min<int64_t>(0xFFFFFFFFll, 2ll * std::max(num_nodes, 0) + b->num_refs + 64),
+        ro.order);
     note_launches();
     const cudaError_t e = cudaGetLastError();
     if (ro.mem) device_free(ro.mem, s);
