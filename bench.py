@@ -296,15 +296,19 @@ def cpu_baseline_and_parity(tris, rays_np, gpu_hits_np, args, threads):
 # ---------------------------------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------------------------------
-# DRAM bytes (read + write) per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
-# current kernels: per triangle of one build and per ray of one closest-hit trace of each workload (captured on a
-# smaller ray batch of the same scene and scaled by the ray count, which the trace's traffic follows).
-MEASURED_TRAFFIC = {}
+# DRAM bytes (read + write) per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on
+# the current kernels, per ray of one closest-hit trace, for the configuration it was captured with (split budget,
+# ray order); other configurations report no traffic. Soup: the full 16M-triangle, 16M-ray launch,
+# 305.19 GB read + 12.09 GB written (profiles/trace_dram_soup16m.md).
+MEASURED_TRAFFIC = {("soup16m", "emc60", "trace"): {"split_budget": 40, "order": "coherent",
+                                                    "per_unit": (305.19e9 + 12.09e9) / 16777216}}
 
 
-def measured_traffic(workload, code, kind, units):
-    per_unit = MEASURED_TRAFFIC.get((workload, code, kind))
-    return None if per_unit is None else per_unit * units
+def measured_traffic(workload, code, kind, units, split_budget, order):
+    m = MEASURED_TRAFFIC.get((workload, code, kind))
+    if m is None or m["split_budget"] != split_budget or m["order"] != order:
+        return None
+    return round(m["per_unit"] * units)
 
 
 def max_over_ranks(values, world, device=None):
@@ -373,6 +377,7 @@ def run_gpu(args, rank, world, local_rank):
 
     split = args.split_budget if args.split_budget is not None else DEFAULT_SPLIT.get(args.workload, 0)
     tflags = trace_flags(args)
+    order_name = "coherent" if tflags else "given"
 
     def config(code_, bv="aabb", layout="binary", split_budget=None):
         return A.AccelerationStructureConfig(getattr(AT, KIND_OF[(code_, bv)]), nn_search_radius=args.radius,
@@ -478,13 +483,14 @@ def run_gpu(args, rank, world, local_rank):
     achieved_trace = ray_bytes * nr / trace_s / 1e9
     value = world * n / build_s / 1e6
     roof_build = {"bound": "hbm", "achieved": round(achieved_build, 1), "peak": peak, "unit": "GB/s",
-                  "frac": round(achieved_build / peak, 4), "traffic": measured_traffic(args.workload, code, "build", n),
+                  "frac": round(achieved_build / peak, 4), "traffic": measured_traffic(args.workload, code, "build", n, split, order_name),
                   "kernel": "build pipeline (bounds, codes, sort, PLOC, layout)", "ms": round(build_s * 1e3, 4),
                   "bytes_per_unit": round(bpt, 1), "unit_of_bytes": "triangle",
                   "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"}
     roof_trace = {"bound": "hbm", "achieved": round(achieved_trace, 1), "peak": peak, "unit": "GB/s",
                   "frac": round(achieved_trace / peak, 4),
-                  "traffic": measured_traffic(args.workload, code, "trace", nr) if args.leaf_test == "ref_mt" else None,
+                  "traffic": (measured_traffic(args.workload, code, "trace", nr, split, order_name)
+                              if args.leaf_test == "ref_mt" else None),
                   "kernel": "closest-hit trace (trace_kernel + tail_kernel)", "ms": round(trace_s * 1e3, 4),
                   "bytes_per_unit": round(ray_bytes, 1), "unit_of_bytes": "ray", "node_bytes": round(node_bytes, 1),
                   "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"}
