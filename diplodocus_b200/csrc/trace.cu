@@ -21,6 +21,7 @@ constexpr int kTraceThreads = 128;
 // Resident blocks per SM the kernel is compiled for: 9 x 128 threads at <= 56 registers. Builds with more
 // registers and 8 blocks per SM measured up to 1.5x slower on the 16M-triangle soup.
 constexpr int kTraceMinBlocks = 9;
+constexpr bool kInterleave = true;
 constexpr float kSlabWiden = 1e-6f;
 constexpr float kPruneSlack = 1e-5f;
 
@@ -158,12 +159,19 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
     __shared__ int2 sh_stack[SHORT > 0 ? SHORT * kTraceThreads : 1];
     const int lane = threadIdx.x & 31;
     const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    // The k-th ray a warp takes: with kInterleave at position ((k / 32) * warps + warp) * 32 + k % 32 of the work
+    // order, so all warps walk the order together and the rays in flight are one window of it (a coherent order
+    // then keeps the whole GPU in one region of the tree); else k positions into the warp's own chunk.
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t beg = warp_id * chunk;
-    const int64_t end = min(n, beg + chunk);
+    const int64_t end = kInterleave ? n : min(n, beg + chunk);
+    auto position = [&](int64_t k) -> int64_t {
+        return kInterleave ? (((k >> 5) * warps + warp_id) << 5) + (k & 31) : beg + k;
+    };
     const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
     const uint32_t lt_mask = lanemask_lt();
     const uint32_t step_limit = tq.step_limit;
-    int64_t next = beg;  // next ray of the chunk (warp-uniform)
+    int64_t next = 0;    // rays this warp has taken (warp-uniform)
     int64_t my = -1;     // this lane's ray, -1 when idle
     RayState r{};
     WtRay w{};
@@ -183,7 +191,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
         const uint32_t idle_mask = __ballot_sync(0xffffffffu, idle);
         if (idle_mask) {
             if (idle) {
-                const int64_t cand = next + __popc(idle_mask & lt_mask);
+                const int64_t cand = position(next + __popc(idle_mask & lt_mask));
                 if (cand < end) {
                     my = order ? (int64_t)__ldg(order + cand) : cand;  // the ray's own index (hits go there)
                     r = load_ray(rays, my);
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
                     steps = 0;
                 }
             }
-            next = min(end, next + (int64_t)__popc(idle_mask));
+            if (position(next) < end) next += __popc(idle_mask);
         }
         const uint32_t active_mask = __ballot_sync(0xffffffffu, my >= 0);
         if (!active_mask) break;
@@ -285,7 +293,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
                 reinterpret_cast<int4*>(hits)[my] = out;
             }
             my = -1;
-        } else if (may_offload && next >= end && steps >= (uint32_t)tq.min_steps &&
+        } else if (may_offload && position(next) >= end && steps >= (uint32_t)tq.min_steps &&
                    __popc(active_mask) <= tq.max_lanes) {
             // the chunk is handed out and this ray is still going: hand it to tail_kernel if a slot is free
             const unsigned slot = atomicAdd(&tq.count[0], 1u);
