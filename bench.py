@@ -680,6 +680,7 @@ def soup_forms(args, lib, L, A, torch, C, v, rays, hits, h_main, cfg, config, bu
     for name, (code_, bv, layout, split_) in SOUP_VARIANTS.items():
         c = config(code_, bv, layout, split_)
         d = A.make_desc(*v, c)
+        timed(lambda: build(d), 1)  # warm-up: the first build of a form sizes its buffers in the memory pool
         b_ms = timed(lambda: build(d), args.variant_builds)
         hv = build(d)
         t_ms = timed(lambda: trace(hv, vh), args.variant_traces)

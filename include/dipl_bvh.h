@@ -77,9 +77,9 @@ typedef enum dipl_leaf_test { DIPL_LEAF_REF_MT = 0, DIPL_LEAF_WATERTIGHT = 1 } d
 /* Trace a batch of 2^20 rays or more in the order of a key of each ray's origin cell and direction octant
  * (computed and sorted on the device inside the call), so that the rays of a warp start close together and head
  * the same way; each record still goes to its ray's index and the records are the same either way. Without it
- * the rays are traced in the order given. On a B200 the sorted order is slower for random rays in a 16M-triangle
- * soup (922 ms against 805 ms) and for 1M camera rays (the sort costs more than it saves), and about 5% faster
- * for the same soup built with pre-splitting, so it is an option and not the default. */
+ * the rays are traced in the order given. On a B200 it pays for incoherent batches (16M random rays in a
+ * pre-split 16M-triangle soup: 163 ms against 211 ms) but not for camera-like rays that already come in order
+ * (4M rays on a 1M-triangle sphere: the sort costs more than it saves), so it is an option of the call. */
 #define DIPL_TRACE_COHERENT_ORDER 2u
 
 /* Build description. The three vertex arrays are the reference GPU scene's SoA positions
