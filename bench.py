@@ -300,13 +300,13 @@ def cpu_baseline_and_parity(tris, rays_np, gpu_hits_np, args, threads):
 # the current kernels, per ray of one closest-hit trace, for the configuration it was captured with (split budget,
 # ray order); other configurations report no traffic. Soup: the full 16M-triangle, 16M-ray launch,
 # 305.19 GB read + 12.09 GB written (profiles/trace_dram_soup16m.md).
-MEASURED_TRAFFIC = {("soup16m", "emc60", "trace"): {"split_budget": 40, "order": "coherent",
+MEASURED_TRAFFIC = {("soup16m", "emc60", "trace"): {"split_budget": 40, "order": "coherent", "triangles": 16777216,
                                                     "per_unit": (305.19e9 + 12.09e9) / 16777216}}
 
 
-def measured_traffic(workload, code, kind, units, split_budget, order):
+def measured_traffic(workload, code, kind, units, split_budget, order, triangles):
     m = MEASURED_TRAFFIC.get((workload, code, kind))
-    if m is None or m["split_budget"] != split_budget or m["order"] != order:
+    if m is None or m["split_budget"] != split_budget or m["order"] != order or m["triangles"] != triangles:
         return None
     return round(m["per_unit"] * units)
 
@@ -483,13 +483,13 @@ def run_gpu(args, rank, world, local_rank):
     achieved_trace = ray_bytes * nr / trace_s / 1e9
     value = world * n / build_s / 1e6
     roof_build = {"bound": "hbm", "achieved": round(achieved_build, 1), "peak": peak, "unit": "GB/s",
-                  "frac": round(achieved_build / peak, 4), "traffic": measured_traffic(args.workload, code, "build", n, split, order_name),
+                  "frac": round(achieved_build / peak, 4), "traffic": measured_traffic(args.workload, code, "build", n, split, order_name, n),
                   "kernel": "build pipeline (bounds, codes, sort, PLOC, layout)", "ms": round(build_s * 1e3, 4),
                   "bytes_per_unit": round(bpt, 1), "unit_of_bytes": "triangle",
                   "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"}
     roof_trace = {"bound": "hbm", "achieved": round(achieved_trace, 1), "peak": peak, "unit": "GB/s",
                   "frac": round(achieved_trace / peak, 4),
-                  "traffic": (measured_traffic(args.workload, code, "trace", nr, split, order_name)
+                  "traffic": (measured_traffic(args.workload, code, "trace", nr, split, order_name, n)
                               if args.leaf_test == "ref_mt" else None),
                   "kernel": "closest-hit trace (trace_kernel + tail_kernel)", "ms": round(trace_s * 1e3, 4),
                   "bytes_per_unit": round(ray_bytes, 1), "unit_of_bytes": "ray", "node_bytes": round(node_bytes, 1),
