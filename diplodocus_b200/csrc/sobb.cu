@@ -457,6 +457,197 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
     }
 }
 
+// Persistent form for rays in the given order: every lane advances its ray by one node, one leaf triangle or one
+// pop per step and takes the warp's next ray when its own ends, and the warps take 32-ray groups interleaved over
+// the batch (warp w takes groups w, w + W, ...), so no lane waits for its warp's longest ray (the one-thread-per-ray
+// kernel above stays for the coherent order, where lanes that start neighbouring rays together matter more).
+template <int LEAF, bool ANY, bool COUNT, int STACK>
+__global__ void __launch_bounds__(kSThreads) sobb_persist_kernel(const SNode* __restrict__ nodes,
+                                                                 const float4* __restrict__ tris, int root,
+                                                                 int num_nodes, int dirs,
+                                                                 const dipl_ray* __restrict__ rays, int64_t n,
+                                                                 dipl_hit* __restrict__ hits,
+                                                                 uint8_t* __restrict__ occluded, uint32_t flags,
+                                                                 unsigned long long* __restrict__ counters,
+                                                                 uint32_t* __restrict__ err, uint32_t step_limit) {
+    constexpr int kDone = 0x7FFFFFFF;
+    __shared__ float4 s_ray[kDirs][kSThreads];
+    const unsigned full = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + tid) >> 5;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    auto position = [&](int64_t k) -> int64_t { return (((k >> 5) * warps + warp_id) << 5) + (k & 31); };
+    const uint32_t lt_mask = lanemask_lt();
+    const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
+    unsigned visits = 0, tests = 0;
+    bool bad = false;
+    int64_t next = 0;  // rays this warp has taken (warp-uniform)
+    int64_t my = -1;   // this lane's ray, -1 when idle
+    float3 o = make_float3(0.f, 0.f, 0.f), d = o;
+    float tmin = 0.0f, tmax = 0.0f;
+    WtRay w{};
+    float best_t = 0.0f, best_u = 0.0f, best_v = 0.0f;
+    int best_prim = -1;
+    bool found = false;
+    int sref[STACK];
+    float st[STACK];
+    int sp = 0;
+    int cur = kDone;
+    uint32_t steps = 0;
+    auto slab_box = [&](int axes, float l0, float h0, float l1, float h1, float l2, float h2, float lim) {
+        float tn = __int_as_float(0xFF800000), tf = __int_as_float(0x7F800000);
+        const float ls[3] = {l0, l1, l2}, hs[3] = {h0, h1, h2};
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int k = (axes >> (8 * j)) & 0xFF;
+            const float4 q = s_ray[k][tid];
+            const float ok = q.x, inv = q.y, tol = q.z, rel = q.w;
+            const float t0 = __fmul_rn(__fsub_rn(ls[j], ok), inv), t1 = __fmul_rn(__fsub_rn(hs[j], ok), inv);
+            const float a0 = fminf(t0, t1), a1 = fmaxf(t0, t1);
+            tn = fmaxf(tn, a0 - fabsf(a0) * rel - tol);
+            tf = fminf(tf, a1 + fabsf(a1) * rel + tol);
+        }
+        return (tn <= tf && tf >= tmin && tn <= lim) ? tn : __int_as_float(0x7F800000);
+    };
+    for (;;) {
+        // ---- refill idle lanes --------------------------------------------------------------------------
+        const bool idle = my < 0;
+        const uint32_t idle_mask = __ballot_sync(full, idle);
+        if (idle_mask) {
+            if (idle) {
+                const int64_t cand = position(next + __popc(idle_mask & lt_mask));
+                if (cand < n) {
+                    my = cand;
+                    const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * my;
+                    const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
+                    o = make_float3(ra.x, ra.y, ra.z);
+                    d = make_float3(rb.x, rb.y, rb.z);
+                    tmin = ra.w;
+                    tmax = rb.w;
+                    const float omag = fabsf(o.x) + fabsf(o.y) + fabsf(o.z);
+                    const float dmag = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+                    for (int k = 0; k < dirs; ++k) {
+                        const float dk = proj(k, d.x, d.y, d.z);
+                        const float inv = __frcp_rn(fabsf(dk) < 1e-20f ? copysignf(1e-20f, dk) : dk);
+                        s_ray[k][tid] = make_float4(proj(k, o.x, o.y, o.z), inv, omag * 4.0e-7f * fabsf(inv),
+                                                    kSSlabWiden + dmag * 4.0e-7f * fabsf(inv));
+                    }
+                    if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(d);
+                    best_t = tmax, best_u = 0.0f, best_v = 0.0f, best_prim = -1, found = false;
+                    sp = 0;
+                    steps = 0;
+                    cur = num_nodes >= 0 ? root : kDone;
+                }
+            }
+            if (position(next) < n) next += __popc(idle_mask);
+        }
+        if (!__ballot_sync(full, my >= 0)) break;
+        if (my < 0) continue;
+
+        // ---- one step: an inner node, one leaf triangle, or a pop -------------------------------------------
+        bool finished = false, pop = false;
+        if (cur == kDone) {
+            finished = true;  // empty BVH
+        } else if (++steps > step_limit || (cur >= 0 && cur >= num_nodes)) {
+            bad = true;  // only a corrupted tree gets here
+            finished = true;
+        } else if (cur >= 0) {
+            const float4* np = reinterpret_cast<const float4*>(nodes + cur);
+            const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+            const int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
+            if (COUNT) ++visits;
+            const float lim = best_t + fabsf(best_t) * kSPruneSlack;
+            const float t0 = slab_box(dd.z, a.x, a.y, a.z, a.w, b.x, b.y, lim);
+            const float t1 = slab_box(dd.w, b.z, b.w, c.x, c.y, c.z, c.w, lim);
+            const bool h0 = t0 != __int_as_float(0x7F800000), h1 = t1 != __int_as_float(0x7F800000);
+            if (h0 && h1) {
+                const bool first0 = t0 <= t1;
+                if (sp >= STACK) {
+                    bad = true;
+                    finished = true;
+                } else {
+                    sref[sp] = first0 ? dd.y : dd.x;
+                    st[sp] = first0 ? t1 : t0;
+                    ++sp;
+                    cur = first0 ? dd.x : dd.y;
+                }
+            } else if (h0) {
+                cur = dd.x;
+            } else if (h1) {
+                cur = dd.y;
+            } else {
+                pop = true;
+            }
+        } else {
+            // one triangle per step (the rest of the leaf stays in cur)
+            const int first = leaf_first(cur), cnt = leaf_count(cur);
+            const float4* tp = tris + 3 * (int64_t)first;
+            const float4 p0 = __ldg(tp), p1 = __ldg(tp + 1), p2 = __ldg(tp + 2);
+            const int prim = __float_as_int(p0.w);
+            float b1 = 0.0f, b2 = 0.0f;
+            const float t = sleaf_test<LEAF>(make_float3(p0.x, p0.y, p0.z), make_float3(p1.x, p1.y, p1.z),
+                                             make_float3(p2.x, p2.y, p2.z), o, d, w, backface, b1, b2);
+            if (COUNT) ++tests;
+            if (ANY) {
+                if (t > tmin && t < tmax && t < kInfinity) found = true;
+            } else if (t > tmin && t < kInfinity && (t < best_t || (t == best_t && found && prim < best_prim))) {
+                best_t = t, best_prim = prim, best_u = b1, best_v = b2, found = true;
+            }
+            if (ANY && found) finished = true;
+            else if (cnt > 1) cur = make_leaf_ref(first + 1, cnt - 1);
+            else pop = true;
+        }
+        if (pop) {
+            cur = kDone;
+            const float lim = best_t + fabsf(best_t) * kSPruneSlack;
+            while (sp > 0) {
+                --sp;
+                if (st[sp] <= lim) {
+                    cur = sref[sp];
+                    break;
+                }
+            }
+            if (cur == kDone) finished = true;
+        }
+        if (finished) {
+            if (ANY) {
+                occluded[my] = found ? 1 : 0;
+            } else {
+                int4 out;
+                out.x = found ? best_prim : -1;
+                out.y = __float_as_int(found ? best_t : __int_as_float(0x7F800000));
+                out.z = __float_as_int(found ? best_u : 0.0f);
+                out.w = __float_as_int(found ? best_v : 0.0f);
+                reinterpret_cast<int4*>(hits)[my] = out;
+            }
+            my = -1;
+        }
+    }
+    if (bad) atomicOr(err, kErrStack);
+    if (COUNT) {
+        const unsigned v = __reduce_add_sync(full, visits);
+        const unsigned t = __reduce_add_sync(full, tests);
+        if (lane == 0) {
+            atomicAdd(&counters[0], (unsigned long long)v);
+            atomicAdd(&counters[1], (unsigned long long)t);
+        }
+    }
+}
+
+// Resident blocks of a traversal kernel on the current device (probed once per device and kernel).
+template <typename Kernel>
+int sobb_grid(Kernel kernel) {
+    static DeviceProbe probe;
+    return probe_per_device(probe, [kernel] {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSThreads, 0);
+        (void)cudaGetLastError();
+        return std::max(1, sms * std::max(1, per_sm));
+    });
+}
+
 template <int LEAF, bool ANY, bool COUNT, int STACK>
 dipl_status launch_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl_hit* hits, uint8_t* occ,
                         uint32_t flags, unsigned long long* counters, cudaStream_t s) {
@@ -469,12 +660,20 @@ dipl_status launch_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl
             return st;
         }
     }
-    sobb_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kSThreads - 1) / kSThreads), kSThreads, 0, s>>>(
-        static_cast<const SNode*>(b->nodes), b->tris, b->root, num_nodes, b->kdop / 2, rays, n, hits, occ, flags,
-        counters, b->d_err,
+    const uint32_t cap =
         trace_step_limit() ? trace_step_limit()
-                           : (uint32_t)std::min<int64_t>(0xFFFFFFFFll, 2ll * std::max(num_nodes, 0) + b->num_refs + 64),
-        ro.order);
+                           : (uint32_t)std::min<int64_t>(0xFFFFFFFFll, 2ll * std::max(num_nodes, 0) + b->num_refs + 64);
+    if (ro.order) {
+        sobb_trace_kernel<LEAF, ANY, COUNT, STACK><<<(unsigned)((n + kSThreads - 1) / kSThreads), kSThreads, 0, s>>>(
+            static_cast<const SNode*>(b->nodes), b->tris, b->root, num_nodes, b->kdop / 2, rays, n, hits, occ, flags,
+            counters, b->d_err, cap, ro.order);
+    } else {
+        auto kernel = sobb_persist_kernel<LEAF, ANY, COUNT, STACK>;
+        const int64_t grid =
+            std::max<int64_t>(1, std::min<int64_t>(sobb_grid(kernel), (n + kSThreads - 1) / kSThreads));
+        kernel<<<(unsigned)grid, kSThreads, 0, s>>>(static_cast<const SNode*>(b->nodes), b->tris, b->root, num_nodes,
+                                                    b->kdop / 2, rays, n, hits, occ, flags, counters, b->d_err, cap);
+    }
     note_launches();
     const cudaError_t e = cudaGetLastError();
     if (ro.mem) device_free(ro.mem, s);
