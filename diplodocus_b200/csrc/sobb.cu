@@ -469,7 +469,8 @@ __global__ void __launch_bounds__(kSThreads) sobb_persist_kernel(const SNode* __
                                                                  dipl_hit* __restrict__ hits,
                                                                  uint8_t* __restrict__ occluded, uint32_t flags,
                                                                  unsigned long long* __restrict__ counters,
-                                                                 uint32_t* __restrict__ err, uint32_t step_limit) {
+                                                                 uint32_t* __restrict__ err, uint32_t step_limit,
+                                                                 const uint32_t* __restrict__ order) {
     constexpr int kDone = 0x7FFFFFFF;
     __shared__ float4 s_ray[kDirs][kSThreads];
     const unsigned full = 0xffffffffu;
@@ -517,7 +518,7 @@ __global__ void __launch_bounds__(kSThreads) sobb_persist_kernel(const SNode* __
             if (idle) {
                 const int64_t cand = position(next + __popc(idle_mask & lt_mask));
                 if (cand < n) {
-                    my = cand;
+                    my = order ? (int64_t)__ldg(order + cand) : cand;  // the ray's own index (hits go there)
                     const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * my;
                     const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
                     o = make_float3(ra.x, ra.y, ra.z);
@@ -672,7 +673,8 @@ dipl_status launch_sobb(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dipl
         const int64_t grid =
             std::max<int64_t>(1, std::min<int64_t>(sobb_grid(kernel), (n + kSThreads - 1) / kSThreads));
         kernel<<<(unsigned)grid, kSThreads, 0, s>>>(static_cast<const SNode*>(b->nodes), b->tris, b->root, num_nodes,
-                                                    b->kdop / 2, rays, n, hits, occ, flags, counters, b->d_err, cap);
+                                                    b->kdop / 2, rays, n, hits, occ, flags, counters, b->d_err, cap,
+                                                    nullptr);
     }
     note_launches();
     const cudaError_t e = cudaGetLastError();
