@@ -632,6 +632,10 @@ def soup_forms(args, lib, L, A, torch, C, v, rays, hits, h_main, cfg, config, bu
         out = []
         for _ in range(reps):
             flush.zero_()
+            # the flush finishes before the timed build is enqueued: builds enqueued behind it measured 1.5-4x
+            # their time now and then (unsplit soup 24-65 ms against 16.1 ms; SOBB 67 against 33.5 ms), the same
+            # builds after a synchronise 16.1 +- 0.03 ms and 33.5 +- 0.05 ms in five runs
+            torch.cuda.synchronize()
             a, b = ev()
             a.record(stream)
             r = fn()
