@@ -1734,7 +1734,7 @@ __device__ __forceinline__ void node_write_one(const LayoutParams& P, const floa
                                                const uint32_t* __restrict__ rev_index,
                                                const int* __restrict__ leaf_start_of, BNode* __restrict__ nodes,
                                                double* __restrict__ sah, const uint32_t* err, double& local_sum,
-                                               double& local_count) {
+                                               double& local_count, int& mesh_out) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= P.num_inner || *err != 0u) return;
     if (__float_as_int(P.node_lo[k].w) < P.L) return;
@@ -1764,14 +1764,9 @@ __device__ __forceinline__ void node_write_one(const LayoutParams& P, const floa
                        pad_up(lo[1].z, hi[1].z));
     nd.d = make_int4(ref[0], ref[1], 0, 0);
     nodes[f] = nd;
-    const int mesh = find_mesh(offsets, m, (long long)perm[__float_as_int(P.node_hi[k].w)]);
-    if (m == 1) {
-        local_sum = acc;
-        local_count = 1.0;
-    } else {
-        atomicAdd(&sah[2 * mesh], acc);
-        atomicAdd(&sah[2 * mesh + 1], 1.0);
-    }
+    local_sum = acc;
+    local_count = 1.0;
+    mesh_out = m == 1 ? 0 : find_mesh(offsets, m, (long long)perm[__float_as_int(P.node_hi[k].w)]);
 }
 
 // Single-mesh builds: one FP64 atomic pair per block instead of one per node.
@@ -1780,8 +1775,30 @@ __global__ void node_write_kernel(LayoutParams P, const float4* __restrict__ tbo
                                   const uint32_t* __restrict__ rev_index, const int* __restrict__ leaf_start_of,
                                   BNode* __restrict__ nodes, double* __restrict__ sah, const uint32_t* err) {
     double local_sum = 0.0, local_count = 0.0;
-    node_write_one(P, tbox, offsets, m, perm, rev_index, leaf_start_of, nodes, sah, err, local_sum, local_count);
-    if (m != 1) return;
+    int mesh = -1;  // this thread's node's mesh, -1 without a node
+    node_write_one(P, tbox, offsets, m, perm, rev_index, leaf_start_of, nodes, sah, err, local_sum, local_count, mesh);
+    if (m != 1) {
+        // Nodes are numbered in position order, so a warp's nodes nearly always belong to one mesh: one FP64 atomic
+        // pair per warp then, instead of 32 on the same two addresses (the 256-mesh batch spent 91 ms in this kernel
+        // with one pair per node). Lanes of a warp that spans meshes add their own.
+        const unsigned full = 0xffffffffu;
+        const int lead = __ffs(__ballot_sync(full, mesh >= 0)) - 1;
+        const int m0 = lead >= 0 ? __shfl_sync(full, mesh, lead) : -1;
+        if (__all_sync(full, mesh < 0 || mesh == m0)) {
+            for (int o = 16; o > 0; o >>= 1) {
+                local_sum += __shfl_xor_sync(full, local_sum, o);
+                local_count += __shfl_xor_sync(full, local_count, o);
+            }
+            if ((threadIdx.x & 31) == 0 && m0 >= 0) {
+                atomicAdd(&sah[2 * m0], local_sum);
+                atomicAdd(&sah[2 * m0 + 1], local_count);
+            }
+        } else if (mesh >= 0) {
+            atomicAdd(&sah[2 * mesh], local_sum);
+            atomicAdd(&sah[2 * mesh + 1], local_count);
+        }
+        return;
+    }
     __shared__ double s_sum[32], s_cnt[32];
     for (int o = 16; o > 0; o >>= 1) {
         local_sum += __shfl_xor_sync(0xffffffffu, local_sum, o);
