@@ -946,7 +946,8 @@ def run_batched(args):
         "plan_graph_ms": round(ms_plan, 3), "sequential_plain_ms": round(ms_plain, 3),
         "speedup_batched_vs_plain": round(ms_plain / ms_plan, 3),
         "plain_mtri_s": round(total / ms_plain / 1e3, 1),
-        "autotuned": {"radius": d0.nn_search_radius, "block": d0.ploc_block_size, "digits": d0.sort_digit_bits,
+        "autotuned": {"clustering": "ploc" if d0.clustering == L.CLUSTER_PLOC else "hploc",
+                      "radius": d0.nn_search_radius, "block": d0.ploc_block_size, "digits": d0.sort_digit_bits,
                       "from_cache": from_cache, "tune_s": round(tune_s, 2)},
         "trace_mrays_s_per_mesh_median": round(float(np.median([nr / t / 1e3 for t in ms_tr])), 2),
         "hit_agreement_plan_vs_plain": min(agree), "gpu_launches_per_plan": int(launches),

@@ -1,12 +1,13 @@
-// Autotuner of the build knobs: PLOC radius, PLOC block size (global PLOC only: the hierarchical clustering's block
-// is fixed) and sort digit width.
+// Autotuner of the build knobs: clustering (hierarchical or global PLOC), PLOC radius, PLOC block size (global PLOC
+// only: the hierarchical clustering's block is fixed) and sort digit width.
 //
 // For a batch (its total triangle count gives a size bucket, floor(log2 N)), it times real builds of the
 // caller's meshes and keeps the fastest setting whose SAH cost stays within 2% of the default radius-16
 // tree (the radius trades build time for tree quality; hits are exact with any valid tree, so only time and
-// quality are compared). Coordinate search: digit width, then block size, then radius, each with the others
-// fixed at the best so far. Winners are cached per (code, bounding volume, layout, leaf size, clustering, bucket) as
-// one JSON object per line in a file, so a bucket is tuned once.
+// quality are compared). Coordinate search: digit width, then the other clustering (under the same SAH rule: one
+// launch over hundreds of meshes can favour the global loop), then block size, then radius, each with the others
+// fixed at the best so far. Winners are cached per (code, bounding volume, layout, leaf size, requested clustering,
+// bucket) as one JSON object per line in a file, so a bucket is tuned once.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -22,6 +23,7 @@ namespace {
 struct Tuned {
     int radius, block, digits;
     double ms, sah;
+    int clustering;
 };
 
 std::string bucket_key(const dipl_build_desc& d, long long total) {
@@ -50,9 +52,10 @@ bool cache_lookup(const char* path, const std::string& key, Tuned* t) {
             *v = std::strtod(line.c_str() + p + k.size(), nullptr);
             return true;
         };
-        double r, b, dg, ms, sah;
+        double r, b, dg, ms, sah, cl;
         if (num("radius", &r) && num("block", &b) && num("digits", &dg) && num("ms", &ms) && num("sah", &sah)) {
             x.radius = (int)r, x.block = (int)b, x.digits = (int)dg, x.ms = ms, x.sah = sah;
+            x.clustering = num("clustering", &cl) ? (int)cl : -1;  // entries without it keep the requested one
             *t = x;  // the last entry of a key wins
             found = true;
         }
@@ -64,7 +67,8 @@ void cache_store(const char* path, const std::string& key, const Tuned& t) {
     if (!path) return;
     std::ofstream f(path, std::ios::app);
     f << "{\"key\": \"" << key << "\", \"radius\": " << t.radius << ", \"block\": " << t.block
-      << ", \"digits\": " << t.digits << ", \"ms\": " << t.ms << ", \"sah\": " << t.sah << "}\n";
+      << ", \"digits\": " << t.digits << ", \"ms\": " << t.ms << ", \"sah\": " << t.sah
+      << ", \"clustering\": " << t.clustering << "}\n";
 }
 
 // Mean wall time of `reps` builds (after one warm-up) and the triangle-weighted SAH cost.
@@ -109,28 +113,37 @@ dipl_status autotune(const dipl_build_desc* descs, int count, const char* cache_
     if (from_cache) *from_cache = cached ? 1 : 0;
     if (!cached) {
         std::vector<dipl_build_desc> v(descs, descs + count);
-        auto apply = [&](int radius, int block, int digits) {
-            for (auto& d : v) d.nn_search_radius = radius, d.ploc_block_size = block, d.sort_digit_bits = digits;
+        auto apply = [&](int clustering, int radius, int block, int digits) {
+            for (auto& d : v)
+                d.clustering = clustering, d.nn_search_radius = radius, d.ploc_block_size = block,
+                d.sort_digit_bits = digits;
         };
         double ms = 0, sah = 0;
-        apply(16, 256, 8);
+        const int requested = descs[0].clustering;
+        apply(requested, 16, 256, 8);
         dipl_status st = time_builds(v, 2, s, &ms, &sah);
         if (st != DIPL_OK) return st;
-        best = Tuned{16, 256, 8, ms, sah};
+        best = Tuned{16, 256, 8, ms, sah, requested};
         const double sah_limit = sah * 1.02;
         for (int digits : {6, 10}) {
-            apply(best.radius, best.block, digits);
+            apply(best.clustering, best.radius, best.block, digits);
             if ((st = time_builds(v, 2, s, &ms, &sah)) != DIPL_OK) return st;
             if (ms < best.ms) best.digits = digits, best.ms = ms, best.sah = sah;
         }
+        {
+            const int other = requested == DIPL_CLUSTER_PLOC ? DIPL_CLUSTER_HPLOC : DIPL_CLUSTER_PLOC;
+            apply(other, best.radius, best.block, best.digits);
+            if ((st = time_builds(v, 2, s, &ms, &sah)) != DIPL_OK) return st;
+            if (ms < best.ms && sah <= sah_limit) best.clustering = other, best.ms = ms, best.sah = sah;
+        }
         for (int block : {128, 512}) {
-            if (descs[0].clustering != DIPL_CLUSTER_PLOC) break;  // the hierarchical clustering has one block size
-            apply(best.radius, block, best.digits);
+            if (best.clustering != DIPL_CLUSTER_PLOC) break;  // the hierarchical clustering has one block size
+            apply(best.clustering, best.radius, block, best.digits);
             if ((st = time_builds(v, 2, s, &ms, &sah)) != DIPL_OK) return st;
             if (ms < best.ms) best.block = block, best.ms = ms, best.sah = sah;
         }
         for (int radius : {8, 12, 24, 32}) {
-            apply(radius, best.block, best.digits);
+            apply(best.clustering, radius, best.block, best.digits);
             if ((st = time_builds(v, 2, s, &ms, &sah)) != DIPL_OK) return st;
             if (ms < best.ms && sah <= sah_limit) best.radius = radius, best.ms = ms, best.sah = sah;
         }
@@ -138,6 +151,7 @@ dipl_status autotune(const dipl_build_desc* descs, int count, const char* cache_
     }
     for (int i = 0; i < count; ++i) {
         tuned[i] = descs[i];
+        if (best.clustering >= 0) tuned[i].clustering = best.clustering;
         tuned[i].nn_search_radius = best.radius;
         tuned[i].ploc_block_size = best.block;
         tuned[i].sort_digit_bits = best.digits;

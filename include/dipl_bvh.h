@@ -169,9 +169,10 @@ DIPL_API dipl_status dipl_build_plan_launch(dipl_build_plan* plan, void* stream)
 DIPL_API dipl_status dipl_build_plan_get_bvhs(dipl_build_plan* plan, dipl_bvh** out, void* stream);
 DIPL_API dipl_status dipl_build_plan_destroy(dipl_build_plan* plan);
 
-/* Autotuner of the build knobs (PLOC radius, PLOC block size, sort digit width) for a batch: times real builds
- * of these meshes and keeps the fastest setting whose SAH cost is within 2% of the radius-16 default; the
- * winner is cached per (code, bounding volume, layout, leaf size, size bucket floor(log2 total triangles)) in
+/* Autotuner of the build knobs (clustering, PLOC radius, PLOC block size, sort digit width) for a batch: times
+ * real builds of these meshes and keeps the fastest setting whose SAH cost is within 2% of the radius-16 default
+ * with the requested clustering; the winner is cached per (code, bounding volume, layout, leaf size, requested
+ * clustering, size bucket floor(log2 total triangles)) in
  * `cache_path` (one JSON object per line; NULL = no cache). tuned[i] = descs[i] with the chosen knobs;
  * *from_cache (may be NULL) tells whether the cache answered. Synchronises `stream` (it builds). */
 DIPL_API dipl_status dipl_autotune_build(const dipl_build_desc* descs, int32_t count, const char* cache_path,

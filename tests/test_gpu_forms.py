@@ -3,6 +3,7 @@ import numpy as np
 import pytest
 import torch
 
+from diplodocus_b200 import _lib as L
 from diplodocus_b200 import accel as A
 from diplodocus_b200 import scenes as S
 from gpu_util import build, fbits, trace
@@ -223,7 +224,8 @@ def test_autotuned_build_keeps_the_sah_rule_and_is_not_slower(tmp_path, clusteri
 
     t_def, c_def = run(default)
     d0 = tuned[0]
-    tcfg = A.AccelerationStructureConfig(clustering=clustering, nn_search_radius=d0.nn_search_radius,
+    tuned_clustering = "ploc" if d0.clustering == L.CLUSTER_PLOC else "hploc"  # the tuner may switch it
+    tcfg = A.AccelerationStructureConfig(clustering=tuned_clustering, nn_search_radius=d0.nn_search_radius,
                                          ploc_block_size=d0.ploc_block_size, sort_digit_bits=d0.sort_digit_bits)
     t_tun, c_tun = run(tcfg)
     w = np.array([len(m) for m in meshes], np.float64)
