@@ -1682,7 +1682,7 @@ __device__ __forceinline__ void write_tri(const MeshDesc* meshes, const long lon
 __global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ meshes,
                                   const long long* __restrict__ offsets, int m, const uint32_t* __restrict__ perm,
                                   const int* __restrict__ ref_tri, const uint32_t* __restrict__ starts, int* __restrict__ leaf_start_of,
-                                  float4* __restrict__ tris, int* __restrict__ pos_slot, const uint32_t* err) {
+                                  float4* __restrict__ tris, int* __restrict__ slot_pos, const uint32_t* err) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.num_leaves || *err != 0u) return;
     int x = p, rank = 0;
@@ -1696,7 +1696,7 @@ __global__ void leaf_write_kernel(LayoutParams P, const MeshDesc* __restrict__ m
     const int first = node_pmin(P, x);
     const int start = (int)starts[first];
     if (p == first) leaf_start_of[x] = start;
-    if (pos_slot) pos_slot[p] = start + rank;
+    if (slot_pos) slot_pos[start + rank] = p;
     write_tri(meshes, offsets, m, perm, ref_tri, p, tris, start + rank);
 }
 
@@ -2041,7 +2041,7 @@ struct BuildPlan {
     int *hp_other = nullptr, *hp_cnt = nullptr, *hp_fid = nullptr;  // hierarchical clustering
     uint32_t *rev_flags = nullptr, *contrib = nullptr, *d_counts = nullptr;
     int *owner_leaf = nullptr, *leaf_start_of = nullptr;
-    int* pos_slot = nullptr;  // pre-split SOBB builds: per sorted position, its slot in the leaf triangle array
+    int* slot_pos = nullptr;  // pre-split SOBB builds: per slot of the leaf triangle array, its sorted position
     unsigned char* scan_scratch = nullptr;
     BNode* nodes = nullptr;
     float4* tris = nullptr;
@@ -2205,7 +2205,7 @@ static dipl_status plan_prepare(BuildPlan& P, const dipl_build_desc* descs, int 
         return st;
     if (d0.bv_type == DIPL_BV_SOBB) {
         if ((st = sobb_prepare(N, K, W, O, &P.sobb, &P.snodes)) != DIPL_OK) return st;
-        if (P.split && (st = W.alloc(&P.pos_slot, N)) != DIPL_OK) return st;
+        if (P.split && (st = W.alloc(&P.slot_pos, N)) != DIPL_OK) return st;
     }
     P.summary_bytes = sizeof(RootInfo) * m + sizeof(double) * 2 * m + 16;
     if (own_summary) {  // a plan replays into its own pinned buffer
@@ -2379,7 +2379,7 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     if ((st = exclusive_scan_u32(P.contrib, P.contrib, N, nullptr, P.scan_scratch, stream, P.d_err)) != DIPL_OK)
         return st;
     leaf_write_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(LP, P.d_meshes, P.d_offsets, m, P.perm, P.ref_tri,
-                                                               P.contrib, P.leaf_start_of, P.tris, P.pos_slot, P.d_err);
+                                                               P.contrib, P.leaf_start_of, P.tris, P.slot_pos, P.d_err);
     note_launches();
     if (K > 0) {
         node_write_kernel<<<blocks_for(K, 256), 256, 0, stream>>>(LP, P.tbox, P.d_coffsets, m, P.perm, P.rev_flags,
@@ -2392,7 +2392,7 @@ static dipl_status plan_enqueue(BuildPlan& P, cudaStream_t stream) {
     DIPL_CUDA(cudaGetLastError());
     if (d0.bv_type == DIPL_BV_SOBB) {
         SobbRefs refs;
-        if (P.split) refs = SobbRefs{P.pos_slot, P.perm, P.tbox};
+        if (P.split) refs = SobbRefs{P.slot_pos, P.perm, P.tbox};
         st = sobb_enqueue(P.child, P.nlo, P.nhi, P.parent, P.leaf_start_of, P.owner_leaf, P.tris, P.nodes, P.rev_flags,
                           (int)N, (int)K, P.L, d0.kdop_size, P.sobb, refs, P.snodes, stream, P.d_err);
         if (st != DIPL_OK) return st;

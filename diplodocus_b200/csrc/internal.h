@@ -191,10 +191,10 @@ struct SobbScratch {
     unsigned* arrivals = nullptr;
     int triples = 0;
 };
-// Pre-split builds: per sorted position its slot in the leaf triangle array, the sorted order of the references
+// Pre-split builds: per slot of the leaf triangle array its sorted position, the sorted order of the references
 // and every reference's box (all NULL without pre-splitting).
 struct SobbRefs {
-    const int* pos_slot = nullptr;
+    const int* slot_pos = nullptr;
     const uint32_t* perm = nullptr;
     const float4* rbox = nullptr;
 };

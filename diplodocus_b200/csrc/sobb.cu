@@ -129,55 +129,56 @@ __device__ __forceinline__ void empty_kdop(Kdop& k) {
 
 // k-DOP of a final leaf from its triangles, then up the tree: the second arriver at a parent merges. All 16
 // table directions are always projected (a smaller kdop_size only restricts which triples the node kernel
-// considers), so the k-DOP never leaves registers.
+// considers), so the k-DOP never leaves registers. In a pre-split build a reference bounds only the part of its
+// triangle inside the reference's box, so each slot's triangle k-DOP is first intersected with the k-DOP of its
+// reference's box (each interval of the intersection holds the projections of every point of the triangle inside
+// the box; an interval that rounding leaves empty keeps the triangle's), then merged into the leaf's.
 __global__ void __launch_bounds__(256) kdop_refit_kernel(SobbIn S, const int* __restrict__ owner_leaf,
-                                                         Kdop* __restrict__ kdop, float* __restrict__ mag,
-                                                         unsigned* __restrict__ arrivals, const uint32_t* err) {
+                                                         SobbRefs refs, Kdop* __restrict__ kdop,
+                                                         float* __restrict__ mag, unsigned* __restrict__ arrivals,
+                                                         const uint32_t* err) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= S.N || *err != 0u) return;
     int x = owner_leaf[p];
     if (x < 0) return;
     const int cnt = scount(S, x);
-    const float4* t = S.btris + 3 * (long long)S.leaf_start_of[x];
+    const int start = S.leaf_start_of[x];
+    const float4* t = S.btris + 3 * (long long)start;
     Kdop k;
     float m = 0.0f;
     empty_kdop(k);
-    for (int tr = 0; tr < cnt; ++tr) tri_kdop(t + 3 * tr, k, m);
+    for (int tr = 0; tr < cnt; ++tr) {
+        const float4 q0 = __ldg(t + 3 * tr), q1 = __ldg(t + 3 * tr + 1), q2 = __ldg(t + 3 * tr + 2);
+        // a triangle with a non-finite coordinate is never hit: it adds nothing
+        if (!(isfinite(q0.x) && isfinite(q0.y) && isfinite(q0.z) && isfinite(q1.x) && isfinite(q1.y) &&
+              isfinite(q1.z) && isfinite(q2.x) && isfinite(q2.y) && isfinite(q2.z)))
+            continue;
+        m = fmaxf(m, fmaxf(fmaxf(fmaxf(fabsf(q0.x), fabsf(q0.y)), fmaxf(fabsf(q0.z), fabsf(q1.x))),
+                           fmaxf(fmaxf(fabsf(q1.y), fabsf(q1.z)), fmaxf(fmaxf(fabsf(q2.x), fabsf(q2.y)), fabsf(q2.z)))));
+        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+        if (refs.slot_pos) {
+            const long long r = refs.perm[refs.slot_pos[start + tr]];
+            lo = __ldg(refs.rbox + 2 * r), hi = __ldg(refs.rbox + 2 * r + 1);
+        }
+#pragma unroll
+        for (int i = 0; i < kDirs; ++i) {
+            const float d0 = proj(i, q0.x, q0.y, q0.z), d1 = proj(i, q1.x, q1.y, q1.z), d2 = proj(i, q2.x, q2.y, q2.z);
+            float tl = fminf(fminf(d0, d1), d2), th = fmaxf(fmaxf(d0, d1), d2);
+            if (refs.slot_pos) {
+                const float bl = proj(i, c_dir[i][0] >= 0.0f ? lo.x : hi.x, c_dir[i][1] >= 0.0f ? lo.y : hi.y,
+                                      c_dir[i][2] >= 0.0f ? lo.z : hi.z);
+                const float bh = proj(i, c_dir[i][0] >= 0.0f ? hi.x : lo.x, c_dir[i][1] >= 0.0f ? hi.y : lo.y,
+                                      c_dir[i][2] >= 0.0f ? hi.z : lo.z);
+                const float nl = fmaxf(tl, bl), nh = fminf(th, bh);
+                if (nl <= nh) tl = nl, th = nh;
+            }
+            k.lo[i] = fminf(k.lo[i], tl);
+            k.hi[i] = fmaxf(k.hi[i], th);
+        }
+    }
     store_kdop(kdop + x, k);
     mag[x] = m;
     kdop_ascend(S, x, k, m, kdop, mag, arrivals);
-}
-
-// Pre-split builds: a reference bounds only the part of its triangle inside the reference's box, so every sorted
-// position starts with the intersection of its triangle's k-DOP and the k-DOP of its box (each interval of the
-// intersection holds the projections of every point of the triangle inside the box; an interval that rounding
-// leaves empty keeps the triangle's), and the tree is merged upwards from the positions.
-__global__ void __launch_bounds__(256) kdop_refit_refs_kernel(SobbIn S, const int* __restrict__ pos_slot,
-                                                              const uint32_t* __restrict__ perm,
-                                                              const float4* __restrict__ rbox, Kdop* __restrict__ kdop,
-                                                              float* __restrict__ mag, unsigned* __restrict__ arrivals,
-                                                              const uint32_t* err) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= S.N || *err != 0u) return;
-    Kdop k;
-    float m = 0.0f;
-    empty_kdop(k);
-    tri_kdop(S.btris + 3 * (long long)pos_slot[p], k, m);
-    const long long r = perm[p];
-    const float4 lo = __ldg(rbox + 2 * r), hi = __ldg(rbox + 2 * r + 1);
-#pragma unroll
-    for (int i = 0; i < kDirs; ++i) {
-        if (!(k.lo[i] <= k.hi[i])) continue;  // an empty (never hit) triangle stays empty
-        const float bl = proj(i, c_dir[i][0] >= 0.0f ? lo.x : hi.x, c_dir[i][1] >= 0.0f ? lo.y : hi.y,
-                              c_dir[i][2] >= 0.0f ? lo.z : hi.z);
-        const float bh = proj(i, c_dir[i][0] >= 0.0f ? hi.x : lo.x, c_dir[i][1] >= 0.0f ? hi.y : lo.y,
-                              c_dir[i][2] >= 0.0f ? hi.z : lo.z);
-        const float nl = fmaxf(k.lo[i], bl), nh = fminf(k.hi[i], bh);
-        if (nl <= nh) k.lo[i] = nl, k.hi[i] = nh;
-    }
-    store_kdop(kdop + p, k);
-    mag[p] = m;
-    kdop_ascend(S, p, k, m, kdop, mag, arrivals);
 }
 
 // One warp per inner node of the final layout, one half-warp per child; lane l of a half holds the child's
@@ -755,11 +756,8 @@ dipl_status sobb_enqueue(const int4* child, const float4* node_lo, const float4*
     Kdop* kdop = static_cast<Kdop*>(sc.kdop);
     DIPL_CUDA(cudaMemsetAsync(sc.arrivals, 0, sizeof(unsigned) * Kalloc, s));
     SobbIn S{child, node_lo, node_hi, parent, leaf_start_of, btris, N, L, kdop_size / 2};
-    if (refs.pos_slot)
-        kdop_refit_refs_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, refs.pos_slot, refs.perm, refs.rbox,
-                                                                           kdop, sc.mag, sc.arrivals, d_err);
-    else
-        kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, kdop, sc.mag, sc.arrivals, d_err);
+    kdop_refit_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(S, owner_leaf, refs, kdop, sc.mag, sc.arrivals,
+                                                                  d_err);
     note_launches();
     if (K > 0) {
         // persistent: each CTA stages the triple table once, then its warps stride over the nodes

@@ -23,7 +23,6 @@ constexpr int kTraceThreads = 128;
 // Resident blocks per SM the kernel is compiled for: 9 x 128 threads at <= 56 registers. Builds with more
 // registers and 8 blocks per SM measured up to 1.5x slower on the 16M-triangle soup.
 constexpr int kTraceMinBlocks = 9;
-constexpr bool kInterleave = true;
 constexpr float kSlabWiden = 1e-6f;
 constexpr float kPruneSlack = 1e-5f;
 
@@ -101,7 +100,7 @@ struct Stack {
     }
 };
 
-// Long rays of a warp whose chunk is handed out move to tail_kernel: once at most kTailLanes lanes of the warp
+// Long rays of a warp that has no rays left to take move to tail_kernel: once at most kTailLanes lanes of the warp
 // are still tracing, a lane whose ray has taken kTailSteps steps or more writes the ray's state (ray index, next
 // node, best hit so far, stack) to a slot and takes no more work; tail_kernel then traverses each such ray with a
 // whole warp. Without it the warp keeps issuing one-lane steps until its longest ray ends (the 1M sphere's
@@ -113,7 +112,7 @@ constexpr int kTailSteps = 64;
 constexpr int kTailLanes = 8;  // ... and only when at most this many lanes of the warp are still tracing
 constexpr int kTailHeaderInts = 12;  // ray (2), cur, sp, best t/u/v, prim, found, pad
 constexpr size_t kTailBytes = 64u << 20;  // slot storage per trace call, at most
-// Batches smaller than this trace without the offload: their warps hand out their chunks early, the rays of
+// Batches smaller than this trace without the offload: their warps run out of rays early, the rays of
 // such batches are mostly short (a 512x512 frame of the small scene), and the offload's allocation, clearing
 // and extra launch cost more there (0.243 against 0.279-0.289 ms per frame of two traces).
 constexpr int64_t kTailMinRays = 1 << 19;
@@ -153,7 +152,7 @@ template <int LEAF, bool ANY, bool COUNT, int STACK, int SHORT>
 __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(const BNode* __restrict__ nodes,
                                                               const float4* __restrict__ tris, int root,
                                                               int num_nodes, const dipl_ray* __restrict__ rays,
-                                                              int64_t n, int64_t chunk, dipl_hit* __restrict__ hits,
+                                                              int64_t n, dipl_hit* __restrict__ hits,
                                                               uint8_t* __restrict__ occluded, uint32_t flags,
                                                               unsigned long long* __restrict__ counters,
                                                               uint32_t* __restrict__ err, TailQueue tq,
@@ -161,15 +160,12 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
     __shared__ int2 sh_stack[SHORT > 0 ? SHORT * kTraceThreads : 1];
     const int lane = threadIdx.x & 31;
     const int64_t warp_id = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    // The k-th ray a warp takes: with kInterleave at position ((k / 32) * warps + warp) * 32 + k % 32 of the work
-    // order, so all warps walk the order together and the rays in flight are one window of it (a coherent order
-    // then keeps the whole GPU in one region of the tree); else k positions into the warp's own chunk.
+    // The k-th ray a warp takes is at position ((k / 32) * warps + warp) * 32 + k % 32 of the work order, so all
+    // warps walk the order together and the rays in flight are one window of it (a coherent order then keeps the
+    // whole GPU in one region of the tree; one chunk per warp measured 181 against 163 ms on the pre-split soup).
     const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t beg = warp_id * chunk;
-    const int64_t end = kInterleave ? n : min(n, beg + chunk);
-    auto position = [&](int64_t k) -> int64_t {
-        return kInterleave ? (((k >> 5) * warps + warp_id) << 5) + (k & 31) : beg + k;
-    };
+    const int64_t end = n;
+    auto position = [&](int64_t k) -> int64_t { return (((k >> 5) * warps + warp_id) << 5) + (k & 31); };
     const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
     const uint32_t lt_mask = lanemask_lt();
     const uint32_t step_limit = tq.step_limit;
@@ -188,7 +184,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
     bool bad = false;
     bool may_offload = tq.min_steps > 0;
     for (;;) {
-        // ---- refill idle lanes from the chunk --------------------------------------------------------
+        // ---- refill idle lanes ---------------------------------------------------------------------
         const bool idle = my < 0;
         const uint32_t idle_mask = __ballot_sync(0xffffffffu, idle);
         if (idle_mask) {
@@ -297,7 +293,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(c
             my = -1;
         } else if (may_offload && position(next) >= end && steps >= (uint32_t)tq.min_steps &&
                    __popc(active_mask) <= tq.max_lanes) {
-            // the chunk is handed out and this ray is still going: hand it to tail_kernel if a slot is free
+            // the warp has no rays left and this ray is still going: hand it to tail_kernel if a slot is free
             const unsigned slot = atomicAdd(&tq.count[0], 1u);
             if (slot < (unsigned)tq.cap) {
                 int* w = tq.slots + (size_t)slot * tq.slot_ints;
@@ -501,8 +497,8 @@ __global__ void __launch_bounds__(kTraceThreads) tail_kernel(const BNode* __rest
 
 // ---- ray order ----------------------------------------------------------------------------------------
 // On request, batches of at least kReorderMinRays rays are traced in the order of a 30-bit key: the direction's octant
-// above a 9-bit-per-axis Morton code of the origin within the batch's origin bounds. A warp's chunk of rays then
-// starts in one small region and heads the same way, so its lanes fetch the same nodes and branch alike.
+// above a 9-bit-per-axis Morton code of the origin within the batch's origin bounds. A warp's 32 rays then
+// start in one small region and head the same way, so its lanes fetch the same nodes and branch alike.
 // Records still go to each ray's own index; only the order of work changes, never a result.
 constexpr int kReorderBits = 30;
 
@@ -588,8 +584,6 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
     const int64_t warps_needed = (n + 31) / 32;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(max_grid, (warps_needed * 32 + kTraceThreads - 1) /
                                                                                kTraceThreads));
-    const int64_t warps = grid * (kTraceThreads / 32);
-    const int64_t chunk = (n + warps - 1) / warps;
     const int num_nodes = b->num_triangles == 0 ? -1 : (int)b->node_capacity;
     if ((reinterpret_cast<uintptr_t>(b->nodes) & 63) != 0) {
         set_last_error("trace: node array is not 64-byte aligned");
@@ -626,7 +620,7 @@ dipl_status launch_trace(const dipl_bvh* b, const dipl_ray* rays, int64_t n, dip
         }
     }
     kernel<<<(unsigned)grid, kTraceThreads, 0, s>>>(static_cast<const BNode*>(b->nodes), b->tris, b->root, num_nodes,
-                                                   rays, n, chunk, hits, occ, flags, counters, b->d_err, tq,
+                                                   rays, n, hits, occ, flags, counters, b->d_err, tq,
                                                    ro.order);
     note_launches();
     cudaError_t e = cudaGetLastError();
