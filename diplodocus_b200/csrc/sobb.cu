@@ -103,25 +103,6 @@ __device__ __forceinline__ void kdop_ascend(const SobbIn& S, int x, Kdop& k, flo
     }
 }
 
-// k-DOP of one triangle (empty for a triangle with a non-finite coordinate: it is never hit) and the largest
-// magnitude of its coordinates folded into m.
-__device__ __forceinline__ void tri_kdop(const float4* __restrict__ t, Kdop& k, float& m) {
-    const float4 q0 = __ldg(t), q1 = __ldg(t + 1), q2 = __ldg(t + 2);
-    if (!(isfinite(q0.x) && isfinite(q0.y) && isfinite(q0.z) && isfinite(q1.x) && isfinite(q1.y) && isfinite(q1.z) &&
-          isfinite(q2.x) && isfinite(q2.y) && isfinite(q2.z)))
-        return;
-    for (int v = 0; v < 3; ++v) {
-        const float4 q = v == 0 ? q0 : (v == 1 ? q1 : q2);
-        m = fmaxf(m, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
-#pragma unroll
-        for (int i = 0; i < kDirs; ++i) {
-            const float d = proj(i, q.x, q.y, q.z);
-            k.lo[i] = fminf(k.lo[i], d);
-            k.hi[i] = fmaxf(k.hi[i], d);
-        }
-    }
-}
-
 __device__ __forceinline__ void empty_kdop(Kdop& k) {
 #pragma unroll
     for (int i = 0; i < kDirs; ++i) k.lo[i] = __int_as_float(0x7F800000), k.hi[i] = __int_as_float(0xFF800000);
@@ -309,6 +290,52 @@ __device__ __forceinline__ float sleaf_test(float3 a, float3 b, float3 c, float3
     return wt_test(a, b, c, o, w, backface, b1, b2);
 }
 
+// The ray's record per table direction, in its shared-memory column: projected origin, reciprocal projected
+// direction, and the two widening terms (the rounding of the projected origin as a distance along the ray,
+// absolute, and of the projected direction as a relative error of every distance on this slab, large for grazing
+// slabs), so a slab costs one shared load.
+__device__ __forceinline__ void sobb_ray_setup(float4 (*s_ray)[kSThreads], int tid, int dirs, float3 o, float3 d) {
+    const float omag = fabsf(o.x) + fabsf(o.y) + fabsf(o.z);
+    const float dmag = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+    for (int k = 0; k < dirs; ++k) {
+        const float dk = proj(k, d.x, d.y, d.z);
+        const float inv = __frcp_rn(fabsf(dk) < 1e-20f ? copysignf(1e-20f, dk) : dk);
+        s_ray[k][tid] = make_float4(proj(k, o.x, o.y, o.z), inv, omag * 4.0e-7f * fabsf(inv),
+                                    kSSlabWiden + dmag * 4.0e-7f * fabsf(inv));
+    }
+}
+
+// Entry distance of the ray into one child's three slabs (directions packed in `axes`, one per byte), widened by
+// the ray's rounding terms; +inf when the slabs are missed, end before tmin or start beyond lim.
+__device__ __forceinline__ float sobb_slab_box(const float4 (*s_ray)[kSThreads], int tid, int axes, float l0, float h0,
+                                               float l1, float h1, float l2, float h2, float tmin, float lim) {
+    float tn = __int_as_float(0xFF800000), tf = __int_as_float(0x7F800000);
+    const float ls[3] = {l0, l1, l2}, hs[3] = {h0, h1, h2};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const int k = (axes >> (8 * j)) & 0xFF;
+        const float4 q = s_ray[k][tid];
+        const float ok = q.x, inv = q.y, tol = q.z, rel = q.w;
+        const float t0 = __fmul_rn(__fsub_rn(ls[j], ok), inv), t1 = __fmul_rn(__fsub_rn(hs[j], ok), inv);
+        const float a0 = fminf(t0, t1), a1 = fmaxf(t0, t1);
+        tn = fmaxf(tn, a0 - fabsf(a0) * rel - tol);
+        tf = fminf(tf, a1 + fabsf(a1) * rel + tol);
+    }
+    return (tn <= tf && tf >= tmin && tn <= lim) ? tn : __int_as_float(0x7F800000);
+}
+
+// One SOBB node: both children's entry distances (t0, t1; +inf when missed) and their references (dd.x, dd.y).
+__device__ __forceinline__ int4 sobb_children(const SNode* __restrict__ nodes, int cur,
+                                              const float4 (*s_ray)[kSThreads], int tid, float tmin, float lim,
+                                              float& t0, float& t1) {
+    const float4* np = reinterpret_cast<const float4*>(nodes + cur);
+    const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+    const int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
+    t0 = sobb_slab_box(s_ray, tid, dd.z, a.x, a.y, a.z, a.w, b.x, b.y, tmin, lim);
+    t1 = sobb_slab_box(s_ray, tid, dd.w, b.z, b.w, c.x, c.y, c.z, c.w, tmin, lim);
+    return dd;
+}
+
 template <int LEAF, bool ANY, bool COUNT, int STACK>
 __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __restrict__ nodes,
                                                                const float4* __restrict__ tris, int root,
@@ -318,9 +345,7 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
                                                                unsigned long long* __restrict__ counters,
                                                                uint32_t* __restrict__ err, uint32_t step_limit,
                                                                const uint32_t* __restrict__ order) {
-    // per table direction: the ray's projected origin, reciprocal projected direction, and the two widening terms,
-    // one 16-byte record per (direction, thread) so a slab costs one shared load
-    __shared__ float4 s_ray[kDirs][kSThreads];
+    __shared__ float4 s_ray[kDirs][kSThreads];  // the rays' records per direction (sobb_ray_setup)
     const int64_t work = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // position in the work order
     unsigned visits = 0, tests = 0;
     if (work < n) {
@@ -330,16 +355,7 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
         const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
         const float3 o = make_float3(ra.x, ra.y, ra.z), d = make_float3(rb.x, rb.y, rb.z);
         const float tmin = ra.w, tmax = rb.w;
-        const float omag = fabsf(o.x) + fabsf(o.y) + fabsf(o.z);
-        const float dmag = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
-        for (int k = 0; k < dirs; ++k) {
-            const float dk = proj(k, d.x, d.y, d.z);
-            const float inv = __frcp_rn(fabsf(dk) < 1e-20f ? copysignf(1e-20f, dk) : dk);
-            // rounding of the projected origin as a distance along the ray (absolute), and of the projected
-            // direction as a relative error of every distance on this slab (large for grazing slabs)
-            s_ray[k][tid] = make_float4(proj(k, o.x, o.y, o.z), inv, omag * 4.0e-7f * fabsf(inv),
-                                        kSSlabWiden + dmag * 4.0e-7f * fabsf(inv));
-        }
+        sobb_ray_setup(s_ray, tid, dirs, o, d);
         const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
         WtRay w{};
         if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(d);
@@ -351,21 +367,6 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
         int sp = 0;
         int cur = num_nodes >= 0 ? root : 0x7FFFFFFF;
         uint32_t steps = 0;
-        auto slab_box = [&](int axes, float l0, float h0, float l1, float h1, float l2, float h2, float lim) {
-            float tn = __int_as_float(0xFF800000), tf = __int_as_float(0x7F800000);
-            const float ls[3] = {l0, l1, l2}, hs[3] = {h0, h1, h2};
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int k = (axes >> (8 * j)) & 0xFF;
-                const float4 q = s_ray[k][tid];
-                const float ok = q.x, inv = q.y, tol = q.z, rel = q.w;
-                const float t0 = __fmul_rn(__fsub_rn(ls[j], ok), inv), t1 = __fmul_rn(__fsub_rn(hs[j], ok), inv);
-                const float a0 = fminf(t0, t1), a1 = fmaxf(t0, t1);
-                tn = fmaxf(tn, a0 - fabsf(a0) * rel - tol);
-                tf = fminf(tf, a1 + fabsf(a1) * rel + tol);
-            }
-            return (tn <= tf && tf >= tmin && tn <= lim) ? tn : __int_as_float(0x7F800000);
-        };
         while (cur != 0x7FFFFFFF) {
             if (++steps > step_limit) {
                 bad = true;
@@ -376,13 +377,10 @@ __global__ void __launch_bounds__(kSThreads) sobb_trace_kernel(const SNode* __re
                     bad = true;
                     break;
                 }
-                const float4* np = reinterpret_cast<const float4*>(nodes + cur);
-                const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
-                const int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
                 if (COUNT) ++visits;
-                const float lim = best_t + fabsf(best_t) * kSPruneSlack;
-                const float t0 = slab_box(dd.z, a.x, a.y, a.z, a.w, b.x, b.y, lim);
-                const float t1 = slab_box(dd.w, b.z, b.w, c.x, c.y, c.z, c.w, lim);
+                float t0, t1;
+                const int4 dd = sobb_children(nodes, cur, s_ray, tid, tmin, best_t + fabsf(best_t) * kSPruneSlack,
+                                              t0, t1);
                 const bool h0 = t0 != __int_as_float(0x7F800000), h1 = t1 != __int_as_float(0x7F800000);
                 if (h0 && h1) {
                     const bool first0 = t0 <= t1;
@@ -496,21 +494,6 @@ __global__ void __launch_bounds__(kSThreads) sobb_persist_kernel(const SNode* __
     int sp = 0;
     int cur = kDone;
     uint32_t steps = 0;
-    auto slab_box = [&](int axes, float l0, float h0, float l1, float h1, float l2, float h2, float lim) {
-        float tn = __int_as_float(0xFF800000), tf = __int_as_float(0x7F800000);
-        const float ls[3] = {l0, l1, l2}, hs[3] = {h0, h1, h2};
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const int k = (axes >> (8 * j)) & 0xFF;
-            const float4 q = s_ray[k][tid];
-            const float ok = q.x, inv = q.y, tol = q.z, rel = q.w;
-            const float t0 = __fmul_rn(__fsub_rn(ls[j], ok), inv), t1 = __fmul_rn(__fsub_rn(hs[j], ok), inv);
-            const float a0 = fminf(t0, t1), a1 = fmaxf(t0, t1);
-            tn = fmaxf(tn, a0 - fabsf(a0) * rel - tol);
-            tf = fminf(tf, a1 + fabsf(a1) * rel + tol);
-        }
-        return (tn <= tf && tf >= tmin && tn <= lim) ? tn : __int_as_float(0x7F800000);
-    };
     for (;;) {
         // ---- refill idle lanes --------------------------------------------------------------------------
         const bool idle = my < 0;
@@ -526,14 +509,7 @@ __global__ void __launch_bounds__(kSThreads) sobb_persist_kernel(const SNode* __
                     d = make_float3(rb.x, rb.y, rb.z);
                     tmin = ra.w;
                     tmax = rb.w;
-                    const float omag = fabsf(o.x) + fabsf(o.y) + fabsf(o.z);
-                    const float dmag = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
-                    for (int k = 0; k < dirs; ++k) {
-                        const float dk = proj(k, d.x, d.y, d.z);
-                        const float inv = __frcp_rn(fabsf(dk) < 1e-20f ? copysignf(1e-20f, dk) : dk);
-                        s_ray[k][tid] = make_float4(proj(k, o.x, o.y, o.z), inv, omag * 4.0e-7f * fabsf(inv),
-                                                    kSSlabWiden + dmag * 4.0e-7f * fabsf(inv));
-                    }
+                    sobb_ray_setup(s_ray, tid, dirs, o, d);
                     if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(d);
                     best_t = tmax, best_u = 0.0f, best_v = 0.0f, best_prim = -1, found = false;
                     sp = 0;
@@ -554,13 +530,9 @@ __global__ void __launch_bounds__(kSThreads) sobb_persist_kernel(const SNode* __
             bad = true;  // only a corrupted tree gets here
             finished = true;
         } else if (cur >= 0) {
-            const float4* np = reinterpret_cast<const float4*>(nodes + cur);
-            const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
-            const int4 dd = __ldg(reinterpret_cast<const int4*>(np + 3));
             if (COUNT) ++visits;
-            const float lim = best_t + fabsf(best_t) * kSPruneSlack;
-            const float t0 = slab_box(dd.z, a.x, a.y, a.z, a.w, b.x, b.y, lim);
-            const float t1 = slab_box(dd.w, b.z, b.w, c.x, c.y, c.z, c.w, lim);
+            float t0, t1;
+            const int4 dd = sobb_children(nodes, cur, s_ray, tid, tmin, best_t + fabsf(best_t) * kSPruneSlack, t0, t1);
             const bool h0 = t0 != __int_as_float(0x7F800000), h1 = t1 != __int_as_float(0x7F800000);
             if (h0 && h1) {
                 const bool first0 = t0 <= t1;

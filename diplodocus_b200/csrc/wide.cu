@@ -292,6 +292,98 @@ __device__ __forceinline__ float wleaf_test(float3 a, float3 b, float3 c, const 
     return wt_test(a, b, c, r.o, w, backface, b1, b2);
 }
 
+// A ray of the 8-wide traversal (1/direction rounded to nearest) and its octant bits: slot s lies towards
+// (s&1 ? +x : -x, ...), so a ray going -x meets the +x children first.
+__device__ __forceinline__ WRay wide_load_ray(const dipl_ray* __restrict__ rays, int64_t i, uint32_t& oct) {
+    const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * i;
+    const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
+    WRay r;
+    r.o = make_float3(ra.x, ra.y, ra.z);
+    r.d = make_float3(rb.x, rb.y, rb.z);
+    r.tmin = ra.w;
+    r.tmax = rb.w;
+    auto safe = [](float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; };
+    r.inv = make_float3(__frcp_rn(safe(r.d.x)), __frcp_rn(safe(r.d.y)), __frcp_rn(safe(r.d.z)));
+    oct = (r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u);
+    return r;
+}
+
+// The children of one wide node that the ray enters before `lim`: inner children as bits in visiting order
+// (bit slot ^ octant), and the triangles of the hit leaf slots as bits over the node's triangle range.
+struct WideHits {
+    uint32_t inner, tris, imask;
+    int child_base, tri_base;
+};
+
+__device__ __forceinline__ WideHits wide_node_hits(const WNode* __restrict__ nodes, int node, const WRay& r,
+                                                   uint32_t oct, float lim) {
+    const float4* np = reinterpret_cast<const float4*>(nodes + node);
+    const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2), f3 = __ldg(np + 3), f4 = __ldg(np + 4);
+    const uint32_t eb = __float_as_uint(f0.w);
+    const float sx = __uint_as_float((eb & 0xFFu) << 23), sy = __uint_as_float(((eb >> 8) & 0xFFu) << 23),
+                sz = __uint_as_float(((eb >> 16) & 0xFFu) << 23);
+    WideHits h;
+    h.imask = eb >> 24;
+    h.child_base = __float_as_int(f1.x);
+    h.tri_base = __float_as_int(f1.y);
+    h.inner = 0u;
+    h.tris = 0u;
+    const uint32_t meta_lo = __float_as_uint(f1.z), meta_hi = __float_as_uint(f1.w);
+    const uint32_t qw[12] = {__float_as_uint(f2.x), __float_as_uint(f2.y), __float_as_uint(f2.z), __float_as_uint(f2.w),
+                             __float_as_uint(f3.x), __float_as_uint(f3.y), __float_as_uint(f3.z), __float_as_uint(f3.w),
+                             __float_as_uint(f4.x), __float_as_uint(f4.y), __float_as_uint(f4.z), __float_as_uint(f4.w)};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t meta = ((k < 4 ? meta_lo : meta_hi) >> (8 * (k & 3))) & 0xFFu;
+        const bool inner = (h.imask >> k) & 1u;
+        if (!inner && meta == 0u) continue;
+        auto qb = [&](int arr) { return (float)((qw[2 * arr + (k >> 2)] >> (8 * (k & 3))) & 0xFFu); };
+        const float lx = __fmaf_rn(qb(0), sx, f0.x), ly = __fmaf_rn(qb(1), sy, f0.y), lz = __fmaf_rn(qb(2), sz, f0.z);
+        const float hx = __fmaf_rn(qb(3), sx, f0.x), hy = __fmaf_rn(qb(4), sy, f0.y), hz = __fmaf_rn(qb(5), sz, f0.z);
+        const float tx0 = __fmul_rn(__fsub_rn(lx, r.o.x), r.inv.x), tx1 = __fmul_rn(__fsub_rn(hx, r.o.x), r.inv.x);
+        const float ty0 = __fmul_rn(__fsub_rn(ly, r.o.y), r.inv.y), ty1 = __fmul_rn(__fsub_rn(hy, r.o.y), r.inv.y);
+        const float tz0 = __fmul_rn(__fsub_rn(lz, r.o.z), r.inv.z), tz1 = __fmul_rn(__fsub_rn(hz, r.o.z), r.inv.z);
+        float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+        float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+        tn = tn - fabsf(tn) * kWSlabWiden;
+        tf = tf + fabsf(tf) * kWSlabWiden;
+        if (!(tn <= tf && tf >= r.tmin && tn <= lim)) continue;
+        if (inner) h.inner |= 1u << (k ^ oct);
+        else h.tris |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+    }
+    return h;
+}
+
+// After a visit: the first inner child hit is next, the others go on the stack as one group (child base, inner
+// mask, remaining hits). False when the stack is full.
+template <int STACK>
+__device__ __forceinline__ bool wide_descend(const WideHits& h, uint32_t oct, int& node, int2* stack, int& sp) {
+    node = -1;
+    if (!h.inner) return true;
+    uint32_t hits = h.inner;
+    const int b = __ffs(hits) - 1;
+    hits &= hits - 1u;
+    node = h.child_base + __popc(h.imask & ((1u << ((uint32_t)b ^ oct)) - 1u));
+    if (!hits) return true;
+    if (sp >= STACK) return false;
+    stack[sp++] = make_int2(h.child_base, (int)((hits << 8) | h.imask));
+    return true;
+}
+
+// The next child of the top group (the group leaves the stack with its last child), -1 on an empty stack.
+__device__ __forceinline__ int wide_pop(int2* stack, int& sp, uint32_t oct) {
+    if (sp == 0) return -1;
+    const int2 e = stack[sp - 1];
+    uint32_t gh = (uint32_t)e.y >> 8;
+    const uint32_t gi = (uint32_t)e.y & 0xFFu;
+    const int b = __ffs(gh) - 1;
+    gh &= gh - 1u;
+    const int next = e.x + __popc(gi & ((1u << ((uint32_t)b ^ oct)) - 1u));
+    if (gh) stack[sp - 1].y = (int)((gh << 8) | gi);
+    else --sp;
+    return next;
+}
+
 // One thread per ray in the work order, blocks launched in order: at any time the GPU traces one window of the
 // order, and a warp's lanes start their rays together. Used for rays in the coherent order, where keeping the
 // lanes of a warp on neighbouring rays matters more than not waiting for a warp's longest ray (16M-ray pre-split
@@ -306,17 +398,8 @@ __global__ void __launch_bounds__(kWTraceThreads) wide_block_kernel(
     unsigned visits = 0, tests = 0;
     if (work < n) {
         const int64_t i = order ? (int64_t)__ldg(order + work) : work;  // the ray's own index
-        const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * i;
-        const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
-        WRay r;
-        r.o = make_float3(ra.x, ra.y, ra.z);
-        r.d = make_float3(rb.x, rb.y, rb.z);
-        r.tmin = ra.w;
-        r.tmax = rb.w;
-        auto safe = [](float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; };
-        r.inv = make_float3(__frcp_rn(safe(r.d.x)), __frcp_rn(safe(r.d.y)), __frcp_rn(safe(r.d.z)));
-        // slot s lies towards (s&1 ? +x : -x, ...): a ray going -x meets the +x children first
-        const uint32_t oct = (r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u);
+        uint32_t oct = 0;
+        const WRay r = wide_load_ray(rays, i, oct);
         const bool backface = (flags & DIPL_TRACE_BACKFACE_CULLING) != 0u;
         WtRay w{};
         if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(r.d);
@@ -359,75 +442,20 @@ __global__ void __launch_bounds__(kWTraceThreads) wide_block_kernel(
                     bad = true;
                     break;
                 }
-                const float4* np = reinterpret_cast<const float4*>(nodes + node);
-                const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2), f3 = __ldg(np + 3),
-                             f4 = __ldg(np + 4);
                 if (COUNT) ++visits;
-                const uint32_t eb = __float_as_uint(f0.w);
-                const float sx = __uint_as_float((eb & 0xFFu) << 23), sy = __uint_as_float(((eb >> 8) & 0xFFu) << 23),
-                            sz = __uint_as_float(((eb >> 16) & 0xFFu) << 23);
-                const uint32_t imask = eb >> 24;
-                const int child_base = __float_as_int(f1.x), tri_base = __float_as_int(f1.y);
-                const uint32_t meta_lo = __float_as_uint(f1.z), meta_hi = __float_as_uint(f1.w);
-                const uint32_t qw[12] = {__float_as_uint(f2.x), __float_as_uint(f2.y), __float_as_uint(f2.z),
-                                         __float_as_uint(f2.w), __float_as_uint(f3.x), __float_as_uint(f3.y),
-                                         __float_as_uint(f3.z), __float_as_uint(f3.w), __float_as_uint(f4.x),
-                                         __float_as_uint(f4.y), __float_as_uint(f4.z), __float_as_uint(f4.w)};
-                const float lim = best_t + fabsf(best_t) * kWPruneSlack;
-                uint32_t inner_hits = 0, tri_mask = 0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const uint32_t meta = ((k < 4 ? meta_lo : meta_hi) >> (8 * (k & 3))) & 0xFFu;
-                    const bool inner = (imask >> k) & 1u;
-                    if (!inner && meta == 0u) continue;
-                    auto qb = [&](int arr) { return (float)((qw[2 * arr + (k >> 2)] >> (8 * (k & 3))) & 0xFFu); };
-                    const float lx = __fmaf_rn(qb(0), sx, f0.x), ly = __fmaf_rn(qb(1), sy, f0.y),
-                                lz = __fmaf_rn(qb(2), sz, f0.z);
-                    const float hx = __fmaf_rn(qb(3), sx, f0.x), hy = __fmaf_rn(qb(4), sy, f0.y),
-                                hz = __fmaf_rn(qb(5), sz, f0.z);
-                    const float tx0 = __fmul_rn(__fsub_rn(lx, r.o.x), r.inv.x), tx1 = __fmul_rn(__fsub_rn(hx, r.o.x), r.inv.x);
-                    const float ty0 = __fmul_rn(__fsub_rn(ly, r.o.y), r.inv.y), ty1 = __fmul_rn(__fsub_rn(hy, r.o.y), r.inv.y);
-                    const float tz0 = __fmul_rn(__fsub_rn(lz, r.o.z), r.inv.z), tz1 = __fmul_rn(__fsub_rn(hz, r.o.z), r.inv.z);
-                    float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
-                    float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
-                    tn = tn - fabsf(tn) * kWSlabWiden;
-                    tf = tf + fabsf(tf) * kWSlabWiden;
-                    if (!(tn <= tf && tf >= r.tmin && tn <= lim)) continue;
-                    if (inner) inner_hits |= 1u << (k ^ oct);
-                    else tri_mask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-                }
-                while (tri_mask) {
-                    const int b = __ffs(tri_mask) - 1;
-                    tri_mask &= tri_mask - 1u;
-                    test_tri(tri_base + b);
+                const WideHits h = wide_node_hits(nodes, node, r, oct, best_t + fabsf(best_t) * kWPruneSlack);
+                for (uint32_t tm = h.tris; tm; tm &= tm - 1u) {
+                    test_tri(h.tri_base + __ffs(tm) - 1);
                     if (ANY && found) break;
                 }
                 if (ANY && found) break;
-                node = -1;
-                if (inner_hits) {
-                    const int b = __ffs(inner_hits) - 1;
-                    inner_hits &= inner_hits - 1u;
-                    const uint32_t slot = (uint32_t)b ^ oct;
-                    node = child_base + __popc(imask & ((1u << slot) - 1u));
-                    if (inner_hits) {
-                        if (sp >= STACK) {
-                            bad = true;
-                            break;
-                        }
-                        stack[sp++] = make_int2(child_base, (int)((inner_hits << 8) | imask));
-                    }
+                if (!wide_descend<STACK>(h, oct, node, stack, sp)) {
+                    bad = true;
+                    break;
                 }
             } else {
-                if (sp == 0) break;
-                const int2 e = stack[sp - 1];
-                uint32_t gh = (uint32_t)e.y >> 8;
-                const uint32_t gi = (uint32_t)e.y & 0xFFu;
-                const int b = __ffs(gh) - 1;
-                gh &= gh - 1u;
-                const uint32_t slot = (uint32_t)b ^ oct;
-                node = e.x + __popc(gi & ((1u << slot) - 1u));
-                if (gh) stack[sp - 1].y = (int)((gh << 8) | gi);
-                else --sp;
+                node = wide_pop(stack, sp, oct);
+                if (node < 0) break;
             }
         }
         if (bad) atomicOr(err, kErrStack);
@@ -510,16 +538,7 @@ __global__ void __launch_bounds__(kWTraceThreads, kWTraceMinBlocks) wide_trace_k
                 const int64_t cand = position(next + __popc(idle_mask & lt_mask));
                 if (cand < n) {
                     my = order ? (int64_t)__ldg(order + cand) : cand;  // the ray's own index (hits go there)
-                    const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * my;
-                    const float4 ra = __ldg(r4), rb = __ldg(r4 + 1);
-                    r.o = make_float3(ra.x, ra.y, ra.z);
-                    r.d = make_float3(rb.x, rb.y, rb.z);
-                    r.tmin = ra.w;
-                    r.tmax = rb.w;
-                    auto safe = [](float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; };
-                    r.inv = make_float3(__frcp_rn(safe(r.d.x)), __frcp_rn(safe(r.d.y)), __frcp_rn(safe(r.d.z)));
-                    // slot s lies towards (s&1 ? +x : -x, ...): a ray going -x meets the +x children first
-                    oct = (r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u);
+                    r = wide_load_ray(rays, my, oct);
                     if (LEAF == DIPL_LEAF_WATERTIGHT) w = wt_setup(r.d);
                     best_t = r.tmax, best_u = 0.0f, best_v = 0.0f, best_prim = -1, found = false;
                     sp = 0;
@@ -549,81 +568,23 @@ __global__ void __launch_bounds__(kWTraceThreads, kWTraceMinBlocks) wide_trace_k
                 bad = true;
                 done = true;
             } else {
-                const float4* np = reinterpret_cast<const float4*>(nodes + node);
-                const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2), f3 = __ldg(np + 3),
-                             f4 = __ldg(np + 4);
                 if (COUNT) ++visits;
-                const uint32_t eb = __float_as_uint(f0.w);
-                const float sx = __uint_as_float((eb & 0xFFu) << 23), sy = __uint_as_float(((eb >> 8) & 0xFFu) << 23),
-                            sz = __uint_as_float(((eb >> 16) & 0xFFu) << 23);
-                const uint32_t imask = eb >> 24;
-                const int child_base = __float_as_int(f1.x), tri_base = __float_as_int(f1.y);
-                const uint32_t meta_lo = __float_as_uint(f1.z), meta_hi = __float_as_uint(f1.w);
-                const uint32_t qw[12] = {__float_as_uint(f2.x), __float_as_uint(f2.y), __float_as_uint(f2.z),
-                                         __float_as_uint(f2.w), __float_as_uint(f3.x), __float_as_uint(f3.y),
-                                         __float_as_uint(f3.z), __float_as_uint(f3.w), __float_as_uint(f4.x),
-                                         __float_as_uint(f4.y), __float_as_uint(f4.z), __float_as_uint(f4.w)};
-                const float lim = best_t + fabsf(best_t) * kWPruneSlack;
-                uint32_t inner_hits = 0, tri_mask = 0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const uint32_t meta = ((k < 4 ? meta_lo : meta_hi) >> (8 * (k & 3))) & 0xFFu;
-                    const bool inner = (imask >> k) & 1u;
-                    if (!inner && meta == 0u) continue;
-                    auto qb = [&](int arr) { return (float)((qw[2 * arr + (k >> 2)] >> (8 * (k & 3))) & 0xFFu); };
-                    const float lx = __fmaf_rn(qb(0), sx, f0.x), ly = __fmaf_rn(qb(1), sy, f0.y),
-                                lz = __fmaf_rn(qb(2), sz, f0.z);
-                    const float hx = __fmaf_rn(qb(3), sx, f0.x), hy = __fmaf_rn(qb(4), sy, f0.y),
-                                hz = __fmaf_rn(qb(5), sz, f0.z);
-                    const float tx0 = __fmul_rn(__fsub_rn(lx, r.o.x), r.inv.x), tx1 = __fmul_rn(__fsub_rn(hx, r.o.x), r.inv.x);
-                    const float ty0 = __fmul_rn(__fsub_rn(ly, r.o.y), r.inv.y), ty1 = __fmul_rn(__fsub_rn(hy, r.o.y), r.inv.y);
-                    const float tz0 = __fmul_rn(__fsub_rn(lz, r.o.z), r.inv.z), tz1 = __fmul_rn(__fsub_rn(hz, r.o.z), r.inv.z);
-                    float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
-                    float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
-                    tn = tn - fabsf(tn) * kWSlabWiden;
-                    tf = tf + fabsf(tf) * kWSlabWiden;
-                    if (!(tn <= tf && tf >= r.tmin && tn <= lim)) continue;
-                    if (inner) inner_hits |= 1u << (k ^ oct);
-                    else tri_mask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-                }
-                while (tri_mask) {
-                    const int bt = __ffs(tri_mask) - 1;
-                    tri_mask &= tri_mask - 1u;
-                    test_tri(tri_base + bt);
+                const WideHits h = wide_node_hits(nodes, node, r, oct, best_t + fabsf(best_t) * kWPruneSlack);
+                for (uint32_t tm = h.tris; tm; tm &= tm - 1u) {
+                    test_tri(h.tri_base + __ffs(tm) - 1);
                     if (ANY && found) break;
                 }
-                node = -1;
                 if (ANY && found) {
+                    node = -1;
                     done = true;
-                } else if (inner_hits) {
-                    const int bt = __ffs(inner_hits) - 1;
-                    inner_hits &= inner_hits - 1u;
-                    const uint32_t slot = (uint32_t)bt ^ oct;
-                    node = child_base + __popc(imask & ((1u << slot) - 1u));
-                    if (inner_hits) {
-                        if (sp >= STACK) {
-                            bad = true;
-                            done = true;
-                        } else {
-                            stack[sp++] = make_int2(child_base, (int)((inner_hits << 8) | imask));
-                        }
-                    }
+                } else if (!wide_descend<STACK>(h, oct, node, stack, sp)) {
+                    bad = true;
+                    done = true;
                 }
             }
         } else if (!done) {
-            if (sp == 0) {
-                done = true;
-            } else {
-                const int2 e = stack[sp - 1];
-                uint32_t gh = (uint32_t)e.y >> 8;
-                const uint32_t gi = (uint32_t)e.y & 0xFFu;
-                const int bt = __ffs(gh) - 1;
-                gh &= gh - 1u;
-                const uint32_t slot = (uint32_t)bt ^ oct;
-                node = e.x + __popc(gi & ((1u << slot) - 1u));
-                if (gh) stack[sp - 1].y = (int)((gh << 8) | gi);
-                else --sp;
-            }
+            node = wide_pop(stack, sp, oct);
+            if (node < 0) done = true;
         }
         if (done) {
             if (ANY) {
