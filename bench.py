@@ -299,9 +299,9 @@ def cpu_baseline_and_parity(tris, rays_np, gpu_hits_np, args, threads):
 # DRAM bytes (read + write) per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on
 # the current kernels, per ray of one closest-hit trace and per triangle of one build, for the configuration each
 # was captured with (split budget, ray order, size); other configurations report no traffic. Soup trace: the full
-# 16M-triangle, 16M-ray launch, 305.19 GB read + 12.09 GB written (profiles/trace_dram_soup16m.md).
+# 16M-triangle, 16M-ray launch, 14.71 GB read + 0.84 GB written (profiles/trace_dram_soup16m.md).
 MEASURED_TRAFFIC = {("soup16m", "emc60", "trace"): {"split_budget": 40, "order": "coherent", "triangles": 16777216,
-                                                    "per_unit": (305.19e9 + 12.09e9) / 16777216},
+                                                    "per_unit": (14.71e9 + 0.845e9) / 16777216},
                     # the first build of the run, all 34 launches (profiles/dram_traffic_build_soup16m.md)
                     ("soup16m", "emc60", "build"): {"split_budget": 40, "order": "coherent", "triangles": 16777216,
                                                     "per_unit": (22778e6 + 7764e6) / 16777216},
