@@ -71,3 +71,29 @@ def test_obj_scene_workload_round_trips_the_sphere(tmp_path):
     np.testing.assert_array_equal(sc.triangles()[4:].view(np.uint32), tris.view(np.uint32))
     assert [a.triangle_id for a in sc.area_lights] == [2, 3]
     assert sc.camera.fov == np.float32(0.9) and len(sc.point_lights) == 1
+
+
+def test_trace_order_defaults_per_workload_and_the_flag_overrides_it():
+    sys.path.insert(0, ROOT)
+    import argparse
+    import bench
+    ns = lambda w, o=None: argparse.Namespace(workload=w, trace_order=o)  # noqa: E731
+    assert bench.trace_flags(ns("soup16m")) == 2          # DIPL_TRACE_COHERENT_ORDER
+    assert bench.trace_flags(ns("displaced_sphere")) == 0
+    assert bench.trace_flags(ns("soup16m", "given")) == 0
+    assert bench.trace_flags(ns("displaced_sphere", "coherent")) == 2
+
+
+def test_measured_traffic_is_reported_only_for_the_captured_configuration():
+    sys.path.insert(0, ROOT)
+    import bench
+    n = 16777216
+    per_ray = bench.measured_traffic("soup16m", "emc60", "trace", 1, 40, "coherent", n)
+    assert per_ray is not None and per_ray > 0
+    assert bench.measured_traffic("soup16m", "emc60", "trace", n, 40, "coherent", n) == round(
+        bench.MEASURED_TRAFFIC[("soup16m", "emc60", "trace")]["per_unit"] * n)
+    # another split budget, ray order, scene size or code has no measurement
+    assert bench.measured_traffic("soup16m", "emc60", "trace", n, 0, "coherent", n) is None
+    assert bench.measured_traffic("soup16m", "emc60", "trace", n, 40, "given", n) is None
+    assert bench.measured_traffic("soup16m", "emc60", "trace", n, 40, "coherent", n // 4) is None
+    assert bench.measured_traffic("soup16m", "morton30", "trace", n, 40, "coherent", n) is None
