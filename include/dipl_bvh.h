@@ -45,7 +45,7 @@ typedef enum dipl_status {
     DIPL_ERR_OUT_OF_MEMORY = 3,    /* a device allocation failed */
     DIPL_ERR_TIMEOUT = 4,          /* a bounded device-side wait (look-back, grid barrier) gave up */
     DIPL_ERR_INTERNAL = 5,         /* a device-side consistency check failed (e.g. traversal stack) */
-    DIPL_ERR_UNSUPPORTED = 6,      /* a valid option this build does not provide */
+    DIPL_ERR_UNSUPPORTED = 6,      /* a valid option the library does not provide */
     DIPL_ERR_IO = 7                /* a scene file could not be read or parsed */
 } dipl_status;
 
